@@ -1,0 +1,210 @@
+// Context lifetime, error reporting, twiddle tables and ε⁻¹ upload.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "context.h"
+#include "ops_impl.cuh"
+
+namespace omb {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+int cuda_fail(cudaError_t e, const char* what) {
+  g_last_error = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
+  return OMB_ERR_CUDA;
+}
+
+bool fft_size_supported(int L) {
+  switch (L) {
+#define OMB_CASE(n) case n:
+    OMB_FFT_SIZES(OMB_CASE)
+#undef OMB_CASE
+    return true;
+    default: return false;
+  }
+}
+
+int row_blocks(int Nx, int Ny) {
+  const int rows = rows_for(Nx);
+  return (Ny + rows - 1) / rows;
+}
+
+int check_grid(const omb_grid* g) {
+  if (!g) return fail(OMB_ERR_INVALID_ARG, "grid is NULL");
+  if (!fft_size_supported(g->Nx) || !fft_size_supported(g->Ny))
+    return fail(OMB_ERR_UNSUPPORTED, "unsupported grid size " + std::to_string(g->Nx) + "x" +
+                                         std::to_string(g->Ny) + " (see omb_fft_size_supported)");
+  if (!(g->Dx > 0) || !(g->Dy > 0) || !std::isfinite(g->Dx) || !std::isfinite(g->Dy))
+    return fail(OMB_ERR_INVALID_ARG, "cell sizes Dx, Dy must be finite and positive");
+  return OMB_OK;
+}
+
+int upload_problem(omb_ctx* ctx, const omb_grid* g, const double* epsinv, Problem& P) {
+  int rc = check_grid(g);
+  if (rc) return rc;
+  if (!epsinv) return fail(OMB_ERR_INVALID_ARG, "epsinv is NULL");
+  P.Nx = g->Nx; P.Ny = g->Ny; P.Dx = g->Dx; P.Dy = g->Dy;
+  const size_t N = P.N();
+  std::vector<float4> a32(N);
+  std::vector<float2> b32(N);
+  std::vector<double2> e64(3 * N);
+  std::vector<float> ea32(N);
+  std::vector<double> ea64(N);
+  double emax = 0, mind = INFINITY, mean = 0;
+  for (size_t p = 0; p < 9 * N; ++p) {
+    const double v = epsinv[p];
+    if (!std::isfinite(v)) return fail(OMB_ERR_NAN, "epsinv holds a non-finite value");
+    emax = std::fmax(emax, std::fabs(v));
+  }
+  for (size_t p = 0; p < N; ++p) {
+    const double* m = epsinv + 9 * p;  // column-major 3x3: m[a + 3b] = ε⁻¹[a,b]
+    const double xx = m[0], yy = m[4], zz = m[8];
+    const double xy = 0.5 * (m[1] + m[3]), xz = 0.5 * (m[2] + m[6]), yz = 0.5 * (m[5] + m[7]);
+    const double asym = std::fmax(std::fabs(m[1] - m[3]), std::fmax(std::fabs(m[2] - m[6]), std::fabs(m[5] - m[7])));
+    if (asym > 1e-9 * emax)
+      return fail(OMB_ERR_INVALID_ARG, "epsinv is not symmetric at pixel " + std::to_string(p) +
+                                           " (the Helmholtz operator needs a real symmetric ε⁻¹)");
+    const double tr = xx + yy + zz;
+    if (!(tr > 0)) return fail(OMB_ERR_INVALID_ARG, "epsinv has a non-positive trace at pixel " + std::to_string(p));
+    mind = std::fmin(mind, std::fmin(xx, std::fmin(yy, zz)));
+    a32[p] = make_float4((float)xx, (float)yy, (float)zz, (float)xy);
+    b32[p] = make_float2((float)xz, (float)yz);
+    e64[3 * p] = make_double2(xx, yy);
+    e64[3 * p + 1] = make_double2(zz, xy);
+    e64[3 * p + 2] = make_double2(xz, yz);
+    ea64[p] = 3.0 / tr;
+    ea32[p] = (float)ea64[p];
+    mean += ea64[p];
+  }
+  if (!(mind > 0)) return fail(OMB_ERR_INVALID_ARG, "epsinv has a non-positive diagonal entry");
+  P.eps_mean = mean / (double)N;
+  P.min_diag = mind;
+  cudaStream_t st = ctx->stream;
+  OMB_CU(P.e32a.alloc(N, st));
+  OMB_CU(P.e32b.alloc(N, st));
+  OMB_CU(P.e64.alloc(3 * N, st));
+  OMB_CU(P.eave32.alloc(N, st));
+  OMB_CU(P.eave64.alloc(N, st));
+  OMB_CU(cudaMemcpyAsync(P.e32a.p, a32.data(), N * sizeof(float4), cudaMemcpyHostToDevice, st));
+  OMB_CU(cudaMemcpyAsync(P.e32b.p, b32.data(), N * sizeof(float2), cudaMemcpyHostToDevice, st));
+  OMB_CU(cudaMemcpyAsync(P.e64.p, e64.data(), 3 * N * sizeof(double2), cudaMemcpyHostToDevice, st));
+  OMB_CU(cudaMemcpyAsync(P.eave32.p, ea32.data(), N * sizeof(float), cudaMemcpyHostToDevice, st));
+  OMB_CU(cudaMemcpyAsync(P.eave64.p, ea64.data(), N * sizeof(double), cudaMemcpyHostToDevice, st));
+  // host vectors die at return: make the copies complete first
+  OMB_CU(cudaStreamSynchronize(st));
+  return OMB_OK;
+}
+
+template <> OpUnit<float> make_unit<float>(const Problem& P) {
+  OpUnit<float> u{};
+  u.e32a = P.e32a.p; u.e32b = P.e32b.p; u.e64 = P.e64.p; u.eave = P.eave32.p;
+  u.Nx = P.Nx; u.Ny = P.Ny;
+  u.inv_dx = (float)(1.0 / P.Dx); u.inv_dy = (float)(1.0 / P.Dy);
+  u.part_stride = row_blocks(P.Nx, P.Ny);
+  return u;
+}
+template <> OpUnit<double> make_unit<double>(const Problem& P) {
+  OpUnit<double> u{};
+  u.e32a = P.e32a.p; u.e32b = P.e32b.p; u.e64 = P.e64.p; u.eave = P.eave64.p;
+  u.Nx = P.Nx; u.Ny = P.Ny;
+  u.inv_dx = 1.0 / P.Dx; u.inv_dy = 1.0 / P.Dy;
+  u.part_stride = row_blocks(P.Nx, P.Ny);
+  return u;
+}
+
+static int make_twiddles(omb_ctx* ctx) {
+  // one table per supported length, exp(-2πi m/L) for m < L, FP64 and FP32 copies
+  std::vector<int> lens;
+#define OMB_CASE(n) lens.push_back(n);
+  OMB_FFT_SIZES(OMB_CASE)
+#undef OMB_CASE
+  size_t tot = 0;
+  for (int L : lens) tot += L;
+  std::vector<double2> h64(tot);
+  std::vector<float2> h32(tot);
+  size_t off = 0;
+  const double two_pi = 6.283185307179586476925286766559;
+  for (int L : lens) {
+    for (int m = 0; m < L; ++m) {
+      // reduce the angle to [0, π/4]-symmetric evaluation for accuracy
+      const double a = -two_pi * (double)m / (double)L;
+      double c = std::cos(a), s = std::sin(a);
+      if (4 * m == L) { c = 0; s = -1; }
+      if (2 * m == L) { c = -1; s = 0; }
+      if (4 * m == 3 * L) { c = 0; s = 1; }
+      h64[off + m] = make_double2(c, s);
+      h32[off + m] = make_float2((float)c, (float)s);
+    }
+    off += L;
+  }
+  void* mem = nullptr;
+  OMB_CU(cudaMalloc(&mem, tot * (sizeof(double2) + sizeof(float2))));
+  double2* d64 = reinterpret_cast<double2*>(mem);
+  float2* d32 = reinterpret_cast<float2*>(d64 + tot);
+  OMB_CU(cudaMemcpy(d64, h64.data(), tot * sizeof(double2), cudaMemcpyHostToDevice));
+  OMB_CU(cudaMemcpy(d32, h32.data(), tot * sizeof(float2), cudaMemcpyHostToDevice));
+  off = 0;
+  for (int L : lens) {
+    ctx->tw.f64[L] = d64 + off;
+    ctx->tw.f32[L] = d32 + off;
+    off += L;
+  }
+  ctx->tw_mem = mem;
+  return OMB_OK;
+}
+
+}  // namespace omb
+
+using namespace omb;
+
+extern "C" {
+
+int omb_version(void) { return 100; }
+
+int omb_fft_size_supported(int n) { return fft_size_supported(n) ? 1 : 0; }
+
+const char* omb_last_error(void) { return g_last_error.c_str(); }
+
+int omb_ctx_create(int device, omb_ctx** out) {
+  if (!out) return fail(OMB_ERR_INVALID_ARG, "out is NULL");
+  *out = nullptr;
+  int ndev = 0;
+  OMB_CU(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev)
+    return fail(OMB_ERR_INVALID_ARG, "device " + std::to_string(device) + " out of range (found " +
+                                         std::to_string(ndev) + ")");
+  OMB_CU(cudaSetDevice(device));
+  omb_ctx* c = new omb_ctx();
+  c->device = device;
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { delete c; return cuda_fail(e, "cudaStreamCreate"); }
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+  // keep freed blocks in the device pool between calls
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  int rc = make_twiddles(c);
+  if (rc) { cudaStreamDestroy(c->stream); delete c; return rc; }
+  *out = c;
+  return OMB_OK;
+}
+
+int omb_ctx_destroy(omb_ctx* ctx) {
+  if (!ctx) return OMB_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->tw_mem) cudaFree(ctx->tw_mem);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return OMB_OK;
+}
+
+}  // extern "C"

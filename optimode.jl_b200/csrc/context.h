@@ -1,0 +1,83 @@
+// Context, error reporting, device buffers and problem upload for libomb200.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <utility>
+
+#include "omb200.h"
+#include "ops.h"
+
+struct omb_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  omb::TwTables tw{};
+  void* tw_mem = nullptr;
+  int num_sms = 0;
+};
+
+namespace omb {
+
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define OMB_CU(x)                                            \
+  do {                                                       \
+    cudaError_t e__ = (x);                                   \
+    if (e__ != cudaSuccess) return ::omb::cuda_fail(e__, #x); \
+  } while (0)
+
+// Stream-ordered device buffer (cudaMallocAsync from the device's pool).
+template <typename T> struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  cudaStream_t st = nullptr;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), st(o.st) { o.p = nullptr; o.n = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) { release(); p = o.p; n = o.n; st = o.st; o.p = nullptr; o.n = 0; }
+    return *this;
+  }
+  ~DevBuf() { release(); }
+  cudaError_t alloc(size_t count, cudaStream_t stream) {
+    release();
+    st = stream;
+    n = count;
+    if (count == 0) return cudaSuccess;
+    return cudaMallocAsync(reinterpret_cast<void**>(&p), count * sizeof(T), stream);
+  }
+  cudaError_t zero() { return n ? cudaMemsetAsync(p, 0, n * sizeof(T), st) : cudaSuccess; }
+  void release() {
+    if (p) cudaFreeAsync(p, st);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+// ε⁻¹ of one cell resident on the device in both precisions (6 unique entries per pixel)
+// plus ε_ave = 3/tr(ε⁻¹) for the MPB-style preconditioner.
+struct Problem {
+  int Nx = 0, Ny = 0;
+  double Dx = 0, Dy = 0;
+  double eps_mean = 0;  // cell mean of ε_ave (diagonal preconditioner scale)
+  double min_diag = 0;  // min over pixels and a of ε⁻¹[a,a] (k_guess)
+  DevBuf<float4> e32a;
+  DevBuf<float2> e32b;
+  DevBuf<double2> e64;
+  DevBuf<float> eave32;
+  DevBuf<double> eave64;
+  size_t N() const { return (size_t)Nx * Ny; }
+};
+
+// Validate the grid and ε⁻¹ and upload them.  Returns OMB_OK or an error code.
+int check_grid(const omb_grid* g);
+int upload_problem(omb_ctx* ctx, const omb_grid* g, const double* epsinv, Problem& P);
+
+// Fill an OpUnit for one problem (pointers to block buffers set by the caller).
+template <typename T> OpUnit<T> make_unit(const Problem& P);
+
+}  // namespace omb

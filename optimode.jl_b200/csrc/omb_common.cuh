@@ -1,0 +1,66 @@
+// Common device/host helpers for libomb200 (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <type_traits>
+
+namespace omb {
+
+template <typename T> struct cplx_t;
+template <> struct cplx_t<float> { using type = float2; };
+template <> struct cplx_t<double> { using type = double2; };
+template <typename T> using cplx = typename cplx_t<T>::type;
+
+template <typename C> __host__ __device__ __forceinline__ C mk(decltype(C::x) a, decltype(C::x) b) {
+  C r; r.x = a; r.y = b; return r;
+}
+__host__ __device__ __forceinline__ float2 operator+(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ float2 operator-(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ float2 operator*(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__host__ __device__ __forceinline__ float2 operator*(float s, float2 a) { return make_float2(a.x * s, a.y * s); }
+__host__ __device__ __forceinline__ double2 operator+(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ double2 operator-(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ double2 operator*(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__host__ __device__ __forceinline__ double2 operator*(double s, double2 a) { return make_double2(a.x * s, a.y * s); }
+
+template <typename C> __host__ __device__ __forceinline__ C cmul(C a, C b) {
+  C r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
+}
+// a * conj(b)
+template <typename C> __host__ __device__ __forceinline__ C cmulc(C a, C b) {
+  C r; r.x = a.x * b.x + a.y * b.y; r.y = a.y * b.x - a.x * b.y; return r;
+}
+template <typename C> __host__ __device__ __forceinline__ C cconj(C a) { C r; r.x = a.x; r.y = -a.y; return r; }
+// multiply by -i (forward) or +i (inverse)
+template <bool INV, typename C> __host__ __device__ __forceinline__ C mul_mi(C a) {
+  C r;
+  if (INV) { r.x = -a.y; r.y = a.x; } else { r.x = a.y; r.y = -a.x; }
+  return r;
+}
+
+// Signed FFT-order frequency index of bin i on an n-point axis (fftfreq order).
+__host__ __device__ __forceinline__ int freq_index(int i, int n) { return (i < (n + 1) / 2) ? i : i - n; }
+
+// Transverse polarisation basis at one plane wave, kpg = k ẑ − G with G = (gx, gy, 0):
+// mag = |kpg|, n̂ = ẑ×kpg/|ẑ×kpg| (ŷ when kpg ∥ ẑ), m̂ = n̂×kpg/|n̂×kpg|.
+template <typename T> struct Basis { T mag, mx, my, mz, nx, ny; };
+
+template <typename T>
+__host__ __device__ __forceinline__ Basis<T> basis_at(T k, T gx, T gy) {
+  Basis<T> b;
+  T p2 = gx * gx + gy * gy;
+  b.mag = sqrt(p2 + k * k);
+  if (p2 > T(0)) {
+    T ip = T(1) / sqrt(p2);
+    T im = T(1) / b.mag;
+    b.nx = gy * ip; b.ny = -gx * ip;
+    b.mx = -gx * k * ip * im; b.my = -gy * k * ip * im; b.mz = -p2 * ip * im;
+  } else {
+    b.nx = T(0); b.ny = T(1);
+    b.mx = (k >= T(0)) ? T(1) : T(-1); b.my = T(0); b.mz = T(0);
+  }
+  return b;
+}
+
+}  // namespace omb

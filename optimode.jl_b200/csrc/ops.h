@@ -1,0 +1,33 @@
+// Host-side launchers for the fused operator passes.
+#pragma once
+
+#include "op_kernels.cuh"
+
+namespace omb {
+
+// Operator pipelines built from the row_in / col / row_out passes.
+enum OpKind : int {
+  OP_M = 0,       // Hout = M̂(k) Hin                       (_M!)
+  OP_P = 1,       // Hout = P̂(k) Hin, MPB-style              (_P!)
+  OP_HMKH = 2,    // partial sums of ⟨Hin, kx_ct bfft ε⁻¹ fft zx_tc Hin⟩/N  (HMₖH)
+  OP_EFIELD = 3,  // scratch ← ε⁻¹·fft2(kx_tc Hin)            (E⃗, un-normalised)
+  OP_H2D = 4,     // scratch ← fft2(kx_tc Hin)                (_H2d!)
+  OP_D2E = 5,     // out (planar 3N) ← bfft2(ε⁻¹·scratch)     (_d2ẽ!)
+  OP_MDOT = 6,    // like OP_M but reduces ⟨Hin, M̂ Hin⟩ partials instead of storing
+};
+
+// Twiddle tables exp(-2πi m/L) for every supported length, per precision.
+struct TwTables {
+  const float2* f32[1025];
+  const double2* f64[1025];
+};
+
+bool fft_size_supported(int L);
+// Number of row blocks row_out uses for a grid with Ny rows (partial sums per column).
+int row_blocks(int Nx, int Ny);
+
+template <typename T>
+cudaError_t launch_op(OpKind op, const OpUnit<T>* d_units, int nunits, int Nx, int Ny, int maxcol,
+                      const TwTables& tw, cudaStream_t st);
+
+}  // namespace omb

@@ -1,0 +1,155 @@
+// Size/mode dispatch for the fused operator passes.  Included once per precision.
+#pragma once
+
+#include "ops.h"
+
+namespace omb {
+
+#define OMB_FFT_SIZES(X) X(8) X(12) X(16) X(20) X(24) X(32) X(40) X(48) X(64) X(80) X(96) \
+  X(128) X(160) X(192) X(256) X(320) X(384) X(512)
+
+// Launch shape policy.  Row passes: NT_ROW threads, ROWS grid rows per CTA (≈512 pixels).
+// Column pass: NT_COL threads, TX adjacent columns per CTA (8 for coalesced row segments,
+// 4 for FP64 above 256 points to stay inside the shared-memory budget).
+constexpr int NT_ROW = 128;
+constexpr int NT_COL = 256;
+__host__ __device__ constexpr int rows_for(int NX) { return NX >= 512 ? 1 : 512 / NX; }
+template <typename T> __host__ __device__ constexpr int tx_for(int NY) {
+  return (NY <= 256) ? 8 : (sizeof(T) == 4 ? 8 : 4);
+}
+
+template <typename T>
+using PassKernel = void (*)(const OpUnit<T>*, const cplx<T>*);
+
+template <typename T>
+static cudaError_t launch_pass(PassKernel<T> kern, dim3 g, int nt, size_t smem, cudaStream_t st,
+                               const OpUnit<T>* units, const cplx<T>* tw) {
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  kern<<<g, nt, smem, st>>>(units, tw);
+  return cudaGetLastError();
+}
+
+template <typename T, int NX>
+static cudaError_t row_in_nx(int mode, const OpUnit<T>* u, int nunits, int Ny, int maxcol,
+                             const cplx<T>* tw, cudaStream_t st) {
+  constexpr int ROWS = rows_for(NX);
+  const size_t sm = (NX + 3 * ROWS * (NX + 1)) * sizeof(cplx<T>);
+  const dim3 g((Ny + ROWS - 1) / ROWS, maxcol, nunits);
+  switch (mode) {
+    case RI_KXTC: return launch_pass<T>(k_row_in<T, NX, ROWS, NT_ROW, RI_KXTC, false>, g, NT_ROW, sm, st, u, tw);
+    case RI_KXINV: return launch_pass<T>(k_row_in<T, NX, ROWS, NT_ROW, RI_KXINV, true>, g, NT_ROW, sm, st, u, tw);
+    case RI_ZXTC: return launch_pass<T>(k_row_in<T, NX, ROWS, NT_ROW, RI_ZXTC, false>, g, NT_ROW, sm, st, u, tw);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <typename T, int NX>
+static cudaError_t row_out_nx(int mode, const OpUnit<T>* u, int nunits, int Ny, int maxcol,
+                              const cplx<T>* tw, cudaStream_t st) {
+  constexpr int ROWS = rows_for(NX);
+  const size_t sm = (NX + 3 * ROWS * (NX + 1)) * sizeof(cplx<T>);
+  const dim3 g((Ny + ROWS - 1) / ROWS, maxcol, nunits);
+  switch (mode) {
+    case RO_KXCT: return launch_pass<T>(k_row_out<T, NX, ROWS, NT_ROW, RO_KXCT, true>, g, NT_ROW, sm, st, u, tw);
+    case RO_KXINVCT: return launch_pass<T>(k_row_out<T, NX, ROWS, NT_ROW, RO_KXINVCT, false>, g, NT_ROW, sm, st, u, tw);
+    case RO_STORE3: return launch_pass<T>(k_row_out<T, NX, ROWS, NT_ROW, RO_STORE3, true>, g, NT_ROW, sm, st, u, tw);
+    case RO_KXCT_DOT: return launch_pass<T>(k_row_out<T, NX, ROWS, NT_ROW, RO_KXCT_DOT, true>, g, NT_ROW, sm, st, u, tw);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+// column-pass modes
+enum ColMode : int { CM_M = 0, CM_P = 1, CM_E = 2, CM_FWD = 3, CM_EPSINV = 4 };
+
+template <typename T, int NY>
+static cudaError_t col_ny(int mode, const OpUnit<T>* u, int nunits, int Nx, int maxcol,
+                          const cplx<T>* tw, cudaStream_t st) {
+  constexpr int TX = tx_for<T>(NY);
+  const size_t sm = (NY + 3 * TX * (NY + 1)) * sizeof(cplx<T>);
+  const dim3 g((Nx + TX - 1) / TX, maxcol, nunits);
+  switch (mode) {
+    case CM_M: return launch_pass<T>(k_col<T, NY, TX, NT_COL, CS_FWD, PW_EPS, CS_INV>, g, NT_COL, sm, st, u, tw);
+    case CM_P: return launch_pass<T>(k_col<T, NY, TX, NT_COL, CS_INV, PW_EAVE, CS_FWD>, g, NT_COL, sm, st, u, tw);
+    case CM_E: return launch_pass<T>(k_col<T, NY, TX, NT_COL, CS_FWD, PW_EPS, CS_NONE>, g, NT_COL, sm, st, u, tw);
+    case CM_FWD: return launch_pass<T>(k_col<T, NY, TX, NT_COL, CS_FWD, PW_NONE, CS_NONE>, g, NT_COL, sm, st, u, tw);
+    case CM_EPSINV: return launch_pass<T>(k_col<T, NY, TX, NT_COL, CS_NONE, PW_EPS, CS_INV>, g, NT_COL, sm, st, u, tw);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+template <typename T> static const cplx<T>* tw_for(const TwTables& t, int L);
+template <> const float2* tw_for<float>(const TwTables& t, int L) { return t.f32[L]; }
+template <> const double2* tw_for<double>(const TwTables& t, int L) { return t.f64[L]; }
+
+template <typename T>
+static cudaError_t row_in(int mode, const OpUnit<T>* u, int nunits, int Nx, int Ny, int maxcol,
+                          const TwTables& t, cudaStream_t st) {
+  switch (Nx) {
+#define OMB_CASE(L) case L: return row_in_nx<T, L>(mode, u, nunits, Ny, maxcol, tw_for<T>(t, L), st);
+    OMB_FFT_SIZES(OMB_CASE)
+#undef OMB_CASE
+    default: return cudaErrorInvalidValue;
+  }
+}
+template <typename T>
+static cudaError_t row_out(int mode, const OpUnit<T>* u, int nunits, int Nx, int Ny, int maxcol,
+                           const TwTables& t, cudaStream_t st) {
+  switch (Nx) {
+#define OMB_CASE(L) case L: return row_out_nx<T, L>(mode, u, nunits, Ny, maxcol, tw_for<T>(t, L), st);
+    OMB_FFT_SIZES(OMB_CASE)
+#undef OMB_CASE
+    default: return cudaErrorInvalidValue;
+  }
+}
+template <typename T>
+static cudaError_t col(int mode, const OpUnit<T>* u, int nunits, int Nx, int Ny, int maxcol,
+                       const TwTables& t, cudaStream_t st) {
+  switch (Ny) {
+#define OMB_CASE(L) case L: return col_ny<T, L>(mode, u, nunits, Nx, maxcol, tw_for<T>(t, L), st);
+    OMB_FFT_SIZES(OMB_CASE)
+#undef OMB_CASE
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+#define OMB_TRY(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) return e_; } while (0)
+
+template <typename T>
+cudaError_t launch_op(OpKind op, const OpUnit<T>* u, int nunits, int Nx, int Ny, int maxcol,
+                      const TwTables& t, cudaStream_t st) {
+  if (nunits <= 0 || maxcol <= 0) return cudaSuccess;
+  switch (op) {
+    case OP_M:
+      OMB_TRY(row_in<T>(RI_KXTC, u, nunits, Nx, Ny, maxcol, t, st));
+      OMB_TRY(col<T>(CM_M, u, nunits, Nx, Ny, maxcol, t, st));
+      return row_out<T>(RO_KXCT, u, nunits, Nx, Ny, maxcol, t, st);
+    case OP_MDOT:
+      OMB_TRY(row_in<T>(RI_KXTC, u, nunits, Nx, Ny, maxcol, t, st));
+      OMB_TRY(col<T>(CM_M, u, nunits, Nx, Ny, maxcol, t, st));
+      return row_out<T>(RO_KXCT_DOT, u, nunits, Nx, Ny, maxcol, t, st);
+    case OP_P:
+      OMB_TRY(row_in<T>(RI_KXINV, u, nunits, Nx, Ny, maxcol, t, st));
+      OMB_TRY(col<T>(CM_P, u, nunits, Nx, Ny, maxcol, t, st));
+      return row_out<T>(RO_KXINVCT, u, nunits, Nx, Ny, maxcol, t, st);
+    case OP_HMKH:
+      OMB_TRY(row_in<T>(RI_ZXTC, u, nunits, Nx, Ny, maxcol, t, st));
+      OMB_TRY(col<T>(CM_M, u, nunits, Nx, Ny, maxcol, t, st));
+      return row_out<T>(RO_KXCT_DOT, u, nunits, Nx, Ny, maxcol, t, st);
+    case OP_EFIELD:
+      OMB_TRY(row_in<T>(RI_KXTC, u, nunits, Nx, Ny, maxcol, t, st));
+      return col<T>(CM_E, u, nunits, Nx, Ny, maxcol, t, st);
+    case OP_H2D:
+      OMB_TRY(row_in<T>(RI_KXTC, u, nunits, Nx, Ny, maxcol, t, st));
+      return col<T>(CM_FWD, u, nunits, Nx, Ny, maxcol, t, st);
+    case OP_D2E:
+      OMB_TRY(col<T>(CM_EPSINV, u, nunits, Nx, Ny, maxcol, t, st));
+      return row_out<T>(RO_STORE3, u, nunits, Nx, Ny, maxcol, t, st);
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace omb

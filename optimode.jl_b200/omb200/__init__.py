@@ -1,0 +1,11 @@
+"""omb200 — host-side Python binding of libomb200, the B200-native plane-wave Helmholtz
+eigensolver (the ``solve_ω²`` / ``solve_k`` hot path of OptiMode.jl and its adjoint).
+
+The compute path is the CUDA library ``libomb200.so`` behind the C ABI in
+``include/omb200.h``; this package only converts arrays and calls it.  There is no CPU
+fallback.
+"""
+
+from ._lib import OmbError, load as load_library  # noqa: F401
+from .grid import Grid  # noqa: F401
+from .ops import apply, apply_M, apply_P, HMkH, E_field  # noqa: F401

@@ -1,0 +1,126 @@
+"""ctypes binding of ``libomb200.so`` (the C ABI declared in ``include/omb200.h``).
+
+The shared library is built in place next to this package (``make -C optimode.jl_b200``
+or ``__graft_entry__.build()``).  There is no CPU fallback: if the library or a CUDA
+device is missing, every entry point raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "libomb200.so")
+
+OMB_OK = 0
+ERROR_NAMES = {
+    1: "OMB_ERR_INVALID_ARG", 2: "OMB_ERR_CUDA", 3: "OMB_ERR_NOT_CONVERGED",
+    4: "OMB_ERR_ORTHO_FAIL", 5: "OMB_ERR_TIMEOUT", 6: "OMB_ERR_UNSUPPORTED", 7: "OMB_ERR_NAN",
+}
+PREC = {"fp32": 0, "f32": 0, "fp64": 1, "f64": 1, "mixed": 2}
+OPS = {"M": 0, "P": 1, "P_diag": 2}
+
+#: every symbol ``include/omb200.h`` declares (checked by the CPU test suite)
+EXPORTS = (
+    "omb_version", "omb_fft_size_supported", "omb_last_error", "omb_ctx_create",
+    "omb_ctx_destroy", "omb_apply", "omb_HMkH", "omb_efield",
+)
+
+
+class OmbError(RuntimeError):
+    """A non-zero status from libomb200, with the library's message."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERROR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class c_grid(ctypes.Structure):
+    _fields_ = [("Nx", ctypes.c_int32), ("Ny", ctypes.c_int32),
+                ("Dx", ctypes.c_double), ("Dy", ctypes.c_double)]
+
+
+_lib = None
+_lock = threading.Lock()
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def load():
+    """Load the library (once).  Raises ``OSError`` naming the missing file."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"libomb200.so not found at {LIB_PATH}: build it with "
+                          "`make -C optimode.jl_b200 -j` (there is no CPU fallback)")
+        lib = ctypes.CDLL(LIB_PATH)
+        vp = ctypes.c_void_p
+        gp = ctypes.POINTER(c_grid)
+        sig = {
+            "omb_version": (ctypes.c_int, []),
+            "omb_fft_size_supported": (ctypes.c_int, [ctypes.c_int]),
+            "omb_last_error": (ctypes.c_char_p, []),
+            "omb_ctx_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(vp)]),
+            "omb_ctx_destroy": (ctypes.c_int, [vp]),
+            "omb_apply": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, gp, ctypes.c_double, _dp,
+                                         ctypes.c_int, _dp, _dp]),
+            "omb_HMkH": (ctypes.c_int, [vp, ctypes.c_int, gp, ctypes.c_double, _dp, ctypes.c_int,
+                                        _dp, _dp]),
+            "omb_efield": (ctypes.c_int, [vp, ctypes.c_int, gp, ctypes.c_double, _dp, _dp, _dp]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+        return lib
+
+
+def check(rc: int) -> None:
+    if rc != OMB_OK:
+        msg = load().omb_last_error().decode("utf-8", "replace")
+        raise OmbError(rc, msg)
+
+
+def dptr(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+class Context:
+    """One libomb200 context (a CUDA stream, twiddle tables, a memory pool) per device."""
+
+    def __init__(self, device: int = 0):
+        lib = load()
+        h = ctypes.c_void_p()
+        check(lib.omb_ctx_create(int(device), ctypes.byref(h)))
+        self.handle = h
+        self.device = int(device)
+
+    def close(self):
+        if self.handle:
+            load().omb_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_contexts: dict = {}
+
+
+def context(device: int = 0) -> Context:
+    with _lock:
+        pass
+    c = _contexts.get(device)
+    if c is None or c.handle is None:
+        c = Context(device)
+        _contexts[device] = c
+    return c

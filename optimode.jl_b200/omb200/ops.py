@@ -1,0 +1,82 @@
+"""Single operator evaluations through the C ABI (``omb_apply``, ``omb_HMkH``,
+``omb_efield``).  These mirror the reference's ``HelmholtzMap`` / ``HelmholtzPreconditioner``
+application, ``HMₖH`` and ``E⃗`` (``lib/MaxwellEigenmodes/src/maxwell.jl``,
+``src/fields.jl``) and are what the parity tests call."""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .grid import Grid
+
+
+def epsinv_host(epsinv, grid: Grid) -> np.ndarray:
+    """Reference-indexed ``(3, 3, Nx, Ny)`` ε⁻¹ as the column-major Float64 memory the C ABI
+    reads."""
+    e = np.asarray(epsinv, dtype=np.float64)
+    if e.shape != (3, 3, grid.Nx, grid.Ny):
+        raise ValueError(f"epsinv must have shape (3, 3, {grid.Nx}, {grid.Ny}), got {e.shape}")
+    return np.asfortranarray(e)
+
+
+def block_host(H, n: int):
+    """Complex block → (column-major complex128 array of shape (n, ncol), ncol, was_vector)."""
+    H = np.asarray(H)
+    vec = H.ndim == 1
+    B = H.reshape(n, 1) if vec else H
+    if B.shape[0] != n:
+        raise ValueError(f"field length must be {n}, got {B.shape[0]}")
+    return np.asfortranarray(B.astype(np.complex128, copy=False)), B.shape[1], vec
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def apply(op: str, k: float, epsinv, grid: Grid, H, precision: str = "fp64", device: int = 0):
+    """``op`` ∈ {"M", "P", "P_diag"} applied to one field or a block of columns."""
+    lib = _lib.load()
+    ctx = _lib.context(device)
+    e = epsinv_host(epsinv, grid)
+    B, ncol, vec = block_host(H, 2 * grid.N)
+    out = np.empty_like(B, order="F")
+    _lib.check(lib.omb_apply(ctx.handle, _lib.OPS[op], _lib.PREC[precision], ctypes.byref(grid.c()),
+                             float(k), _dptr(e), ncol, _dptr(B), _dptr(out)))
+    return out[:, 0].copy() if vec else out
+
+
+def apply_M(k, epsinv, grid, H, precision="fp64", device=0):
+    return apply("M", k, epsinv, grid, H, precision, device)
+
+
+def apply_P(k, epsinv, grid, H, precision="fp64", kind="mpb", device=0):
+    return apply("P" if kind == "mpb" else "P_diag", k, epsinv, grid, H, precision, device)
+
+
+def HMkH(k, epsinv, grid, H, precision="fp64", device=0):
+    """⟨H|∂M̂/∂k|H⟩ per column (a float for a single vector)."""
+    lib = _lib.load()
+    ctx = _lib.context(device)
+    e = epsinv_host(epsinv, grid)
+    B, ncol, vec = block_host(H, 2 * grid.N)
+    out = np.empty(ncol)
+    _lib.check(lib.omb_HMkH(ctx.handle, _lib.PREC[precision], ctypes.byref(grid.c()), float(k),
+                            _dptr(e), ncol, _dptr(B), _dptr(out)))
+    return float(out[0]) if vec else out
+
+
+def E_field(k, epsinv, grid, H, precision="fp64", device=0):
+    """Un-normalised E = ε⁻¹·fft(kx_tc H) as a flat ``(3, Nx, Ny)`` column-major vector."""
+    lib = _lib.load()
+    ctx = _lib.context(device)
+    e = epsinv_host(epsinv, grid)
+    B, ncol, vec = block_host(H, 2 * grid.N)
+    if ncol != 1:
+        raise ValueError("E_field takes one column")
+    out = np.empty(3 * grid.N, dtype=np.complex128)
+    _lib.check(lib.omb_efield(ctx.handle, _lib.PREC[precision], ctypes.byref(grid.c()), float(k),
+                              _dptr(e), _dptr(B), _dptr(out)))
+    return out

@@ -1,0 +1,60 @@
+"""The C-ABI library builds, loads and exports every symbol its header declares; without a
+GPU it refuses to run instead of falling back to the CPU.  No GPU needed."""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "omb200.h")
+
+
+def _ensure_built():
+    from omb200 import _lib
+    if not os.path.exists(_lib.LIB_PATH):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "optimode.jl_b200"), "-j8"], check=True,
+                       stdout=subprocess.DEVNULL)
+    return _lib
+
+
+def _declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(omb_[a-zA-Z0-9_]+)\s*\(", src)))
+
+
+def test_header_declares_what_the_binding_exports():
+    from omb200 import _lib
+    assert sorted(_lib.EXPORTS) == _declared_functions()
+
+
+def test_library_exports_every_declared_symbol():
+    _lib = _ensure_built()
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    for name in _declared_functions():
+        assert hasattr(lib, name), name
+
+
+def test_library_metadata_without_gpu():
+    _lib = _ensure_built()
+    lib = _lib.load()
+    assert lib.omb_version() >= 100
+    for n in (8, 12, 16, 20, 24, 128, 192, 256, 512):
+        assert lib.omb_fft_size_supported(n) == 1
+    for n in (7, 14, 1000, 0, -4):
+        assert lib.omb_fft_size_supported(n) == 0
+
+
+def test_no_cpu_fallback_without_gpu(cuda_available):
+    if cuda_available:
+        pytest.skip("a GPU is present")
+    _lib = _ensure_built()
+    with pytest.raises(_lib.OmbError) as ei:
+        _lib.Context(0)
+    assert "CUDA" in str(ei.value)

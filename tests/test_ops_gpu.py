@@ -1,0 +1,116 @@
+"""Parity of the fused operator kernels (M̂, P̂, HMₖH, E) with the FP64 oracle, through the
+C ABI.  Tolerances: relative L2 ≤ 1e-12 in FP64 and ≤ 3e-6 in FP32."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import gaussian_epsinv, P_WG
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-12, "fp32": 3e-6}
+
+# (Nx, Ny, Dx, Dy): non-square, radix-2/3/5, the bench sizes and the largest size
+GRIDS = [(24, 16, 6.0, 4.0), (12, 8, 3.0, 2.0), (20, 40, 2.0, 4.0), (128, 128, 6.0, 4.0),
+         (192, 128, 6.0, 4.0), (256, 192, 8.0, 5.0), (256, 256, 8.0, 5.0), (512, 512, 8.0, 8.0)]
+
+
+def random_epsinv(Nx, Ny, seed=0):
+    """Random anisotropic symmetric positive-definite ε per pixel, inverted."""
+    rng = np.random.default_rng(seed)
+    Q, _ = np.linalg.qr(rng.standard_normal((Nx, Ny, 3, 3)))
+    d = rng.uniform(1.0, 12.0, (Nx, Ny, 3))
+    eps = np.einsum("xyab,xyb,xycb->xyac", Q, d, Q)
+    ei = np.linalg.inv(eps)
+    ei = 0.5 * (ei + np.swapaxes(ei, -1, -2))
+    return np.ascontiguousarray(np.transpose(ei, (2, 3, 0, 1)))
+
+
+def rand_block(n, m, seed):
+    rng = np.random.default_rng(seed)
+    return rng.standard_normal((n, m)) + 1j * rng.standard_normal((n, m))
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+@pytest.fixture(scope="module")
+def omb():
+    import omb200
+    return omb200
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("Nx,Ny,Dx,Dy", GRIDS)
+def test_apply_M_and_P(omb, prec, Nx, Ny, Dx, Dy):
+    g = omb.Grid(Dx, Dy, Nx, Ny)
+    og = O.Grid(Dx, Dy, Nx, Ny)
+    ei = random_epsinv(Nx, Ny, seed=Nx + Ny)
+    k = 1.37
+    H = rand_block(2 * g.N, 3, seed=1)
+    op = O.Operator(k, ei, og)
+    out = omb.apply_M(k, ei, g, H, precision=prec)
+    ref = op.M_block(H)
+    assert rel(out, ref) < TOL[prec]
+    outp = omb.apply_P(k, ei, g, H, precision=prec)
+    assert rel(outp, op.P_block(H)) < TOL[prec]
+    outd = omb.apply_P(k, ei, g, H, precision=prec, kind="diag")
+    assert rel(outd, op.P_block(H, "diag")) < TOL[prec]
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("Nx,Ny,Dx,Dy", GRIDS[:5])
+def test_HMkH_and_Efield(omb, prec, Nx, Ny, Dx, Dy):
+    g = omb.Grid(Dx, Dy, Nx, Ny)
+    og = O.Grid(Dx, Dy, Nx, Ny)
+    ei = random_epsinv(Nx, Ny, seed=3)
+    k = 1.1
+    H = rand_block(2 * g.N, 2, seed=2)
+    H /= np.linalg.norm(H, axis=0)
+    op = O.Operator(k, ei, og)
+    got = omb.HMkH(k, ei, g, H, precision=prec)
+    ref = np.array([op.HMkH(H[:, j]) for j in range(2)])
+    assert np.allclose(got, ref, rtol=10 * TOL[prec], atol=0)
+    E = omb.E_field(k, ei, g, H[:, 0], precision=prec)
+    assert rel(E, O.E_field(k, H[:, 0], ei, og)) < TOL[prec]
+
+
+def test_hermitian_fp64(omb):
+    # ME/test/runtests.jl:50-58, rtol 1e-9
+    g = omb.Grid(6.0, 4.0, 24, 16)
+    ei = gaussian_epsinv(P_WG)
+    k0 = O.k_guess(1 / 1.55, ei)
+    V = rand_block(2 * g.N, 2, seed=9)
+    MV = omb.apply_M(k0, ei, g, V)
+    a = np.vdot(V[:, 1], MV[:, 0])
+    b = np.conj(np.vdot(V[:, 0], MV[:, 1]))
+    assert np.isclose(a, b, rtol=1e-9)
+
+
+def test_uniform_medium_is_diagonal(omb):
+    g = omb.Grid(6.0, 4.0, 24, 16)
+    ei = np.zeros((3, 3, 24, 16))
+    for a in range(3):
+        ei[a, a] = 1 / 2.5
+    op = O.Operator(1.3, ei, O.Grid(6.0, 4.0, 24, 16))
+    v = rand_block(2 * g.N, 1, 4)[:, 0]
+    assert rel(omb.apply_M(1.3, ei, g, v), np.repeat((op.mag ** 2 / 2.5).reshape(-1), 2) * v) < 1e-13
+
+
+def test_rejects_bad_input(omb):
+    g = omb.Grid(6.0, 4.0, 24, 16)
+    ei = gaussian_epsinv(P_WG)
+    bad = ei.copy()
+    bad[0, 1, 3, 3] = 0.3  # asymmetric
+    with pytest.raises(omb.OmbError, match="symmetric"):
+        omb.apply_M(1.2, bad, g, np.ones(2 * g.N, complex))
+    with pytest.raises(omb.OmbError, match="unsupported grid"):
+        omb.apply_M(1.2, np.zeros((3, 3, 14, 16)), omb.Grid(6.0, 4.0, 14, 16), np.ones(2 * 14 * 16, complex))
+    nan = ei.copy()
+    nan[1, 1, 0, 0] = np.nan
+    with pytest.raises(omb.OmbError, match="non-finite"):
+        omb.apply_M(1.2, nan, g, np.ones(2 * g.N, complex))
