@@ -1,0 +1,306 @@
+#!/usr/bin/env python
+"""Benchmark: converged modes/s at residual 1e-8 on 256² LiNbO₃ ridge cross-sections.
+
+One *step* is one batched ``solve_k`` over a fixed batch of synthetic cross-sections of the
+x-cut LiNbO₃ ridge family (8×5 μm cell, 256×256 grid, 4 bands, film 0.6 μm, etch 0.3 μm,
+70° sidewalls, top widths {1.0, 1.5, 2.0} μm, ω swept over [1/1.60, 1/1.50] μm⁻¹), solved
+with the batched, mixed-precision, inner-Newton B200 solver.  ``value`` counts converged
+modes (Newton |Δk| < 1e-8 and FP64 residual < 1e-8) per device second with the inputs
+resident (``omb_batch_run``); ``e2e`` is the same metric through ``omb_solve_k`` with host
+buffers (upload, solve, download, phase canonicalisation).  The plain arm (one instance,
+FP64, the reference's band-by-band Newton loop) runs on the same GPU for comparison.
+
+``--impl reference`` times the reference algorithm's CPU restatement (the FP64 oracle,
+NumPy/SciPy with every host thread) on the same workload: each step solves one mode.
+
+Launch: ``python bench.py [--gpus 1] [--steps K] [--warmup W]``; for N>1 through
+``torch.distributed.run`` (one rank per GPU, every rank solves its own batch: weak scaling,
+no data-path collective).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "optimode.jl_b200"))
+
+METRIC = "converged modes/s at residual 1e-8, 256² grid: batched+warm-start vs plain"
+UNIT = "modes/s"
+NX = NY = 256
+DX, DY = 8.0, 5.0
+NEV = 4
+WIDTHS = (1.0, 1.5, 2.0)
+FALLBACK_HBM_GBS = 6650.0
+
+
+def workload(n_inst: int, seed: int = 0):
+    from omb200 import Grid
+    from omb200 import geometry as G
+    g = Grid(DX, DY, NX, NY)
+    n_w = len(WIDTHS)
+    n_om = max(1, (n_inst + n_w - 1) // n_w)
+    omegas = np.linspace(1 / 1.60, 1 / 1.50, n_om)
+    eps = {w: G.ln_ridge(g, top_width=w) for w in WIDTHS}
+    probs = []
+    for i in range(n_inst):
+        w = WIDTHS[i % n_w]
+        om = omegas[(i // n_w) % n_om]
+        probs.append({"omega": float(om), "eps_inv": eps[w], "grid": g, "nev": NEV})
+    return g, probs
+
+
+def sample_clocks(stop: threading.Event, out: list, index: int):
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    while not stop.is_set():
+        try:
+            r = subprocess.run(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                "-i", str(index)], capture_output=True, text=True, timeout=5)
+            if r.returncode == 0 and r.stdout.strip():
+                out.append([x.strip() for x in r.stdout.strip().split(",")])
+        except Exception:
+            pass
+        stop.wait(0.2)
+
+
+def clock_summary(samples):
+    if not samples:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+    sm = [float(s[1]) for s in samples if s[1].replace(".", "").isdigit()]
+    mx = [float(s[2]) for s in samples if s[2].replace(".", "").isdigit()]
+    reasons = set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for s in samples:
+        for name, v in zip(names, s[5:9]):
+            if v.strip().lower() == "active":
+                reasons.add(name)
+    return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+            "reasons": sorted(reasons), "samples": len(samples)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per operator apply from the committed ncu summary (null if absent)."""
+    p = os.path.join(ROOT, "profiles", "operator_apply_256x256_fp32.md")
+    try:
+        m = re.search(r"traffic_bytes_per_apply:\s*([0-9.eE+]+)", open(p).read())
+        return float(m.group(1)) if m else None
+    except Exception:
+        return None
+
+
+def cpu_baseline(seconds_budget: float):
+    """FP64 oracle (the reference algorithm restated in NumPy/SciPy) on one mode of the
+    workload: band 0 of the 1.5 μm ridge at ω = 1/1.55, all host threads for the FFTs."""
+    sys.path.insert(0, ROOT)
+    import oracle as O
+    from omb200 import geometry as G
+    from omb200 import Grid
+    g = Grid(DX, DY, NX, NY)
+    ei = G.ln_ridge(g, top_width=1.5)
+    cores = os.cpu_count() or 1
+    O.maxwell.FFT_WORKERS = cores
+    t0 = time.perf_counter()
+    O.solve_k(1 / 1.55, ei, O.Grid(DX, DY, NX, NY), nev=1)
+    dt = time.perf_counter() - t0
+    return {"value": 1.0 / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"1 converged mode (band 0, 1.5 um ridge, omega=1/1.55, 256^2) in {dt:.1f} s"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    sys.path.insert(0, ROOT)
+    import oracle as O
+    from omb200 import Grid
+    g, probs = workload(max(args.instances, 1))
+    cores = os.cpu_count() or 1
+    O.maxwell.FFT_WORKERS = cores
+    og = O.Grid(DX, DY, NX, NY)
+
+    def step(i):
+        pr = probs[i % len(probs)]
+        O.solve_k(pr["omega"], pr["eps_inv"], og, nev=1)
+
+    for i in range(args.warmup):
+        step(i)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        step(args.warmup + i)
+    dt = time.perf_counter() - t0
+    v = args.steps / dt
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded LiNbO3 ridge cross-sections, Kottke-smoothed)",
+        "config": {"workload": "LiNbO3 ridge 8x5um 256x256, band 0 per step (one converged mode)",
+                   "grid": [NX, NY], "nev": 1},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} modes, one per step, scipy.fft workers={cores}"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--instances", type=int, default=12)
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    import omb200
+    solver = omb200.B200Solver(precision="mixed", preconditioner="mpb", newton="inner", device=local)
+    g, probs = workload(args.instances, seed=rank)
+    batch = omb200.Batch(probs, solver)
+
+    def barrier():
+        torch.cuda.synchronize(local)
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        batch.run()
+    barrier()
+    stop = threading.Event()
+    samples: list = []
+    th = threading.Thread(target=sample_clocks, args=(stop, samples, local), daemon=True)
+    th.start()
+    dev_s = 0.0
+    kernels = 0
+    for _ in range(args.steps):
+        batch.run()
+        st = batch.stats()
+        dev_s += st["run_seconds"]
+        kernels += st["kernel_launches"]
+    barrier()
+    stop.set()
+    th.join(timeout=5)
+    res, info = batch.results(return_info=True, raise_on_failure=False)
+    converged = int(sum(int(np.sum(i["status"] == 0)) for i in info))
+    max_dev_s = dev_s
+    if dist is not None:
+        t = torch.tensor([dev_s], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        max_dev_s = float(t.item())
+        c = torch.tensor([converged], device=f"cuda:{local}")
+        dist.all_reduce(c, op=dist.ReduceOp.SUM)
+        converged_all = int(c.item())
+    else:
+        converged_all = converged
+    value = converged_all * args.steps / max_dev_s
+    batch.close()
+
+    # end to end through the public C ABI call with host buffers
+    e2e_s = 0.0
+    for _ in range(args.e2e_steps):
+        barrier()
+        t0 = time.perf_counter()
+        omb200.solve_k_batch(probs, solver, raise_on_failure=False)
+        torch.cuda.synchronize(local)
+        e2e_s += time.perf_counter() - t0
+    # byte counts of one end-to-end step from a staged run of the same batch
+    b4 = omb200.Batch(probs, solver)
+    b4.run()
+    b4.results(raise_on_failure=False)
+    st4 = b4.stats()
+    h2d, d2h = st4["h2d_bytes"], st4["d2h_bytes"]
+    b4.close()
+    e2e_val = converged * args.e2e_steps / e2e_s
+    if dist is not None:
+        t = torch.tensor([e2e_s], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_val = converged_all * args.e2e_steps / float(t.item())
+
+    out = None
+    if rank == 0:
+        # roofline of the fused operator apply (3 passes) on the bench grid, 4 columns per
+        # cell, 64 cells (≈1.3 GB resident, far above L2)
+        N = NX * NY
+        ncol, nbatch = NEV, 64
+        t_apply = omb200.profile_apply("M", 1.3, probs[0]["eps_inv"], g, ncol, nbatch, reps=20,
+                                       precision="fp32", device=local)
+        alg = (32 * N * ncol + 24 * N) * nbatch
+        peak, peak_kind = measured_peak_hbm()
+        achieved = alg / t_apply / 1e9
+        traffic = profiled_traffic()
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "traffic": traffic,
+                    "kernel": "operator apply M(k) (row_in + col + row_out, FP32), 4 columns x 64 cells",
+                    "algorithmic_bytes_per_launch": alg, "seconds_per_launch": t_apply,
+                    "peak_source": peak_kind}
+        plain = None
+        if not args.no_plain:
+            ps = omb200.B200Solver(precision="fp64", preconditioner="mpb", newton="outer", device=local)
+            pb = omb200.Batch(probs[:1], ps)
+            pb.run()
+            pst = pb.stats()
+            _, pinfo = pb.results(return_info=True, raise_on_failure=False)
+            pconv = int(np.sum(pinfo[0]["status"] == 0))
+            plain = {"value": pconv / pst["run_seconds"], "unit": UNIT,
+                     "what": "one instance, FP64, reference band-by-band Newton loop, same kernels",
+                     "seconds": pst["run_seconds"], "converged": pconv}
+            pb.close()
+        cpu = None if args.no_cpu_baseline or world > 1 else cpu_baseline(30.0)
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * max_dev_s / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32+fp64",
+            "data": "synthetic (seeded LiNbO3 ridge cross-sections, Kottke-smoothed eps)",
+            "config": {"workload": f"x-cut LiNbO3 ridge, 8x5 um cell, {NX}x{NY}, {NEV} bands, "
+                                   f"{len(probs)} instances per GPU (widths {list(WIDTHS)} x omega)",
+                       "instances_per_gpu": len(probs), "nev": NEV, "grid": [NX, NY],
+                       "precision": "mixed (FP32 iterations, FP64 polish)", "tol": 1e-8, "k_tol": 1e-8,
+                       "l2": "working set per step is GBs (inputs larger than L2)",
+                       "parallelism": f"instances sharded, {world} rank(s)"},
+            "converged_modes_per_step": converged_all, "modes_per_step": len(probs) * NEV * world,
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(kernels),
+            "roofline": roofline,
+            "plain_fp64_single": plain,
+            "cpu_baseline": cpu,
+            "clocks": clock_summary(samples),
+        }
+        print(json.dumps(out), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -87,6 +87,110 @@ int omb_HMkH(omb_ctx* ctx, int precision, const omb_grid* grid, double k,
 int omb_efield(omb_ctx* ctx, int precision, const omb_grid* grid, double k,
                const double* epsinv, const double* H, double* E);
 
+/* ---------------------------------------------------------------------------------
+ * Eigensolves
+ * --------------------------------------------------------------------------------- */
+
+/* Newton strategy for solve_k */
+#define OMB_NEWTON_INNER 0 /* Newton steps inside the eigensolver iteration (default)     */
+#define OMB_NEWTON_OUTER 1 /* the reference loop: bands one after another, a full block
+                              eigensolve per Newton step (the plain baseline)            */
+
+typedef struct {
+  double k_tol;           /* Newton tolerance on |Δk|                       (1e-8) */
+  double eig_tol;         /* residual ‖M̂h − ω²h‖ of a unit eigenvector       (1e-8) */
+  int32_t max_eigsolves;  /* Newton steps per band                            (60)   */
+  int32_t maxiter;        /* eigensolver iterations per band and phase        (300)  */
+  int32_t precision;      /* OMB_PREC_MIXED / OMB_PREC_FP64 / OMB_PREC_FP32   (MIXED)*/
+  int32_t preconditioner; /* OMB_OP_P (MPB-style) or OMB_OP_P_DIAG           (P)    */
+  int32_t newton;         /* OMB_NEWTON_INNER or OMB_NEWTON_OUTER             (INNER)*/
+  int32_t canonicalize;   /* 1: rotate each eigenvector so the largest E component is
+                             real and positive (fields.jl:258-260)           (1)    */
+  uint64_t seed;          /* random start blocks                              (0)    */
+} omb_options;
+
+/* One solve_k problem: the lowest `nev` guided modes of one cell at frequency ω. */
+typedef struct {
+  omb_grid grid;
+  double omega;            /* ω = 1/λ (μm⁻¹)                                         */
+  const double* epsinv;    /* (3, 3, Nx, Ny) Float64                                 */
+  int32_t nev;             /* bands (≤ 10)                                           */
+  double kguess;           /* Newton start; ≤ 0 → k_guess(ω, ε⁻¹) = ω/√(min diag ε⁻¹) */
+  const double* Hguess;    /* NULL or `nguess` warm-start columns (2, Nx, Ny)        */
+  int32_t nguess;
+} omb_instance;
+
+/* Caller-owned outputs of one instance; any pointer but kmags may be NULL. */
+typedef struct {
+  double* kmags;           /* nev                                                    */
+  double* evecs;           /* nev columns ComplexF64 (2, Nx, Ny): 4·Nx·Ny·nev doubles */
+  double* residuals;       /* nev: ‖M̂h − λh‖ at the last eigensolve                 */
+  double* dw2dk;           /* nev: ∂ω²/∂k = 2⟨h|∂M̂/∂k|h⟩ (group index n_g = 2ω/dw2dk) */
+  int32_t* status;         /* nev: OMB_OK or the band's error code                   */
+  int32_t* iterations;     /* nev: eigensolver iterations                            */
+  int32_t* newton_steps;   /* nev                                                    */
+} omb_result;
+
+/* Fill `opt` with the defaults shown above. */
+int omb_options_default(omb_options* opt);
+
+/* Solve `n_inst` independent problems in one batched device run.
+ * Replaces solve_k(ω, ε⁻¹, grid, solver; nev, max_eigsolves, maxiter, k_tol, eig_tol,
+ * kguess, Hguess) (lib/MaxwellEigenmodes/src/solve.jl:182-196; the GPU backend
+ * src/solvers/gpu.jl:213-242).  kmags[b] is the band-b propagation constant after the
+ * final Newton update; evecs are unit-norm and phase-canonicalised.  Returns OMB_OK when
+ * every band converged, else OMB_ERR_NOT_CONVERGED (results are still written, per-band
+ * status says which), or another error code. */
+int omb_solve_k(omb_ctx* ctx, const omb_instance* inst, int n_inst, const omb_options* opt,
+                omb_result* out);
+
+/* Lowest `nev` eigenpairs (ω², h) of M̂(k) for one cell.
+ * Replaces solve_ω²(ms, solver; nev, maxiter, tol) (src/solve.jl:38-63) and
+ * solve_ω²(ms, ::GPUSolver) (src/solvers/gpu.jl:201-211).  evecs may be NULL; Hguess is
+ * NULL or `nguess` warm-start columns. */
+int omb_solve_omega2(omb_ctx* ctx, const omb_grid* grid, double k, const double* epsinv, int nev,
+                     const double* Hguess, int nguess, const omb_options* opt, double* evals,
+                     double* evecs, double* residuals, int32_t* status);
+
+/* ---------------------------------------------------------------------------------
+ * Staged batches: the same solve as omb_solve_k split into its host→device, device and
+ * device→host parts, so the device part can run (and be timed) with its inputs resident.
+ * omb_solve_k(...) ≡ create + run + results + destroy.  No reference counterpart: the
+ * reference has no batch call (its callers loop over solve_k).
+ * --------------------------------------------------------------------------------- */
+
+typedef struct omb_batch omb_batch;
+
+typedef struct {
+  int64_t graph_launches;  /* CUDA graph replays (two eigensolver iterations each)      */
+  int64_t kernel_launches; /* library kernels launched (graph nodes counted per replay) */
+  int64_t h2d_bytes;       /* host→device bytes of the inputs                           */
+  int64_t d2h_bytes;       /* device→host bytes of the results                          */
+  int32_t tracks;          /* Newton/eigensolve units                                   */
+  int32_t max_iterations;  /* largest iteration count of any unit                      */
+  double run_seconds;      /* device time of the last omb_batch_run (CUDA events)       */
+} omb_stats;
+
+/* Validate and upload `n_inst` problems (ε⁻¹ and any warm starts are copied). */
+int omb_batch_create(omb_ctx* ctx, const omb_instance* inst, int n_inst, const omb_options* opt,
+                     omb_batch** out);
+/* Run the whole solve on the device (may be called again; each run starts afresh). */
+int omb_batch_run(omb_batch* b);
+/* Copy instance results to the caller's buffers (canonicalising if requested).  Returns
+ * OMB_OK or OMB_ERR_NOT_CONVERGED like omb_solve_k. */
+int omb_batch_results(omb_batch* b, omb_result* out);
+int omb_batch_stats(const omb_batch* b, omb_stats* out);
+int omb_batch_destroy(omb_batch* b);
+
+/* Mean device seconds of one application of `op` to `ncol` columns on each of `nbatch`
+ * copies of the cell, over `reps` back-to-back applications on device-resident data
+ * (CUDA events on the library's stream, after 3 warm-up applications).  The inputs
+ * (nbatch·ncol columns plus ε⁻¹ per copy) are allocated once, so choose nbatch to exceed
+ * the 126 MB L2 when timing against HBM bandwidth.  No reference counterpart
+ * (measurement support). */
+int omb_profile_apply(omb_ctx* ctx, int op, int precision, const omb_grid* grid, double k,
+                      const double* epsinv, int ncol, int nbatch, int reps, double* seconds);
+
 #ifdef __cplusplus
 }
 #endif

@@ -3,6 +3,7 @@
 #include <vector>
 
 #include "context.h"
+#include "lobpcg.cuh"
 #include "vec.cuh"
 
 namespace omb {
@@ -144,6 +145,66 @@ static int run_efield(omb_ctx* ctx, const Problem& P, double k, const double* H,
   return OMB_OK;
 }
 
+template <typename T>
+static int run_profile(omb_ctx* ctx, int op, const Problem& P, double k, int ncol, int nbatch, int reps,
+                       double* seconds) {
+  const size_t N = P.N(), n2 = 2 * N;
+  cudaStream_t st = ctx->stream;
+  // nbatch private copies of the cell's ε⁻¹ so every copy streams its own tensor from HBM
+  DevBuf<float4> a32;
+  DevBuf<float2> b32;
+  DevBuf<double2> e64;
+  DevBuf<T> eave;
+  OMB_CU(a32.alloc(N * nbatch, st));
+  OMB_CU(b32.alloc(N * nbatch, st));
+  OMB_CU(e64.alloc(3 * N * nbatch, st));
+  OMB_CU(eave.alloc(N * nbatch, st));
+  const T* eave_src = std::is_same<T, float>::value ? (const T*)P.eave32.p : (const T*)P.eave64.p;
+  for (int c = 0; c < nbatch; ++c) {
+    OMB_CU(cudaMemcpyAsync(a32.p + c * N, P.e32a.p, N * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+    OMB_CU(cudaMemcpyAsync(b32.p + c * N, P.e32b.p, N * sizeof(float2), cudaMemcpyDeviceToDevice, st));
+    OMB_CU(cudaMemcpyAsync(e64.p + 3 * c * N, P.e64.p, 3 * N * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+    OMB_CU(cudaMemcpyAsync(eave.p + c * N, eave_src, N * sizeof(T), cudaMemcpyDeviceToDevice, st));
+  }
+  DevBuf<cplx<T>> hin, hout, scr;
+  OMB_CU(hin.alloc(n2 * ncol * nbatch, st));
+  OMB_CU(hout.alloc(n2 * ncol * nbatch, st));
+  OMB_CU(scr.alloc(3 * N * ncol * nbatch, st));
+  k_random_block<T><<<grid_blocks(n2 * ncol * nbatch), 256, 0, st>>>(hin.p, (long long)n2, ncol * nbatch, 99);
+  OMB_CU(cudaGetLastError());
+  DevBuf<double> kd;
+  OMB_CU(kd.alloc(1, st));
+  OMB_CU(cudaMemcpyAsync(kd.p, &k, sizeof(double), cudaMemcpyHostToDevice, st));
+  std::vector<OpUnit<T>> units(nbatch);
+  for (int c = 0; c < nbatch; ++c) {
+    OpUnit<T> u = make_unit<T>(P);
+    u.e32a = a32.p + c * N; u.e32b = b32.p + c * N; u.e64 = e64.p + 3 * c * N; u.eave = eave.p + c * N;
+    u.in = hin.p + c * n2 * ncol; u.out = hout.p + c * n2 * ncol; u.scr = scr.p + c * 3 * N * ncol;
+    u.k_dev = kd.p;
+    u.in_cs = u.out_cs = (long long)n2; u.scr_cs = (long long)(3 * N); u.ncol = ncol;
+    units[c] = u;
+  }
+  DevBuf<OpUnit<T>> du;
+  OMB_CU(du.alloc(nbatch, st));
+  OMB_CU(cudaMemcpyAsync(du.p, units.data(), nbatch * sizeof(OpUnit<T>), cudaMemcpyHostToDevice, st));
+  const OpKind kind = op == OMB_OP_M ? OP_M : OP_P;
+  for (int w = 0; w < 3; ++w) OMB_CU(launch_op<T>(kind, du.p, nbatch, P.Nx, P.Ny, ncol, ctx->tw, st));
+  cudaEvent_t e0, e1;
+  OMB_CU(cudaEventCreate(&e0));
+  OMB_CU(cudaEventCreate(&e1));
+  OMB_CU(cudaStreamSynchronize(st));
+  OMB_CU(cudaEventRecord(e0, st));
+  for (int r = 0; r < reps; ++r) OMB_CU(launch_op<T>(kind, du.p, nbatch, P.Nx, P.Ny, ncol, ctx->tw, st));
+  OMB_CU(cudaEventRecord(e1, st));
+  OMB_CU(cudaEventSynchronize(e1));
+  float ms = 0;
+  OMB_CU(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *seconds = (double)ms * 1e-3 / reps;
+  return OMB_OK;
+}
+
 static int check_common(omb_ctx* ctx, int precision, double k) {
   if (!ctx) return fail(OMB_ERR_INVALID_ARG, "ctx is NULL");
   if (precision != OMB_PREC_FP32 && precision != OMB_PREC_FP64)
@@ -182,6 +243,20 @@ int omb_HMkH(omb_ctx* ctx, int precision, const omb_grid* grid, double k, const 
   if (rc) return rc;
   return precision == OMB_PREC_FP64 ? run_hmkh<double>(ctx, P, k, ncol, H, out)
                                     : run_hmkh<float>(ctx, P, k, ncol, H, out);
+}
+
+int omb_profile_apply(omb_ctx* ctx, int op, int precision, const omb_grid* grid, double k,
+                      const double* epsinv, int ncol, int nbatch, int reps, double* seconds) {
+  int rc = check_common(ctx, precision, k);
+  if (rc) return rc;
+  if (op != OMB_OP_M && op != OMB_OP_P) return fail(OMB_ERR_INVALID_ARG, "op must be OMB_OP_M or OMB_OP_P");
+  if (ncol <= 0 || nbatch <= 0 || reps <= 0 || !seconds)
+    return fail(OMB_ERR_INVALID_ARG, "need ncol, nbatch, reps > 0 and non-NULL seconds");
+  Problem P;
+  rc = upload_problem(ctx, grid, epsinv, P);
+  if (rc) return rc;
+  return precision == OMB_PREC_FP64 ? run_profile<double>(ctx, op, P, k, ncol, nbatch, reps, seconds)
+                                    : run_profile<float>(ctx, op, P, k, ncol, nbatch, reps, seconds);
 }
 
 int omb_efield(omb_ctx* ctx, int precision, const omb_grid* grid, double k, const double* epsinv,

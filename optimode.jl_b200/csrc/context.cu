@@ -1,6 +1,8 @@
 // Context lifetime, error reporting, twiddle tables and ε⁻¹ upload.
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "context.h"
@@ -30,6 +32,19 @@ bool fft_size_supported(int L) {
   }
 }
 
+cudaError_t ensure_smem(const void* func, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& have = done[{func, dev}];
+  if (have >= bytes) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) have = bytes;
+  return e;
+}
+
 int row_blocks(int Nx, int Ny) {
   const int rows = rows_for(Nx);
   return (Ny + rows - 1) / rows;
@@ -56,7 +71,7 @@ int upload_problem(omb_ctx* ctx, const omb_grid* g, const double* epsinv, Proble
   std::vector<double2> e64(3 * N);
   std::vector<float> ea32(N);
   std::vector<double> ea64(N);
-  double emax = 0, mind = INFINITY, mean = 0;
+  double emax = 0, mind = INFINITY, mean = 0, maxtr = 0;
   for (size_t p = 0; p < 9 * N; ++p) {
     const double v = epsinv[p];
     if (!std::isfinite(v)) return fail(OMB_ERR_NAN, "epsinv holds a non-finite value");
@@ -73,6 +88,7 @@ int upload_problem(omb_ctx* ctx, const omb_grid* g, const double* epsinv, Proble
     const double tr = xx + yy + zz;
     if (!(tr > 0)) return fail(OMB_ERR_INVALID_ARG, "epsinv has a non-positive trace at pixel " + std::to_string(p));
     mind = std::fmin(mind, std::fmin(xx, std::fmin(yy, zz)));
+    maxtr = std::fmax(maxtr, tr);
     a32[p] = make_float4((float)xx, (float)yy, (float)zz, (float)xy);
     b32[p] = make_float2((float)xz, (float)yz);
     e64[3 * p] = make_double2(xx, yy);
@@ -85,6 +101,7 @@ int upload_problem(omb_ctx* ctx, const omb_grid* g, const double* epsinv, Proble
   if (!(mind > 0)) return fail(OMB_ERR_INVALID_ARG, "epsinv has a non-positive diagonal entry");
   P.eps_mean = mean / (double)N;
   P.min_diag = mind;
+  P.max_trace = maxtr;
   cudaStream_t st = ctx->stream;
   OMB_CU(P.e32a.alloc(N, st));
   OMB_CU(P.e32b.alloc(N, st));

@@ -65,6 +65,7 @@ struct Problem {
   double Dx = 0, Dy = 0;
   double eps_mean = 0;  // cell mean of ε_ave (diagonal preconditioner scale)
   double min_diag = 0;  // min over pixels and a of ε⁻¹[a,a] (k_guess)
+  double max_trace = 0; // max over pixels of tr ε⁻¹ (bounds the largest eigenvalue of ε⁻¹)
   DevBuf<float4> e32a;
   DevBuf<float2> e32b;
   DevBuf<double2> e64;

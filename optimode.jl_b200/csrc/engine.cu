@@ -1,0 +1,497 @@
+// Batched device LOBPCG/Newton engine: buffer management, graph capture, phase loop.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "engine.h"
+#include "vec.cuh"
+
+namespace omb {
+
+static int blocks_for(size_t n, int nt = 256) {
+  size_t b = (n + nt - 1) / nt;
+  return (int)std::max<size_t>(1, std::min<size_t>(b, 65535 * 4));
+}
+
+template <typename K> static cudaError_t set_smem(K kern, size_t bytes) {
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  return ensure_smem(reinterpret_cast<const void*>(kern), bytes);
+}
+
+Engine::Engine(omb_ctx* ctx, std::vector<Problem>* problems, std::vector<TrackSpec> tracks, SolveOptions opt)
+    : ctx_(ctx), probs_(problems), tracks_(std::move(tracks)), opt_(opt) {
+  nt_ = (int)tracks_.size();
+  order_.resize(nt_);
+  for (int i = 0; i < nt_; ++i) order_[i] = i;
+  std::stable_sort(order_.begin(), order_.end(), [&](int a, int b) {
+    const Problem& pa = (*probs_)[tracks_[a].prob];
+    const Problem& pb = (*probs_)[tracks_[b].prob];
+    return std::make_pair(pa.Nx, pa.Ny) < std::make_pair(pb.Nx, pb.Ny);
+  });
+  for (int i = 0; i < nt_;) {
+    const Problem& p = (*probs_)[tracks_[order_[i]].prob];
+    Group g{i, 0, p.Nx, p.Ny, 0};
+    while (i < nt_) {
+      const Problem& q = (*probs_)[tracks_[order_[i]].prob];
+      if (q.Nx != p.Nx || q.Ny != p.Ny) break;
+      g.Mmax = std::max(g.Mmax, tracks_[order_[i]].M);
+      ++g.n;
+      ++i;
+    }
+    groups_.push_back(g);
+  }
+  const int target = 4 * std::max(ctx_->num_sms, 1);
+  gram_chunks_ = std::max(4, std::min(32, (target + nt_ - 1) / std::max(nt_, 1)));
+  upd_chunks_ = std::max(4, std::min(256, (2 * target + nt_ - 1) / std::max(nt_, 1)));
+}
+
+Engine::~Engine() { cudaStreamSynchronize(ctx_->stream); }
+
+int Engine::upload_states() {
+  OMB_CU(cudaMemcpyAsync(d_states_.p, host_states_.data(), nt_ * sizeof(TrackState), cudaMemcpyHostToDevice,
+                         ctx_->stream));
+  OMB_CU(cudaStreamSynchronize(ctx_->stream));
+  return OMB_OK;
+}
+int Engine::download_states() {
+  OMB_CU(cudaMemcpyAsync(host_states_.data(), d_states_.p, nt_ * sizeof(TrackState), cudaMemcpyDeviceToHost,
+                         ctx_->stream));
+  OMB_CU(cudaStreamSynchronize(ctx_->stream));
+  return OMB_OK;
+}
+
+// Fill X (columns 0..M-1 of Y[0]) for the first phase: random, then the caller's guesses.
+template <typename T> int Engine::init_block(int phase) {
+  cudaStream_t st = ctx_->stream;
+  DevBuf<cplx<T>>& Y = std::is_same<T, float>::value ? reinterpret_cast<DevBuf<cplx<T>>&>(y32_)
+                                                      : reinterpret_cast<DevBuf<cplx<T>>&>(y64_);
+  for (int t = 0; t < nt_; ++t) {
+    const TrackSpec& ts = tracks_[t];
+    const Problem& P = (*probs_)[ts.prob];
+    const long long n2 = 2 * (long long)P.N();
+    cplx<T>* X = Y.p + yoff_[t];
+    if (phase == 0) {
+      k_random_block<T><<<blocks_for(n2 * ts.M), 256, 0, st>>>(X, n2, ts.M, opt_.seed * 1000003ull + 7919ull * t + 1);
+      OMB_CU(cudaGetLastError());
+      const int ng = std::min(ts.nguess, ts.M);
+      if (ng > 0 && ts.guess) {
+        DevBuf<double2> g;
+        OMB_CU(g.alloc(n2 * ng, st));
+        OMB_CU(cudaMemcpyAsync(g.p, ts.guess, n2 * ng * sizeof(double2), cudaMemcpyHostToDevice, st));
+        if constexpr (std::is_same<T, double>::value) {
+          OMB_CU(cudaMemcpyAsync(X, g.p, n2 * ng * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+        } else {
+          k_c64_to_c32<<<blocks_for(n2 * ng), 256, 0, st>>>(g.p, X, n2 * ng);
+          OMB_CU(cudaGetLastError());
+        }
+        OMB_CU(cudaStreamSynchronize(st));
+      }
+    } else {
+      // previous phase ran in FP32: promote its X
+      if constexpr (std::is_same<T, double>::value) {
+        const size_t src = yoff_[t] + (size_t)host_states_[t].cur_par * 3 * ts.M * n2;
+        k_c32_to_c64<<<blocks_for(n2 * ts.M), 256, 0, st>>>(y32_.p + src, X, n2 * ts.M);
+        OMB_CU(cudaGetLastError());
+      }
+    }
+  }
+  return OMB_OK;
+}
+
+template <typename T>
+int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool reuse) {
+  cudaStream_t st = ctx_->stream;
+  DevBuf<cplx<T>>& Y = std::is_same<T, float>::value ? reinterpret_cast<DevBuf<cplx<T>>&>(y32_)
+                                                      : reinterpret_cast<DevBuf<cplx<T>>&>(y64_);
+  DevBuf<cplx<T>>& Sc = std::is_same<T, float>::value ? reinterpret_cast<DevBuf<cplx<T>>&>(s32_)
+                                                       : reinterpret_cast<DevBuf<cplx<T>>&>(s64_);
+  int rc = OMB_OK;
+  if (!reuse) {
+    // ---- buffers: per track Y[2], AY[2] (3M columns each) and the operator scratch
+    yoff_.assign(nt_, 0);
+    soff_.assign(nt_, 0);
+    size_t ytot = 0, stot = 0;
+    for (int t = 0; t < nt_; ++t) {
+      const Problem& P = (*probs_)[tracks_[t].prob];
+      const size_t n2 = 2 * P.N();
+      yoff_[t] = ytot;
+      ytot += 12 * (size_t)tracks_[t].M * n2;
+      soff_[t] = stot;
+      stot += 2 * (size_t)tracks_[t].M * 3 * P.N();
+    }
+    OMB_CU(Y.alloc(ytot, st));
+    OMB_CU(Sc.alloc(stot, st));
+    rc = init_block<T>(phase);
+    if (rc) return rc;
+    if (phase > 0 && std::is_same<T, double>::value) y32_.release(), s32_.release();
+  } else {
+    // continue from the current block: bring it to parity 0
+    for (int t = 0; t < nt_; ++t) {
+      if (host_states_[t].cur_par == 0) continue;
+      const size_t n2 = 2 * (*probs_)[tracks_[t].prob].N();
+      const size_t M = tracks_[t].M;
+      OMB_CU(cudaMemcpyAsync(Y.p + yoff_[t], Y.p + yoff_[t] + 3 * M * n2, M * n2 * sizeof(cplx<T>),
+                             cudaMemcpyDeviceToDevice, st));
+    }
+  }
+
+  // ---- per-phase state
+  for (int t = 0; t < nt_; ++t) {
+    TrackState& s = host_states_[t];
+    s.band = tracks_[t].band + round_;
+    s.done = (round_ < tracks_[t].nbands) ? 0 : 1;
+    s.status = s.done ? s.status : TS_RUNNING;
+    s.nlocked = 0; s.nWa = 0; s.nP = 0; s.nP_next = 0;
+    s.op_col0 = 0; s.op_ncol = s.M; s.pw_col0 = 0; s.pw_ncol = 0; s.hmkh_ncol = 0;
+    s.iter_phase = 0; s.newton_phase = 0; s.since_newton = 0; s.stall = 0; s.resid_best = 1e300;
+    s.phase = phase;
+    s.cur_par = 0;
+  }
+  rc = upload_states();
+  if (rc) return rc;
+
+  // ---- descriptors
+  std::vector<TrackDesc<T>> descs(nt_);
+  std::vector<OpUnit<T>> uA[2], uP[2], uH[2];
+  for (int par = 0; par < 2; ++par) { uA[par].resize(nt_); uP[par].resize(nt_); uH[par].resize(nt_); }
+  for (int t = 0; t < nt_; ++t) {
+    const TrackSpec& ts = tracks_[t];
+    const Problem& P = (*probs_)[ts.prob];
+    const long long n2 = 2 * (long long)P.N();
+    const int M = ts.M;
+    TrackDesc<T>& d = descs[t];
+    cplx<T>* base = Y.p + yoff_[t];
+    d.Y[0] = base;
+    d.Y[1] = base + 3 * M * n2;
+    d.AY[0] = base + 6 * M * n2;
+    d.AY[1] = base + 9 * M * n2;
+    d.st = d_states_.p + t;
+    d.coef = coef_.p + (size_t)t * 2 * NMAX * MMAX;
+    d.gram_part = gram_part_.p + (size_t)t * 32 * 2 * NMAX * NMAX;
+    d.res_part = res_part_.p + (size_t)t * 256 * MMAX;
+    d.hmkh_part = hmkh_part_.p + (size_t)t * 2 * 512;
+    d.n2 = n2; d.Nx = P.Nx; d.Ny = P.Ny; d.M = M;
+    d.hmkh_nb = row_blocks(P.Nx, P.Ny);
+    d.inv_dx = 1.0 / P.Dx; d.inv_dy = 1.0 / P.Dy; d.eps_mean = P.eps_mean;
+  }
+  for (int gi = 0; gi < nt_; ++gi) {
+    const int t = order_[gi];
+    const TrackSpec& ts = tracks_[t];
+    const Problem& P = (*probs_)[ts.prob];
+    const long long n2 = 2 * (long long)P.N();
+    const int M = ts.M;
+    for (int par = 0; par < 2; ++par) {
+      OpUnit<T> u = make_unit<T>(P);
+      u.k_dev = &d_states_.p[t].k;
+      u.scr = Sc.p + soff_[t];
+      u.scr_cs = 3 * (long long)P.N();
+      u.in_cs = u.out_cs = n2;
+      // A pass over [X | W] of this parity
+      OpUnit<T> a = u;
+      a.in = descs[t].Y[par];
+      a.out = descs[t].AY[par];
+      a.ncol_dev = &d_states_.p[t].op_ncol;
+      a.col0_dev = &d_states_.p[t].op_col0;
+      uA[par][gi] = a;
+      // MPB preconditioner in place on the W slot
+      OpUnit<T> p = u;
+      p.in = descs[t].Y[par] + M * n2;
+      p.out = const_cast<cplx<T>*>(p.in);
+      p.ncol_dev = &d_states_.p[t].pw_ncol;
+      p.col0_dev = &d_states_.p[t].pw_col0;
+      uP[par][gi] = p;
+      // ⟨x_b|∂M̂/∂k|x_b⟩ on the Newton band
+      OpUnit<T> h = u;
+      h.in = descs[t].Y[par] + (long long)(ts.band + round_) * n2;
+      h.ncol_dev = &d_states_.p[t].hmkh_ncol;
+      h.partial = descs[t].hmkh_part;
+      uH[par][gi] = h;
+    }
+  }
+  DevBuf<TrackDesc<T>> d_descs;
+  DevBuf<OpUnit<T>> d_uA[2], d_uP[2], d_uH[2];
+  OMB_CU(d_descs.alloc(nt_, st));
+  OMB_CU(cudaMemcpyAsync(d_descs.p, descs.data(), nt_ * sizeof(TrackDesc<T>), cudaMemcpyHostToDevice, st));
+  for (int par = 0; par < 2; ++par) {
+    OMB_CU(d_uA[par].alloc(nt_, st));
+    OMB_CU(d_uP[par].alloc(nt_, st));
+    OMB_CU(d_uH[par].alloc(nt_, st));
+    OMB_CU(cudaMemcpyAsync(d_uA[par].p, uA[par].data(), nt_ * sizeof(OpUnit<T>), cudaMemcpyHostToDevice, st));
+    OMB_CU(cudaMemcpyAsync(d_uP[par].p, uP[par].data(), nt_ * sizeof(OpUnit<T>), cudaMemcpyHostToDevice, st));
+    OMB_CU(cudaMemcpyAsync(d_uH[par].p, uH[par].data(), nt_ * sizeof(OpUnit<T>), cudaMemcpyHostToDevice, st));
+  }
+  OMB_CU(cudaStreamSynchronize(st));
+
+  IterParams prm{};
+  prm.tol = opt_.tol;
+  prm.k_tol = opt_.k_tol;
+  prm.lock_tol = lock_tol;
+  prm.tau_phase = tau;
+  prm.dk_phase = 1e-6;
+  prm.gram_drop = std::is_same<T, float>::value ? 1e-6 : 1e-12;
+  prm.maxiter = opt_.maxiter;
+  prm.max_newton = opt_.max_newton;
+  prm.last_phase = last ? 1 : 0;
+  prm.prec_diag = opt_.prec_diag ? 1 : 0;
+  prm.gram_chunks = gram_chunks_;
+  prm.upd_chunks = upd_chunks_;
+
+  int Mmax = 1;
+  for (const auto& ts : tracks_) Mmax = std::max(Mmax, ts.M);
+  const int nmax = 3 * Mmax;
+  const size_t sm_gram = 2 * (size_t)nmax * GRAM_ROWS * sizeof(cplx<T>);
+  const size_t sm_upd = 2 * (size_t)nmax * UPD_ROWS * sizeof(cplx<T>) + 2 * (size_t)nmax * MMAX * sizeof(cplx<T>);
+  const size_t sm_rr = 4 * (size_t)NMAX * NMAX * sizeof(double2);
+  OMB_CU(set_smem(k_gram<T>, sm_gram));
+  OMB_CU(set_smem(k_update<T>, sm_upd));
+  OMB_CU(set_smem(k_rr, sm_rr));
+  const int cb = (nt_ + 127) / 128;
+
+  auto iteration = [&](int par) -> cudaError_t {
+    cudaError_t e;
+    if (!opt_.prec_diag)
+      for (const Group& g : groups_)
+        if ((e = launch_op<T>(OP_P, d_uP[par].p + g.off, g.n, g.Nx, g.Ny, g.Mmax, ctx_->tw, st)) != cudaSuccess) return e;
+    for (const Group& g : groups_)
+      if ((e = launch_op<T>(OP_HMKH, d_uH[par].p + g.off, g.n, g.Nx, g.Ny, 1, ctx_->tw, st)) != cudaSuccess) return e;
+    k_newton<<<cb, 128, 0, st>>>(d_state_ptrs_.p, d_hmkh_ptrs_.p, d_hmkh_nb_.p, nt_, prm);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    for (const Group& g : groups_)
+      if ((e = launch_op<T>(OP_M, d_uA[par].p + g.off, g.n, g.Nx, g.Ny, 2 * g.Mmax, ctx_->tw, st)) != cudaSuccess) return e;
+    k_gram<T><<<dim3(gram_chunks_, nt_), GRAM_NT, sm_gram, st>>>(d_descs.p, par, gram_chunks_);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_rr<<<nt_, RR_NT, sm_rr, st>>>(d_state_ptrs_.p, d_gram_ptrs_.p, d_coef_ptrs_.p, nt_, prm);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_update<T><<<dim3(upd_chunks_, nt_), UPD_NT, sm_upd, st>>>(d_descs.p, par, upd_chunks_, prm.prec_diag);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_control<<<cb, 128, 0, st>>>(d_state_ptrs_.p, d_res_ptrs_.p, nt_, prm);
+    return cudaGetLastError();
+  };
+
+  // two eager iterations (they also size the kernels' shared memory), then the graph
+  OMB_CU(iteration(0));
+  OMB_CU(iteration(1));
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  OMB_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  cudaError_t ce = iteration(0);
+  if (ce == cudaSuccess) ce = iteration(1);
+  cudaError_t ee = cudaStreamEndCapture(st, &graph);
+  if (ce != cudaSuccess) { if (graph) cudaGraphDestroy(graph); return cuda_fail(ce, "graph capture"); }
+  OMB_CU(ee);
+  OMB_CU(cudaGraphInstantiate(&exec, graph, 0));
+  size_t nodes = 0;
+  OMB_CU(cudaGraphGetNodes(graph, nullptr, &nodes));
+  kernels_ += (int64_t)nodes;  // the two eager iterations
+  // every track ends a phase within maxiter (+2) iterations, per Newton step in the
+  // reference loop; two iterations per graph launch
+  const int per = opt_.maxiter / 2 + 4;
+  const int cap = per * (opt_.newton_mode == MODE_NEWTON_OUTER ? opt_.max_newton + 1 : 1) + 4;
+  int rc_out = OMB_OK;
+  for (int it = 0; it < cap; ++it) {
+    cudaError_t e = cudaGraphLaunch(exec, st);
+    if (e != cudaSuccess) { rc_out = cuda_fail(e, "cudaGraphLaunch"); break; }
+    launches_++;
+    kernels_ += (int64_t)nodes;
+    if ((it & 3) == 3 || it < 4) {
+      rc_out = download_states();
+      if (rc_out) break;
+      bool all = true;
+      for (const TrackState& s : host_states_) all = all && s.done;
+      if (all) break;
+    }
+  }
+  cudaGraphExecDestroy(exec);
+  cudaGraphDestroy(graph);
+  if (rc_out) return rc_out;
+  rc_out = download_states();
+  last_prec_ = std::is_same<T, float>::value ? 0 : 1;
+  return rc_out;
+}
+
+int Engine::run() {
+  cudaStream_t st = ctx_->stream;
+  OMB_CU(cudaSetDevice(ctx_->device));
+  // ---- per-track FP64 state and small buffers
+  host_states_.assign(nt_, TrackState{});
+  double normA = 0;
+  for (int t = 0; t < nt_; ++t) {
+    const TrackSpec& ts = tracks_[t];
+    const Problem& P = (*probs_)[ts.prob];
+    TrackState& s = host_states_[t];
+    std::memset(&s, 0, sizeof(s));
+    s.k = ts.k0; s.k_eig = ts.k0; s.omega2 = ts.omega2;
+    s.M = ts.M; s.band = ts.band; s.need = ts.need; s.mode = ts.mode;
+    s.dk_last = 1e300;
+    const double gx = 0.5 * P.Nx / P.Dx, gy = 0.5 * P.Ny / P.Dy;
+    normA = std::max(normA, (gx * gx + gy * gy + ts.k0 * ts.k0) * P.max_trace);
+  }
+  OMB_CU(d_states_.alloc(nt_, st));
+  OMB_CU(coef_.alloc((size_t)nt_ * 2 * NMAX * MMAX, st));
+  OMB_CU(gram_part_.alloc((size_t)nt_ * 32 * 2 * NMAX * NMAX, st));
+  OMB_CU(res_part_.alloc((size_t)nt_ * 256 * MMAX, st));
+  OMB_CU(hmkh_part_.alloc((size_t)nt_ * 2 * 512, st));
+  OMB_CU(gram_part_.zero());
+  OMB_CU(res_part_.zero());
+  std::vector<TrackState*> sp(nt_);
+  std::vector<double2*> gp(nt_), cp(nt_);
+  std::vector<double*> rp(nt_), hp(nt_);
+  std::vector<int> hnb(nt_);
+  for (int t = 0; t < nt_; ++t) {
+    const Problem& P = (*probs_)[tracks_[t].prob];
+    sp[t] = d_states_.p + t;
+    gp[t] = gram_part_.p + (size_t)t * 32 * 2 * NMAX * NMAX;
+    cp[t] = coef_.p + (size_t)t * 2 * NMAX * MMAX;
+    rp[t] = res_part_.p + (size_t)t * 256 * MMAX;
+    hp[t] = hmkh_part_.p + (size_t)t * 2 * 512;
+    hnb[t] = row_blocks(P.Nx, P.Ny);
+  }
+  OMB_CU(d_state_ptrs_.alloc(nt_, st));
+  OMB_CU(d_gram_ptrs_.alloc(nt_, st));
+  OMB_CU(d_coef_ptrs_.alloc(nt_, st));
+  OMB_CU(d_res_ptrs_.alloc(nt_, st));
+  OMB_CU(d_hmkh_ptrs_.alloc(nt_, st));
+  OMB_CU(d_hmkh_nb_.alloc(nt_, st));
+  OMB_CU(cudaMemcpyAsync(d_state_ptrs_.p, sp.data(), nt_ * sizeof(void*), cudaMemcpyHostToDevice, st));
+  OMB_CU(cudaMemcpyAsync(d_gram_ptrs_.p, gp.data(), nt_ * sizeof(void*), cudaMemcpyHostToDevice, st));
+  OMB_CU(cudaMemcpyAsync(d_coef_ptrs_.p, cp.data(), nt_ * sizeof(void*), cudaMemcpyHostToDevice, st));
+  OMB_CU(cudaMemcpyAsync(d_res_ptrs_.p, rp.data(), nt_ * sizeof(void*), cudaMemcpyHostToDevice, st));
+  OMB_CU(cudaMemcpyAsync(d_hmkh_ptrs_.p, hp.data(), nt_ * sizeof(void*), cudaMemcpyHostToDevice, st));
+  OMB_CU(cudaMemcpyAsync(d_hmkh_nb_.p, hnb.data(), nt_ * sizeof(int), cudaMemcpyHostToDevice, st));
+  OMB_CU(cudaStreamSynchronize(st));
+
+  // FP32 noise floor of the residual of a unit vector: ~ ε₃₂·√‖M̂‖ (FFT round-off scales
+  // with the field's norm, the curl epilogue with |k+G|)
+  const double tauA = std::max(opt_.tol, 64.0 * 5.96e-8 * std::sqrt(normA));
+  // result store: one FP64 vector per finished band
+  store_off_.assign(nt_, 0);
+  snaps_.assign(nt_, {});
+  size_t tot = 0;
+  for (int t = 0; t < nt_; ++t) {
+    store_off_[t] = tot;
+    const int nb = tracks_[t].mode == MODE_OMEGA2 ? 1 : tracks_[t].nbands;
+    tot += (size_t)nb * 2 * (*probs_)[tracks_[t].prob].N();
+    snaps_[t].resize(nb);
+  }
+  OMB_CU(store_.alloc(tot, st));
+  round_ = 0;
+  int rc = OMB_OK;
+  if (opt_.precision == OMB_PREC_FP64) {
+    rc = run_phase<double>(0, true, opt_.tol, opt_.tol, false);
+  } else if (opt_.precision == OMB_PREC_FP32) {
+    // tolerances clamped to what FP32 can resolve (the reference clamps to 50·eps(T),
+    // src/solvers/gpu.jl:58)
+    opt_.tol = std::max(opt_.tol, tauA);
+    opt_.k_tol = std::max(opt_.k_tol, 50 * 1.1920929e-7);
+    rc = run_phase<float>(0, true, opt_.tol, opt_.tol, false);
+  } else {
+    rc = run_phase<float>(0, false, tauA, tauA, false);
+    if (!rc) rc = run_phase<double>(1, true, opt_.tol, opt_.tol, false);
+  }
+  if (!rc) rc = snapshot(0);
+  int maxb = 1;
+  for (const auto& ts : tracks_) maxb = std::max(maxb, ts.mode == MODE_NEWTON_OUTER ? ts.nbands : 1);
+  for (round_ = 1; round_ < maxb && !rc; ++round_) {
+    rc = last_prec_ == 1 ? run_phase<double>(2, true, opt_.tol, opt_.tol, true)
+                         : run_phase<float>(2, true, opt_.tol, opt_.tol, true);
+    if (!rc) rc = snapshot(round_);
+  }
+  round_ = 0;
+  return rc;
+}
+
+int Engine::snapshot(int round) {
+  cudaStream_t st = ctx_->stream;
+  int rc = download_states();
+  if (rc) return rc;
+  for (int t = 0; t < nt_; ++t) {
+    const TrackSpec& ts = tracks_[t];
+    const int nb = ts.mode == MODE_OMEGA2 ? 1 : ts.nbands;
+    if (round >= nb) continue;
+    snaps_[t][round] = host_states_[t];
+    if (ts.mode == MODE_OMEGA2) continue;  // solve_ω² reads the block itself
+    const size_t n2 = 2 * (*probs_)[ts.prob].N();
+    double2* dst = store_.p + store_off_[t] + (size_t)round * n2;
+    const size_t src = col_offset(t, ts.band + round);
+    if (last_prec_ == 1) {
+      OMB_CU(cudaMemcpyAsync(dst, y64_.p + src, n2 * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+    } else {
+      k_c32_to_c64<<<blocks_for(n2), 256, 0, st>>>(y32_.p + src, dst, n2);
+      OMB_CU(cudaGetLastError());
+    }
+  }
+  return OMB_OK;
+}
+
+int Engine::max_iterations() const {
+  int m = 0;
+  for (const auto& v : snaps_)
+    for (const auto& s : v) m = std::max(m, s.iter);
+  return m;
+}
+
+size_t Engine::col_offset(int t, int col) const {
+  const Problem& P = (*probs_)[tracks_[t].prob];
+  const size_t n2 = 2 * P.N();
+  return yoff_[t] + ((size_t)host_states_[t].cur_par * 3 * tracks_[t].M + col) * n2;
+}
+
+int Engine::fetch_result(int t, int b, double* out) {
+  const size_t n2 = 2 * (*probs_)[tracks_[t].prob].N();
+  OMB_CU(cudaMemcpyAsync(out, store_.p + store_off_[t] + (size_t)b * n2, n2 * sizeof(double2),
+                         cudaMemcpyDeviceToHost, ctx_->stream));
+  OMB_CU(cudaStreamSynchronize(ctx_->stream));
+  return OMB_OK;
+}
+
+int Engine::fetch_block_column(int t, int col, double* out) {
+  const Problem& P = (*probs_)[tracks_[t].prob];
+  const size_t n2 = 2 * P.N();
+  cudaStream_t st = ctx_->stream;
+  if (last_prec_ == 1) {
+    OMB_CU(cudaMemcpyAsync(out, y64_.p + col_offset(t, col), n2 * sizeof(double2), cudaMemcpyDeviceToHost, st));
+  } else {
+    DevBuf<double2> tmp;
+    OMB_CU(tmp.alloc(n2, st));
+    k_c32_to_c64<<<blocks_for(n2), 256, 0, st>>>(y32_.p + col_offset(t, col), tmp.p, n2);
+    OMB_CU(cudaGetLastError());
+    OMB_CU(cudaMemcpyAsync(out, tmp.p, n2 * sizeof(double2), cudaMemcpyDeviceToHost, st));
+    OMB_CU(cudaStreamSynchronize(st));
+  }
+  OMB_CU(cudaStreamSynchronize(st));
+  return OMB_OK;
+}
+
+int Engine::result_efield_argmax(int t, int b, long long* idx, double* re, double* im) {
+  const TrackSpec& ts = tracks_[t];
+  const Problem& P = (*probs_)[ts.prob];
+  const size_t N = P.N(), n2 = 2 * N;
+  cudaStream_t st = ctx_->stream;
+  DevBuf<double> red, kd;
+  DevBuf<double2> scr;
+  OMB_CU(red.alloc(3, st));
+  OMB_CU(kd.alloc(1, st));
+  OMB_CU(scr.alloc(3 * N, st));
+  const double k = snaps_[t][b].k;
+  OMB_CU(cudaMemcpyAsync(kd.p, &k, sizeof(double), cudaMemcpyHostToDevice, st));
+  OpUnit<double> u = make_unit<double>(P);
+  u.in = store_.p + store_off_[t] + (size_t)b * n2;
+  u.scr = scr.p;
+  u.k_dev = kd.p;
+  u.in_cs = n2; u.scr_cs = 3 * N; u.ncol = 1;
+  DevBuf<OpUnit<double>> du;
+  OMB_CU(du.alloc(1, st));
+  OMB_CU(cudaMemcpyAsync(du.p, &u, sizeof(u), cudaMemcpyHostToDevice, st));
+  OMB_CU(launch_op<double>(OP_EFIELD, du.p, 1, P.Nx, P.Ny, 1, ctx_->tw, st));
+  k_argmax_abs2<double><<<1, 1024, 0, st>>>(scr.p, (long long)N, 3 * (long long)N, 1, red.p);
+  OMB_CU(cudaGetLastError());
+  double h[3];
+  OMB_CU(cudaMemcpyAsync(h, red.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+  OMB_CU(cudaStreamSynchronize(st));
+  *idx = (long long)h[0];
+  *re = h[1];
+  *im = h[2];
+  return OMB_OK;
+}
+
+}  // namespace omb

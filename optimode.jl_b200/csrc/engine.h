@@ -1,0 +1,96 @@
+// Batched device LOBPCG/Newton engine: host side.
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "context.h"
+#include "lobpcg.cuh"
+
+namespace omb {
+
+struct SolveOptions {
+  double tol = 1e-8;
+  double k_tol = 1e-8;
+  int max_newton = 60;
+  int maxiter = 300;
+  int precision = OMB_PREC_MIXED;
+  bool prec_diag = false;
+  int newton_mode = MODE_NEWTON_INNER;
+  uint64_t seed = 0;
+};
+
+// One eigensolve unit: a Newton band track (solve_k) or a fixed-k block (solve_ω²).
+// In the reference-loop mode a unit runs `nbands` bands one after another (band b+1
+// continues from band b's block and k).
+struct TrackSpec {
+  int prob = 0;             // index into the problem list
+  int band = 0;             // (first) Newton band
+  int nbands = 1;           // bands run in turn (MODE_NEWTON_OUTER)
+  int M = 1;                // block columns
+  int need = 1;             // leading columns that must converge
+  int mode = MODE_NEWTON_INNER;
+  double omega2 = 0, k0 = 0;
+  const double* guess = nullptr;  // host, interleaved complex, nguess columns of length n2
+  int nguess = 0;
+};
+
+class Engine {
+ public:
+  Engine(omb_ctx* ctx, std::vector<Problem>* problems, std::vector<TrackSpec> tracks, SolveOptions opt);
+  ~Engine();
+  // Run all phases (and, in the reference-loop mode, all bands) to completion.
+  int run();
+  // Result b of track t: its state when the band finished, the FP64 eigenvector (band
+  // column of the block, or block column b for solve_ω²) and the argmax of its E field.
+  const TrackState& result_state(int t, int b) const { return snaps_[t][b]; }
+  int fetch_result(int t, int b, double* out);
+  int fetch_block_column(int t, int col, double* out);
+  int result_efield_argmax(int t, int b, long long* idx, double* re, double* im);
+  int64_t graph_launches() const { return launches_; }
+  int64_t kernel_launches() const { return kernels_; }
+  int max_iterations() const;
+
+ private:
+  template <typename T> int run_phase(int phase, bool last, double tau, double lock_tol, bool reuse);
+  template <typename T> int init_block(int phase);
+  int upload_states();
+  int download_states();
+  int snapshot(int round);
+  size_t col_offset(int t, int col) const;  // complex offset of a column of the current block
+
+  omb_ctx* ctx_;
+  std::vector<Problem>* probs_;
+  std::vector<TrackSpec> tracks_;
+  SolveOptions opt_;
+  int nt_ = 0;
+  int round_ = 0;
+  int last_prec_ = 1;  // precision of the buffers holding the final block (0 fp32, 1 fp64)
+  int64_t launches_ = 0, kernels_ = 0;
+
+  struct Group { int off, n, Nx, Ny, Mmax; };
+  std::vector<Group> groups_;
+  std::vector<int> order_;  // tracks sorted by grid size
+
+  DevBuf<TrackState> d_states_;
+  std::vector<TrackState> host_states_;
+  DevBuf<double2> coef_, gram_part_;
+  DevBuf<double> res_part_, hmkh_part_;
+  DevBuf<TrackState*> d_state_ptrs_;
+  DevBuf<double2*> d_gram_ptrs_, d_coef_ptrs_;
+  DevBuf<double*> d_res_ptrs_, d_hmkh_ptrs_;
+  DevBuf<int> d_hmkh_nb_;
+  int gram_chunks_ = 8, upd_chunks_ = 8;
+
+  // block buffers of the current precision (Y/AY per parity, scratch)
+  DevBuf<float2> y32_, s32_;
+  DevBuf<double2> y64_, s64_;
+  std::vector<size_t> yoff_, soff_;  // per-track offsets (complex elements) into the pools
+
+  // finished bands: FP64 vectors on the device and the state at the end of each band
+  DevBuf<double2> store_;
+  std::vector<size_t> store_off_;  // per track; band b at store_off_[t] + b·n2
+  std::vector<std::vector<TrackState>> snaps_;
+};
+
+}  // namespace omb

@@ -1,0 +1,249 @@
+// Rayleigh–Ritz, control and Newton kernels of the device LOBPCG (FP64, precision-agnostic).
+#include "lobpcg.cuh"
+
+namespace omb {
+
+__global__ void __launch_bounds__(RR_NT) k_rr(TrackState* const* __restrict__ states,
+                                               double2* const* __restrict__ gram_parts,
+                                               double2* const* __restrict__ coefs, int ntracks,
+                                               IterParams prm) {
+  const int t = blockIdx.x;
+  if (t >= ntracks) return;
+  TrackState& s = *states[t];
+  if (s.done) return;
+  const int M = s.M;
+  const int n = M + s.nWa + s.nP;
+  constexpr int ld = NMAX;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* G = reinterpret_cast<double2*>(smem_raw);
+  double2* S = G + NMAX * NMAX;
+  double2* V = S + NMAX * NMAX;
+  double2* B = V + NMAX * NMAX;
+  __shared__ Rot rot[NMAX / 2 + 1];
+  __shared__ double red[64];
+  __shared__ int order[NMAX];
+  __shared__ double dsc[NMAX];
+  __shared__ double theta[NMAX];
+  __shared__ int keep[NMAX];
+  __shared__ int rank;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const double2* part = gram_parts[t];
+  // 1. sum the per-chunk partial Gram matrices
+  for (int e = tid; e < n * n; e += nt) {
+    const int a = e / n, b = e % n;
+    double2 g = make_double2(0, 0), sv = make_double2(0, 0);
+    for (int c = 0; c < prm.gram_chunks; ++c) {
+      const double2* pc = part + (size_t)c * (2 * NMAX * NMAX);
+      const double2 x = pc[a * NMAX + b], y = pc[NMAX * NMAX + a * NMAX + b];
+      g.x += x.x; g.y += x.y; sv.x += y.x; sv.y += y.y;
+    }
+    G[a * ld + b] = g;
+    S[a * ld + b] = sv;
+  }
+  __syncthreads();
+  // Hermitian parts
+  for (int e = tid; e < n * n; e += nt) {
+    const int a = e / n, b = e % n;
+    if (a < b) {
+      const double2 g1 = G[a * ld + b], g2 = G[b * ld + a];
+      const double2 gh = make_double2(0.5 * (g1.x + g2.x), 0.5 * (g1.y - g2.y));
+      G[a * ld + b] = gh; G[b * ld + a] = make_double2(gh.x, -gh.y);
+      const double2 s1 = S[a * ld + b], s2 = S[b * ld + a];
+      const double2 sh = make_double2(0.5 * (s1.x + s2.x), 0.5 * (s1.y - s2.y));
+      S[a * ld + b] = sh; S[b * ld + a] = make_double2(sh.x, -sh.y);
+    } else if (a == b) {
+      G[a * ld + a].y = 0; S[a * ld + a].y = 0;
+    }
+  }
+  __syncthreads();
+  // 2. unit-diagonal scaling
+  for (int a = tid; a < n; a += nt) {
+    const double g = G[a * ld + a].x;
+    dsc[a] = (g > 0 && isfinite(g)) ? 1.0 / sqrt(g) : 0.0;
+  }
+  __syncthreads();
+  for (int e = tid; e < n * n; e += nt) {
+    const int a = e / n, b = e % n;
+    const double f = dsc[a] * dsc[b];
+    G[a * ld + b].x *= f; G[a * ld + b].y *= f;
+    S[a * ld + b].x *= f; S[a * ld + b].y *= f;
+  }
+  __syncthreads();
+  // 3. Gram eigen-decomposition, drop near-dependent directions
+  jacobi_eigh(G, V, n, ld, rot, red);
+  if (tid == 0) {
+    double tmax = 0;
+    for (int i = 0; i < n; ++i) { theta[i] = G[i * ld + i].x; tmax = fmax(tmax, theta[i]); }
+    int r = 0;
+    for (int i = 0; i < n; ++i)
+      if (theta[i] > prm.gram_drop * tmax && dsc[i] >= 0) keep[r++] = i;
+    rank = r;
+  }
+  __syncthreads();
+  const int r = rank;
+  if (r < M) {
+    if (tid == 0) {
+      s.status = TS_ORTHO; s.done = 1; s.op_ncol = 0; s.pw_ncol = 0; s.hmkh_ncol = 0;
+      s.rr_n = n; s.rr_rank = r;
+    }
+    return;
+  }
+  // B = V_keep Θ^{-1/2}   (n × r)
+  for (int e = tid; e < n * r; e += nt) {
+    const int l = e / r, j = e % r;
+    const double f = 1.0 / sqrt(theta[keep[j]]);
+    const double2 v = V[l * ld + keep[j]];
+    B[l * ld + j] = make_double2(v.x * f, v.y * f);
+  }
+  __syncthreads();
+  // V ← S B (n × r), then G ← Bᴴ V (r × r)
+  for (int e = tid; e < n * r; e += nt) {
+    const int l = e / r, j = e % r;
+    double2 acc = make_double2(0, 0);
+    for (int m = 0; m < n; ++m) {
+      const double2 a = S[l * ld + m], b = B[m * ld + j];
+      acc.x += a.x * b.x - a.y * b.y;
+      acc.y += a.x * b.y + a.y * b.x;
+    }
+    V[l * ld + j] = acc;
+  }
+  __syncthreads();
+  for (int e = tid; e < r * r; e += nt) {
+    const int i = e / r, j = e % r;
+    double2 acc = make_double2(0, 0);
+    for (int l = 0; l < n; ++l) {
+      const double2 a = B[l * ld + i], b = V[l * ld + j];
+      acc.x += a.x * b.x + a.y * b.y;  // conj(a)·b
+      acc.y += a.x * b.y - a.y * b.x;
+    }
+    G[i * ld + j] = acc;
+  }
+  __syncthreads();
+  // 4. projected eigenproblem
+  jacobi_eigh(G, V, r, ld, rot, red);
+  sort_diag(G, r, ld, order);
+  // 5. C = D B U[:, order[:M]] (coefficients of the new X in the Z columns), Ritz values
+  double2* coef = coefs[t];
+  for (int e = tid; e < n * M; e += nt) {
+    const int l = e / M, m = e % M;
+    const int um = order[m];
+    double2 acc = make_double2(0, 0);
+    for (int j = 0; j < r; ++j) {
+      const double2 a = B[l * ld + j], b = V[j * ld + um];
+      acc.x += a.x * b.x - a.y * b.y;
+      acc.y += a.x * b.y + a.y * b.x;
+    }
+    coef[l * MMAX + m] = make_double2(acc.x * dsc[l], acc.y * dsc[l]);
+  }
+  for (int m = tid; m < M; m += nt) s.lam[m] = G[order[m] * ld + order[m]].x;
+  __syncthreads();
+  // 6. P coefficients for the active columns: the W and P parts of the Ritz vectors
+  const int nPn = (s.nWa + s.nP > 0) ? (M - s.nlocked) : 0;
+  for (int e = tid; e < n * nPn; e += nt) {
+    const int l = e / nPn, mp = e % nPn;
+    coef[NMAX * MMAX + l * MMAX + mp] = (l < M) ? make_double2(0, 0) : coef[l * MMAX + (s.nlocked + mp)];
+  }
+  if (tid == 0) { s.nP_next = nPn; s.rr_n = n; s.rr_rank = r; }
+}
+
+__device__ __forceinline__ void finish(TrackState& s, int status) {
+  s.status = status;
+  s.done = 1;
+  s.op_ncol = 0; s.pw_ncol = 0; s.hmkh_ncol = 0;
+}
+
+__global__ void k_control(TrackState* const* __restrict__ states, double* const* __restrict__ res_parts,
+                          int ntracks, IterParams prm) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntracks) return;
+  TrackState& s = *states[t];
+  if (s.done) return;
+  const int M = s.M;
+  const double* rp = res_parts[t];
+  bool bad = false;
+  for (int m = 0; m < M; ++m) {
+    double v = 0;
+    for (int c = 0; c < prm.upd_chunks; ++c) v += rp[(size_t)c * MMAX + m];
+    s.resid[m] = sqrt(v);
+    if (!isfinite(s.resid[m]) || !isfinite(s.lam[m])) bad = true;
+  }
+  s.nP = s.nP_next;
+  s.iter++; s.iter_phase++; s.since_newton++;
+  if (bad || !isfinite(s.k)) { finish(s, TS_NAN); return; }
+  const int need = s.need;
+  double maxres = 0;
+  for (int i = 0; i < need; ++i) maxres = fmax(maxres, s.resid[i]);
+  if (maxres < 0.9 * s.resid_best) { s.resid_best = maxres; s.stall = 0; } else { s.stall++; }
+  while (s.nlocked < need && s.resid[s.nlocked] < prm.lock_tol) s.nlocked++;
+  const bool last = prm.last_phase != 0;
+  s.hmkh_ncol = 0;
+  if (s.mode == MODE_OMEGA2) {
+    if (maxres < prm.tau_phase) { finish(s, last ? TS_CONVERGED : TS_PHASE_DONE); return; }
+    if (!last && s.stall >= 8) { finish(s, TS_PHASE_DONE); return; }
+  } else if (s.mode == MODE_NEWTON_INNER) {
+    const double dw2 = s.lam[s.band] - s.omega2;
+    if (last) {
+      // final steps from converged eigenpairs; earlier ones while the k mismatch dominates
+      // the eigen-residual, plus at most one early step per phase near the tolerance
+      if (maxres < prm.tol) s.hmkh_ncol = 1;
+      else if (s.since_newton >= 2 && maxres < 0.1 * fabs(dw2)) s.hmkh_ncol = 1;
+      else if (s.since_newton >= 2 && s.newton_phase == 0 && maxres < 100 * prm.tol) s.hmkh_ncol = 1;
+    } else {
+      if (s.newton_steps > 0 && maxres < prm.tau_phase && fabs(s.dk_last) < prm.dk_phase) {
+        finish(s, TS_PHASE_DONE); return;
+      }
+      if (s.newton_steps > 0 && s.stall >= 8) { finish(s, TS_PHASE_DONE); return; }
+      if (s.since_newton >= 2 && maxres < fmax(0.1 * fabs(dw2), prm.tau_phase)) s.hmkh_ncol = 1;
+    }
+  } else {  // MODE_NEWTON_OUTER: the reference loop, a step after each converged eigensolve
+    if (maxres < prm.tol) s.hmkh_ncol = 1;
+  }
+  if (s.iter_phase >= prm.maxiter && s.hmkh_ncol == 0) { finish(s, last ? TS_MAXITER : TS_PHASE_DONE); return; }
+  s.nWa = M - s.nlocked;
+  s.op_col0 = M + s.nlocked;
+  s.op_ncol = s.nWa;
+  s.pw_col0 = s.nlocked;
+  s.pw_ncol = s.nWa;
+}
+
+__global__ void k_newton(TrackState* const* __restrict__ states, double* const* __restrict__ hmkh_parts,
+                         const int* __restrict__ hmkh_nb, int ntracks, IterParams prm) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntracks) return;
+  TrackState& s = *states[t];
+  if (s.done || s.hmkh_ncol == 0) return;
+  const double* hp = hmkh_parts[t];
+  double re = 0;
+  for (int b = 0; b < hmkh_nb[t]; ++b) re += hp[2 * b];
+  const double h = -re;
+  const double dw2dk = 2.0 * h;
+  const int j = s.band;
+  const double dk = (s.lam[j] - s.omega2) / dw2dk;
+  s.hmkh_ncol = 0;
+  if (!(dw2dk > 0) || !isfinite(dk)) { finish(s, TS_NAN); return; }
+  s.k_eig = s.k;
+  s.hmkh = h;
+  s.k -= dk;
+  s.dk_last = dk;
+  s.newton_steps++;
+  s.newton_phase++;
+  s.since_newton = 0;
+  if (s.mode == MODE_NEWTON_OUTER) s.iter_phase = 0;  // the reference budgets each eigensolve
+  double maxres = 0;
+  for (int i = 0; i < s.need; ++i) maxres = fmax(maxres, s.resid[i]);
+  if (!(s.k > 0)) { finish(s, TS_NAN); return; }
+  if (prm.last_phase && maxres < prm.tol && fabs(dk) < prm.k_tol) { finish(s, TS_CONVERGED); return; }
+  if (s.newton_steps >= prm.max_newton) { finish(s, prm.last_phase ? TS_MAXITER : TS_PHASE_DONE); return; }
+  // k moved: recompute AX (and AW) at the new k, restart the P direction and locking
+  const int M = s.M;
+  s.nP = 0;
+  s.nlocked = 0;
+  s.nWa = M;
+  s.op_col0 = 0;
+  s.op_ncol = 2 * M;
+  s.pw_ncol = 0;
+  s.resid_best = 1e300;
+  s.stall = 0;
+}
+
+}  // namespace omb

@@ -36,6 +36,7 @@ template <typename T> struct OpUnit {
   const double* k_dev;    // wavevector magnitude (device, so the solver can update it)
   double* partial;        // per-(column, row-block) partial sums for RO_KXCT_DOT
   const int* ncol_dev;    // optional device-side column count
+  const int* col0_dev;    // optional device-side first column of in/out (scratch is not offset)
   long long in_cs, out_cs, scr_cs;  // column strides in complex elements
   int Nx, Ny, ncol;
   int part_stride;        // partial sums per column (≥ gridDim.x of row_out)
@@ -61,6 +62,9 @@ template <> __device__ __forceinline__ void load_eps<double>(const OpUnit<double
 template <typename T> __device__ __forceinline__ int unit_ncol(const OpUnit<T>& U) {
   return U.ncol_dev ? *U.ncol_dev : U.ncol;
 }
+template <typename T> __device__ __forceinline__ int unit_col0(const OpUnit<T>& U) {
+  return U.col0_dev ? *U.col0_dev : 0;
+}
 
 template <typename C> __device__ __forceinline__ void load_tw(C* tw, const C* tw_g, int L) {
   for (int i = threadIdx.x; i < L; i += blockDim.x) tw[i] = tw_g[i];
@@ -85,7 +89,7 @@ __global__ void __launch_bounds__(NT) k_row_in(const OpUnit<T>* __restrict__ uni
   const size_t N = (size_t)NX * Ny;
   load_tw(tw, tw_g, NX);
   const T k = (T)(*U.k_dev);
-  const C* __restrict__ H = U.in + (size_t)col * U.in_cs;
+  const C* __restrict__ H = U.in + (size_t)(col + unit_col0(U)) * U.in_cs;
   for (int q = threadIdx.x; q < ROWS * NX; q += NT) {
     const int r = q / NX, ix = q - r * NX, iy = row0 + r;
     C d0 = mk<C>(0, 0), d1 = d0, d2 = d0;
@@ -217,7 +221,8 @@ __global__ void __launch_bounds__(NT) k_row_out(const OpUnit<T>* __restrict__ un
   fft_lines<C, NX, INV, 3 * ROWS, NT>(s, LS, tw);
   const T k = (T)(*U.k_dev);
   const T sN = T(1) / T(N);
-  C* __restrict__ O = U.out + (size_t)col * U.out_cs;
+  const int c0 = unit_col0(U);
+  C* __restrict__ O = U.out + (size_t)(col + c0) * U.out_cs;
   double accr = 0.0, acci = 0.0;
   for (int q = threadIdx.x; q < ROWS * NX; q += NT) {
     const int r = q / NX, ix = q - r * NX, iy = row0 + r;
@@ -239,7 +244,7 @@ __global__ void __launch_bounds__(NT) k_row_out(const OpUnit<T>* __restrict__ un
         h1 = en * (-sc); h2 = em * sc;
       }
       if constexpr (MODE == RO_KXCT_DOT) {
-        const C* Hin = U.in + (size_t)col * U.in_cs;
+        const C* Hin = U.in + (size_t)(col + c0) * U.in_cs;
         const C g1 = Hin[2 * p], g2 = Hin[2 * p + 1];
         // ⟨H_in, out⟩ = Σ conj(H_in)·out
         accr += (double)g1.x * h1.x + (double)g1.y * h1.y + (double)g2.x * h2.x + (double)g2.y * h2.y;

@@ -23,6 +23,10 @@ struct TwTables {
 };
 
 bool fft_size_supported(int L);
+// Raise a kernel's dynamic shared-memory limit once per (kernel, device); later calls for
+// the same or a smaller size return without touching the driver (so they are safe inside
+// a stream capture after a warm-up launch).
+cudaError_t ensure_smem(const void* func, size_t bytes);
 // Number of row blocks row_out uses for a grid with Ny rows (partial sums per column).
 int row_blocks(int Nx, int Ny);
 

@@ -25,7 +25,7 @@ template <typename T>
 static cudaError_t launch_pass(PassKernel<T> kern, dim3 g, int nt, size_t smem, cudaStream_t st,
                                const OpUnit<T>* units, const cplx<T>* tw) {
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = ensure_smem(reinterpret_cast<const void*>(kern), smem);
     if (e != cudaSuccess) return e;
   }
   kern<<<g, nt, smem, st>>>(units, tw);

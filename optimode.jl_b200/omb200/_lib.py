@@ -77,6 +77,8 @@ def load():
             f = getattr(lib, name)
             f.restype = res
             f.argtypes = args
+        for declare in _DECLARERS:
+            declare(lib)
         _lib = lib
         return lib
 
@@ -117,10 +119,81 @@ _contexts: dict = {}
 
 
 def context(device: int = 0) -> Context:
-    with _lock:
-        pass
     c = _contexts.get(device)
     if c is None or c.handle is None:
         c = Context(device)
         _contexts[device] = c
     return c
+
+
+class c_options(ctypes.Structure):
+    _fields_ = [("k_tol", ctypes.c_double), ("eig_tol", ctypes.c_double),
+                ("max_eigsolves", ctypes.c_int32), ("maxiter", ctypes.c_int32),
+                ("precision", ctypes.c_int32), ("preconditioner", ctypes.c_int32),
+                ("newton", ctypes.c_int32), ("canonicalize", ctypes.c_int32),
+                ("seed", ctypes.c_uint64)]
+
+
+class c_instance(ctypes.Structure):
+    _fields_ = [("grid", c_grid), ("omega", ctypes.c_double), ("epsinv", _dp),
+                ("nev", ctypes.c_int32), ("kguess", ctypes.c_double), ("Hguess", _dp),
+                ("nguess", ctypes.c_int32)]
+
+
+_ip = ctypes.POINTER(ctypes.c_int32)
+
+
+class c_result(ctypes.Structure):
+    _fields_ = [("kmags", _dp), ("evecs", _dp), ("residuals", _dp), ("dw2dk", _dp),
+                ("status", _ip), ("iterations", _ip), ("newton_steps", _ip)]
+
+
+def _declare_solve(lib):
+    vp = ctypes.c_void_p
+    sig = {
+        "omb_options_default": (ctypes.c_int, [ctypes.POINTER(c_options)]),
+        "omb_solve_k": (ctypes.c_int, [vp, ctypes.POINTER(c_instance), ctypes.c_int,
+                                       ctypes.POINTER(c_options), ctypes.POINTER(c_result)]),
+        "omb_solve_omega2": (ctypes.c_int, [vp, ctypes.POINTER(c_grid), ctypes.c_double, _dp,
+                                            ctypes.c_int, _dp, ctypes.c_int,
+                                            ctypes.POINTER(c_options), _dp, _dp, _dp, _ip]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+
+
+EXPORTS = EXPORTS + ("omb_options_default", "omb_solve_k", "omb_solve_omega2")
+_DECLARERS = [_declare_solve]
+
+
+class c_stats(ctypes.Structure):
+    _fields_ = [("graph_launches", ctypes.c_int64), ("kernel_launches", ctypes.c_int64),
+                ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64),
+                ("tracks", ctypes.c_int32), ("max_iterations", ctypes.c_int32),
+                ("run_seconds", ctypes.c_double)]
+
+
+def _declare_batch(lib):
+    vp = ctypes.c_void_p
+    sig = {
+        "omb_batch_create": (ctypes.c_int, [vp, ctypes.POINTER(c_instance), ctypes.c_int,
+                                            ctypes.POINTER(c_options), ctypes.POINTER(vp)]),
+        "omb_batch_run": (ctypes.c_int, [vp]),
+        "omb_batch_results": (ctypes.c_int, [vp, ctypes.POINTER(c_result)]),
+        "omb_batch_stats": (ctypes.c_int, [vp, ctypes.POINTER(c_stats)]),
+        "omb_batch_destroy": (ctypes.c_int, [vp]),
+        "omb_profile_apply": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(c_grid),
+                                             ctypes.c_double, _dp, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_int, _dp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+
+
+EXPORTS = EXPORTS + ("omb_batch_create", "omb_batch_run", "omb_batch_results", "omb_batch_stats",
+                     "omb_batch_destroy", "omb_profile_apply")
+_DECLARERS.append(_declare_batch)

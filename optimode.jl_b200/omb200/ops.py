@@ -80,3 +80,16 @@ def E_field(k, epsinv, grid, H, precision="fp64", device=0):
     _lib.check(lib.omb_efield(ctx.handle, _lib.PREC[precision], ctypes.byref(grid.c()), float(k),
                               _dptr(e), _dptr(B), _dptr(out)))
     return out
+
+
+def profile_apply(op: str, k, epsinv, grid: Grid, ncol: int, nbatch: int, reps: int = 20,
+                  precision: str = "fp32", device: int = 0) -> float:
+    """Mean device seconds of one application of ``op`` ("M" or "P") to ``ncol`` columns on
+    each of ``nbatch`` device-resident copies of the cell (``omb_profile_apply``)."""
+    lib = _lib.load()
+    ctx = _lib.context(device)
+    e = epsinv_host(epsinv, grid)
+    out = np.zeros(1)
+    _lib.check(lib.omb_profile_apply(ctx.handle, _lib.OPS[op], _lib.PREC[precision], ctypes.byref(grid.c()),
+                                     float(k), _dptr(e), int(ncol), int(nbatch), int(reps), _dptr(out)))
+    return float(out[0])
