@@ -171,12 +171,30 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--case", default="full", choices=["full", "apply", "solve1"],
+                    help="apply / solve1: one operator-apply timing or one single-instance solve "
+                         "(small, self-contained runs for profiling)")
+    ap.add_argument("--apply-cells", type=int, default=64)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank)
+    if args.case != "full":
+        import omb200
+        g, probs = workload(1)
+        if args.case == "apply":
+            t = omb200.profile_apply("M", 1.3, probs[0]["eps_inv"], g, NEV, args.apply_cells, reps=args.steps)
+            print(json.dumps({"case": "apply", "seconds_per_apply": t, "cells": args.apply_cells, "ncol": NEV}))
+        else:
+            b = omb200.Batch(probs, omb200.B200Solver(device=local))
+            b.run()
+            _, info = b.results(return_info=True, raise_on_failure=False)
+            print(json.dumps({"case": "solve1", **{k: v for k, v in b.stats().items()},
+                              "iterations": info[0]["iterations"].tolist()}))
+            b.close()
+        return
 
     import torch
     dist = None
@@ -266,8 +284,10 @@ def main():
                     "peak_source": peak_kind}
         plain = None
         if not args.no_plain:
-            ps = omb200.B200Solver(precision="fp64", preconditioner="mpb", newton="outer", device=local)
-            pb = omb200.Batch(probs[:1], ps)
+            # the reference loop's per-eigensolve budget is raised so that it converges
+            # every band from its random start
+            ps = omb200.B200Solver(precision="fp64", preconditioner="diag", newton="outer", device=local)
+            pb = omb200.Batch(probs[:1], ps, maxiter=3000)
             pb.run()
             pst = pb.stats()
             _, pinfo = pb.results(return_info=True, raise_on_failure=False)

@@ -71,7 +71,7 @@ int omb_options_default(omb_options* o) {
   o->max_eigsolves = 60;
   o->maxiter = 300;
   o->precision = OMB_PREC_MIXED;
-  o->preconditioner = OMB_OP_P;
+  o->preconditioner = OMB_OP_P_DIAG;
   o->newton = OMB_NEWTON_INNER;
   o->canonicalize = 1;
   o->seed = 0;

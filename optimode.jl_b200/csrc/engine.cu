@@ -13,8 +13,10 @@ static int blocks_for(size_t n, int nt = 256) {
   return (int)std::max<size_t>(1, std::min<size_t>(b, 65535 * 4));
 }
 
+// Opt in to large dynamic shared memory.  The default limit covers static + dynamic, so
+// opt in whenever the dynamic part alone comes near it.
 template <typename K> static cudaError_t set_smem(K kern, size_t bytes) {
-  if (bytes <= 48 * 1024) return cudaSuccess;
+  if (bytes <= 32 * 1024) return cudaSuccess;
   return ensure_smem(reinterpret_cast<const void*>(kern), bytes);
 }
 
@@ -239,45 +241,51 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
   int Mmax = 1;
   for (const auto& ts : tracks_) Mmax = std::max(Mmax, ts.M);
   const int nmax = 3 * Mmax;
-  const size_t sm_gram = 2 * (size_t)nmax * GRAM_ROWS * sizeof(cplx<T>);
-  const size_t sm_upd = 2 * (size_t)nmax * UPD_ROWS * sizeof(cplx<T>) + 2 * (size_t)nmax * MMAX * sizeof(cplx<T>);
+  const int nbmax = (nmax + 1) / 2;
+  const size_t sm_gram = gram_smem<T>(nbmax);
+  const int item_chunks = (2 * (nbmax * (nbmax + 1) / 2) + gram_ipc<T>() - 1) / gram_ipc<T>();
   const size_t sm_rr = 4 * (size_t)NMAX * NMAX * sizeof(double2);
   OMB_CU(set_smem(k_gram<T>, sm_gram));
-  OMB_CU(set_smem(k_update<T>, sm_upd));
+  auto update_kernel = Mmax <= 4 ? k_update<T, 4> : (Mmax <= 8 ? k_update<T, 8> : k_update<T, MMAX>);
   OMB_CU(set_smem(k_rr, sm_rr));
   const int cb = (nt_ + 127) / 128;
 
+  const char* step = "";
   auto iteration = [&](int par) -> cudaError_t {
-    cudaError_t e;
+    cudaError_t e = cudaSuccess;
+    auto ok = [&](const char* name, cudaError_t r) { step = name; e = r; return r == cudaSuccess; };
     if (!opt_.prec_diag)
       for (const Group& g : groups_)
-        if ((e = launch_op<T>(OP_P, d_uP[par].p + g.off, g.n, g.Nx, g.Ny, g.Mmax, ctx_->tw, st)) != cudaSuccess) return e;
+        if (!ok("preconditioner pass", launch_op<T>(OP_P, d_uP[par].p + g.off, g.n, g.Nx, g.Ny, g.Mmax, ctx_->tw, st))) return e;
     for (const Group& g : groups_)
-      if ((e = launch_op<T>(OP_HMKH, d_uH[par].p + g.off, g.n, g.Nx, g.Ny, 1, ctx_->tw, st)) != cudaSuccess) return e;
+      if (!ok("HMkH pass", launch_op<T>(OP_HMKH, d_uH[par].p + g.off, g.n, g.Nx, g.Ny, 1, ctx_->tw, st))) return e;
     k_newton<<<cb, 128, 0, st>>>(d_state_ptrs_.p, d_hmkh_ptrs_.p, d_hmkh_nb_.p, nt_, prm);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (!ok("k_newton", cudaGetLastError())) return e;
     for (const Group& g : groups_)
-      if ((e = launch_op<T>(OP_M, d_uA[par].p + g.off, g.n, g.Nx, g.Ny, 2 * g.Mmax, ctx_->tw, st)) != cudaSuccess) return e;
-    k_gram<T><<<dim3(gram_chunks_, nt_), GRAM_NT, sm_gram, st>>>(d_descs.p, par, gram_chunks_);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      if (!ok("operator pass", launch_op<T>(OP_M, d_uA[par].p + g.off, g.n, g.Nx, g.Ny, 2 * g.Mmax, ctx_->tw, st))) return e;
+    k_gram<T><<<dim3(gram_chunks_, nt_, item_chunks), GRAM_NT, sm_gram, st>>>(d_descs.p, par, gram_chunks_);
+    if (!ok("k_gram", cudaGetLastError())) return e;
     k_rr<<<nt_, RR_NT, sm_rr, st>>>(d_state_ptrs_.p, d_gram_ptrs_.p, d_coef_ptrs_.p, nt_, prm);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_update<T><<<dim3(upd_chunks_, nt_), UPD_NT, sm_upd, st>>>(d_descs.p, par, upd_chunks_, prm.prec_diag);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_control<<<cb, 128, 0, st>>>(d_state_ptrs_.p, d_res_ptrs_.p, nt_, prm);
-    return cudaGetLastError();
+    if (!ok("k_rr", cudaGetLastError())) return e;
+    update_kernel<<<dim3(upd_chunks_, nt_), UPD_NT, 0, st>>>(d_descs.p, par, upd_chunks_, prm.prec_diag);
+    if (!ok("k_update", cudaGetLastError())) return e;
+    k_control<<<(nt_ + 3) / 4, 128, 0, st>>>(d_state_ptrs_.p, d_res_ptrs_.p, nt_, prm);
+    ok("k_control", cudaGetLastError());
+    return e;
   };
 
   // two eager iterations (they also size the kernels' shared memory), then the graph
-  OMB_CU(iteration(0));
-  OMB_CU(iteration(1));
+  for (int par = 0; par < 2; ++par) {
+    const cudaError_t e = iteration(par);
+    if (e != cudaSuccess) return cuda_fail(e, step);
+  }
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   OMB_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
   cudaError_t ce = iteration(0);
   if (ce == cudaSuccess) ce = iteration(1);
   cudaError_t ee = cudaStreamEndCapture(st, &graph);
-  if (ce != cudaSuccess) { if (graph) cudaGraphDestroy(graph); return cuda_fail(ce, "graph capture"); }
+  if (ce != cudaSuccess) { if (graph) cudaGraphDestroy(graph); return cuda_fail(ce, step); }
   OMB_CU(ee);
   OMB_CU(cudaGraphInstantiate(&exec, graph, 0));
   size_t nodes = 0;

@@ -28,32 +28,21 @@ __global__ void __launch_bounds__(RR_NT) k_rr(TrackState* const* __restrict__ st
   __shared__ int rank;
   const int tid = threadIdx.x, nt = blockDim.x;
   const double2* part = gram_parts[t];
-  // 1. sum the per-chunk partial Gram matrices
-  for (int e = tid; e < n * n; e += nt) {
-    const int a = e / n, b = e % n;
-    double2 g = make_double2(0, 0), sv = make_double2(0, 0);
+  // 1. sum the per-chunk partial Gram matrices (upper triangles) and mirror them
+  for (int e = tid; e < 2 * n * n; e += nt) {
+    const int which = e / (n * n), ab = e % (n * n), a = ab / n, b = ab % n;
+    if (a > b) continue;
+    double2 g = make_double2(0, 0);
+    const double2* pc = part + which * NMAX * NMAX + a * NMAX + b;
+#pragma unroll 4
     for (int c = 0; c < prm.gram_chunks; ++c) {
-      const double2* pc = part + (size_t)c * (2 * NMAX * NMAX);
-      const double2 x = pc[a * NMAX + b], y = pc[NMAX * NMAX + a * NMAX + b];
-      g.x += x.x; g.y += x.y; sv.x += y.x; sv.y += y.y;
+      const double2 x = pc[(size_t)c * (2 * NMAX * NMAX)];
+      g.x += x.x; g.y += x.y;
     }
-    G[a * ld + b] = g;
-    S[a * ld + b] = sv;
-  }
-  __syncthreads();
-  // Hermitian parts
-  for (int e = tid; e < n * n; e += nt) {
-    const int a = e / n, b = e % n;
-    if (a < b) {
-      const double2 g1 = G[a * ld + b], g2 = G[b * ld + a];
-      const double2 gh = make_double2(0.5 * (g1.x + g2.x), 0.5 * (g1.y - g2.y));
-      G[a * ld + b] = gh; G[b * ld + a] = make_double2(gh.x, -gh.y);
-      const double2 s1 = S[a * ld + b], s2 = S[b * ld + a];
-      const double2 sh = make_double2(0.5 * (s1.x + s2.x), 0.5 * (s1.y - s2.y));
-      S[a * ld + b] = sh; S[b * ld + a] = make_double2(sh.x, -sh.y);
-    } else if (a == b) {
-      G[a * ld + a].y = 0; S[a * ld + a].y = 0;
-    }
+    double2* Mx = which ? S : G;
+    if (a == b) g.y = 0;
+    Mx[a * ld + b] = g;
+    Mx[b * ld + a] = make_double2(g.x, -g.y);
   }
   __syncthreads();
   // 2. unit-diagonal scaling
@@ -69,73 +58,189 @@ __global__ void __launch_bounds__(RR_NT) k_rr(TrackState* const* __restrict__ st
     S[a * ld + b].x *= f; S[a * ld + b].y *= f;
   }
   __syncthreads();
-  // 3. Gram eigen-decomposition, drop near-dependent directions
-  jacobi_eigh(G, V, n, ld, rot, red);
-  if (tid == 0) {
-    double tmax = 0;
-    for (int i = 0; i < n; ++i) { theta[i] = G[i * ld + i].x; tmax = fmax(tmax, theta[i]); }
-    int r = 0;
-    for (int i = 0; i < n; ++i)
-      if (theta[i] > prm.gram_drop * tmax && dsc[i] >= 0) keep[r++] = i;
-    rank = r;
+  // 3. Basis of the Gram metric.  Fast path: Cholesky Gs = L Lᴴ, then the projected
+  //    problem L⁻¹ Ss L⁻ᴴ u = λu and C = D L⁻ᴴ u.  When a pivot falls below the floor
+  //    (near-dependent directions) the SVQB path below drops them instead.
+  __shared__ int chol_ok;
+  if (tid == 0) chol_ok = 1;
+  __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    const double piv = G[j * ld + j].x;
+    if (!(piv > prm.gram_drop)) { chol_ok = 0; break; }  // uniform across the block
+    const double ljj = sqrt(piv);
+    for (int i = j + 1 + tid; i < n; i += nt) {
+      const double2 g = G[i * ld + j];
+      G[i * ld + j] = make_double2(g.x / ljj, g.y / ljj);
+    }
+    __syncthreads();
+    if (tid == 0) G[j * ld + j] = make_double2(ljj, 0.0);
+    const int w = n - j - 1;
+    for (int e = tid; e < w * w; e += nt) {
+      const int i = j + 1 + e / w, k = j + 1 + e % w;
+      if (k <= i) {
+        const double2 li = G[i * ld + j], lk = G[k * ld + j];
+        G[i * ld + k].x -= li.x * lk.x + li.y * lk.y;  // L_ij·conj(L_kj)
+        G[i * ld + k].y -= li.y * lk.x - li.x * lk.y;
+      }
+    }
+    __syncthreads();
   }
   __syncthreads();
-  const int r = rank;
-  if (r < M) {
+  int r;
+  double2* Ev;  // eigenvectors of the projected problem (columns), n_eff × n_eff
+  double2* Av;  // the projected matrix, eigenvalues on its diagonal after Jacobi
+  if (chol_ok) {
+    r = n;
+    // V ← L⁻¹ Ss (column-parallel forward substitution)
+    for (int c = tid; c < n; c += nt) {
+      for (int i = 0; i < n; ++i) {
+        double2 t = S[i * ld + c];
+        for (int k = 0; k < i; ++k) {
+          const double2 l = G[i * ld + k], v = V[k * ld + c];
+          t.x -= l.x * v.x - l.y * v.y;
+          t.y -= l.x * v.y + l.y * v.x;
+        }
+        const double d = G[i * ld + i].x;
+        V[i * ld + c] = make_double2(t.x / d, t.y / d);
+      }
+    }
+    __syncthreads();
+    // B ← L⁻¹ Vᴴ = L⁻¹ Ss L⁻ᴴ
+    for (int c = tid; c < n; c += nt) {
+      for (int i = 0; i < n; ++i) {
+        const double2 vc = V[c * ld + i];
+        double2 t = make_double2(vc.x, -vc.y);
+        for (int k = 0; k < i; ++k) {
+          const double2 l = G[i * ld + k], v = B[k * ld + c];
+          t.x -= l.x * v.x - l.y * v.y;
+          t.y -= l.x * v.y + l.y * v.x;
+        }
+        const double d = G[i * ld + i].x;
+        B[i * ld + c] = make_double2(t.x / d, t.y / d);
+      }
+    }
+    __syncthreads();
+    for (int e = tid; e < n * n; e += nt) {  // Hermitian part
+      const int i = e / n, j = e % n;
+      if (i < j) {
+        const double2 x = B[i * ld + j], y = B[j * ld + i];
+        const double2 h = make_double2(0.5 * (x.x + y.x), 0.5 * (x.y - y.y));
+        B[i * ld + j] = h;
+        B[j * ld + i] = make_double2(h.x, -h.y);
+      } else if (i == j) {
+        B[i * ld + i].y = 0;
+      }
+    }
+    __syncthreads();
+    jacobi_eigh(B, V, r, ld, rot, red);
+    Ev = V;
+    Av = B;
+  } else {
+    // SVQB: rebuild the scaled Gram matrix (the Cholesky attempt overwrote it)
+    for (int e = tid; e < n * n; e += nt) {
+      const int a = e / n, b = e % n;
+      if (a > b) continue;
+      double2 g = make_double2(0, 0);
+      const double2* pc = part + a * NMAX + b;
+      for (int c = 0; c < prm.gram_chunks; ++c) {
+        const double2 x = pc[(size_t)c * (2 * NMAX * NMAX)];
+        g.x += x.x; g.y += x.y;
+      }
+      const double f = dsc[a] * dsc[b];
+      if (a == b) g.y = 0;
+      G[a * ld + b] = make_double2(g.x * f, g.y * f);
+      G[b * ld + a] = make_double2(g.x * f, -g.y * f);
+    }
+    __syncthreads();
+    jacobi_eigh(G, V, n, ld, rot, red);
     if (tid == 0) {
-      s.status = TS_ORTHO; s.done = 1; s.op_ncol = 0; s.pw_ncol = 0; s.hmkh_ncol = 0;
-      s.rr_n = n; s.rr_rank = r;
+      double tmax = 0;
+      for (int i = 0; i < n; ++i) { theta[i] = G[i * ld + i].x; tmax = fmax(tmax, theta[i]); }
+      int rr = 0;
+      for (int i = 0; i < n; ++i)
+        if (theta[i] > prm.gram_drop * tmax) keep[rr++] = i;
+      rank = rr;
     }
-    return;
-  }
-  // B = V_keep Θ^{-1/2}   (n × r)
-  for (int e = tid; e < n * r; e += nt) {
-    const int l = e / r, j = e % r;
-    const double f = 1.0 / sqrt(theta[keep[j]]);
-    const double2 v = V[l * ld + keep[j]];
-    B[l * ld + j] = make_double2(v.x * f, v.y * f);
-  }
-  __syncthreads();
-  // V ← S B (n × r), then G ← Bᴴ V (r × r)
-  for (int e = tid; e < n * r; e += nt) {
-    const int l = e / r, j = e % r;
-    double2 acc = make_double2(0, 0);
-    for (int m = 0; m < n; ++m) {
-      const double2 a = S[l * ld + m], b = B[m * ld + j];
-      acc.x += a.x * b.x - a.y * b.y;
-      acc.y += a.x * b.y + a.y * b.x;
+    __syncthreads();
+    r = rank;
+    if (r < M) {
+      if (tid == 0) {
+        s.status = TS_ORTHO; s.done = 1; s.op_ncol = 0; s.pw_ncol = 0; s.hmkh_ncol = 0;
+        s.rr_n = n; s.rr_rank = r;
+      }
+      return;
     }
-    V[l * ld + j] = acc;
-  }
-  __syncthreads();
-  for (int e = tid; e < r * r; e += nt) {
-    const int i = e / r, j = e % r;
-    double2 acc = make_double2(0, 0);
-    for (int l = 0; l < n; ++l) {
-      const double2 a = B[l * ld + i], b = V[l * ld + j];
-      acc.x += a.x * b.x + a.y * b.y;  // conj(a)·b
-      acc.y += a.x * b.y - a.y * b.x;
+    // B = V_keep Θ^{-1/2}   (n × r)
+    for (int e = tid; e < n * r; e += nt) {
+      const int l = e / r, j = e % r;
+      const double f = 1.0 / sqrt(theta[keep[j]]);
+      const double2 v = V[l * ld + keep[j]];
+      B[l * ld + j] = make_double2(v.x * f, v.y * f);
     }
-    G[i * ld + j] = acc;
+    __syncthreads();
+    // V ← S B (n × r), then G ← Bᴴ V (r × r)
+    for (int e = tid; e < n * r; e += nt) {
+      const int l = e / r, j = e % r;
+      double2 acc = make_double2(0, 0);
+      for (int m = 0; m < n; ++m) {
+        const double2 a = S[l * ld + m], b = B[m * ld + j];
+        acc.x += a.x * b.x - a.y * b.y;
+        acc.y += a.x * b.y + a.y * b.x;
+      }
+      V[l * ld + j] = acc;
+    }
+    __syncthreads();
+    for (int e = tid; e < r * r; e += nt) {
+      const int i = e / r, j = e % r;
+      double2 acc = make_double2(0, 0);
+      for (int l = 0; l < n; ++l) {
+        const double2 a = B[l * ld + i], b = V[l * ld + j];
+        acc.x += a.x * b.x + a.y * b.y;  // conj(a)·b
+        acc.y += a.x * b.y - a.y * b.x;
+      }
+      G[i * ld + j] = acc;
+    }
+    __syncthreads();
+    jacobi_eigh(G, V, r, ld, rot, red);
+    Ev = V;
+    Av = G;
   }
-  __syncthreads();
-  // 4. projected eigenproblem
-  jacobi_eigh(G, V, r, ld, rot, red);
-  sort_diag(G, r, ld, order);
-  // 5. C = D B U[:, order[:M]] (coefficients of the new X in the Z columns), Ritz values
+  sort_diag(Av, r, ld, order);
+  // 5. coefficients of the new X in the Z columns, Ritz values
   double2* coef = coefs[t];
-  for (int e = tid; e < n * M; e += nt) {
-    const int l = e / M, m = e % M;
-    const int um = order[m];
-    double2 acc = make_double2(0, 0);
-    for (int j = 0; j < r; ++j) {
-      const double2 a = B[l * ld + j], b = V[j * ld + um];
-      acc.x += a.x * b.x - a.y * b.y;
-      acc.y += a.x * b.y + a.y * b.x;
+  if (chol_ok) {
+    // C = D L⁻ᴴ U[:, order[:M]] (column-parallel back substitution; S is free scratch)
+    for (int m = tid; m < M; m += nt) {
+      const int um = order[m];
+      for (int i = n - 1; i >= 0; --i) {
+        double2 y = Ev[i * ld + um];
+        for (int k = i + 1; k < n; ++k) {
+          const double2 l = G[k * ld + i], v = S[k * ld + m];  // conj(L_ki)·y_k
+          y.x -= l.x * v.x + l.y * v.y;
+          y.y -= l.x * v.y - l.y * v.x;
+        }
+        const double d = G[i * ld + i].x;
+        S[i * ld + m] = make_double2(y.x / d, y.y / d);
+      }
+      for (int i = 0; i < n; ++i) {
+        const double2 y = S[i * ld + m];
+        coef[i * MMAX + m] = make_double2(y.x * dsc[i], y.y * dsc[i]);
+      }
     }
-    coef[l * MMAX + m] = make_double2(acc.x * dsc[l], acc.y * dsc[l]);
+  } else {
+    for (int e = tid; e < n * M; e += nt) {
+      const int l = e / M, m = e % M;
+      const int um = order[m];
+      double2 acc = make_double2(0, 0);
+      for (int j = 0; j < r; ++j) {
+        const double2 a = B[l * ld + j], b = Ev[j * ld + um];
+        acc.x += a.x * b.x - a.y * b.y;
+        acc.y += a.x * b.y + a.y * b.x;
+      }
+      coef[l * MMAX + m] = make_double2(acc.x * dsc[l], acc.y * dsc[l]);
+    }
   }
-  for (int m = tid; m < M; m += nt) s.lam[m] = G[order[m] * ld + order[m]].x;
+  for (int m = tid; m < M; m += nt) s.lam[m] = Av[order[m] * ld + order[m]].x;
   __syncthreads();
   // 6. P coefficients for the active columns: the W and P parts of the Ritz vectors
   const int nPn = (s.nWa + s.nP > 0) ? (M - s.nlocked) : 0;
@@ -154,17 +259,25 @@ __device__ __forceinline__ void finish(TrackState& s, int status) {
 
 __global__ void k_control(TrackState* const* __restrict__ states, double* const* __restrict__ res_parts,
                           int ntracks, IterParams prm) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
   if (t >= ntracks) return;
   TrackState& s = *states[t];
   if (s.done) return;
   const int M = s.M;
   const double* rp = res_parts[t];
-  bool bad = false;
+  // the warp sums the per-chunk ‖R‖² partials, lane 0 runs the control logic
+  double rs[MMAX];
   for (int m = 0; m < M; ++m) {
     double v = 0;
-    for (int c = 0; c < prm.upd_chunks; ++c) v += rp[(size_t)c * MMAX + m];
-    s.resid[m] = sqrt(v);
+    for (int c = lane; c < prm.upd_chunks; c += 32) v += rp[(size_t)c * MMAX + m];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    rs[m] = v;
+  }
+  if (lane != 0) return;
+  bool bad = false;
+  for (int m = 0; m < M; ++m) {
+    s.resid[m] = sqrt(rs[m]);
     if (!isfinite(s.resid[m]) || !isfinite(s.lam[m])) bad = true;
   }
   s.nP = s.nP_next;

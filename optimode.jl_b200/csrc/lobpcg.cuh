@@ -30,8 +30,6 @@ namespace omb {
 
 constexpr int MMAX = 12;         // block columns per track
 constexpr int NMAX = 3 * MMAX;   // Rayleigh–Ritz basis size
-constexpr int GRAM_ROWS = 64;    // rows per Gram tile
-constexpr int UPD_ROWS = 64;     // rows per update tile
 constexpr int GRAM_NT = 256;
 constexpr int UPD_NT = 256;
 constexpr int RR_NT = 128;
@@ -91,69 +89,131 @@ __device__ __forceinline__ int z_phys(const TrackState& s, int M, int l) {
 }
 
 // ---------------------------------------------------------------------------------
-// Gram: partial G = ZᴴZ and S = ZᴴAZ over row tiles (FP64 accumulation).
+// Gram: partial G = ZᴴZ and S = ZᴴAZ, upper triangles only, per CTA row slice.
+// The n columns (padded to even) are cut into 2×2 output blocks; each warp owns
+// gram_ipw blocks and its lanes stride the rows of a staged tile, so shared-memory reads
+// are consecutive (conflict-free) and every lane keeps 4 complex accumulators per block.
+// Tiles are staged with double-buffered cp.async copies (the next tile's loads are in
+// flight while the current one is reduced).  Lane partials are reduced in FP64 at the end.
+// Grid: (row chunks, tracks, block chunks).
+template <typename T> __host__ __device__ constexpr int gram_ipw() { return sizeof(T) == 4 ? 6 : 4; }
+template <typename T> __host__ __device__ constexpr int gram_ipc() { return (GRAM_NT / 32) * gram_ipw<T>(); }
+template <typename T> __host__ __device__ constexpr int gram_rows() { return sizeof(T) == 4 ? 128 : 64; }
+template <typename T> __host__ __device__ constexpr size_t gram_smem(int nbmax) {
+  return 2 /*buffers*/ * 2 /*Z, AZ*/ * (size_t)(2 * nbmax) * gram_rows<T>() * sizeof(cplx<T>);
+}
+
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src));
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::); }
+
 template <typename T>
 __global__ void __launch_bounds__(GRAM_NT) k_gram(const TrackDesc<T>* __restrict__ D, int par, int nchunk) {
   using C = cplx<T>;
+  constexpr int IPW = gram_ipw<T>();
+  constexpr int ROWS = gram_rows<T>();
   const TrackDesc<T>& d = D[blockIdx.y];
   const TrackState& s = *d.st;
   if (s.done) return;
   const int M = d.M;
   const int n = M + s.nWa + s.nP;
+  const int nb = (n + 1) / 2;
+  const int nblk = nb * (nb + 1) / 2;
+  const int item0 = blockIdx.z * gram_ipc<T>();
+  if (item0 >= 2 * nblk) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* Zs = reinterpret_cast<C*>(smem_raw);      // [l][r]
-  C* AZs = Zs + (size_t)n * GRAM_ROWS;
-  __shared__ int phys[NMAX];
-  for (int l = threadIdx.x; l < n; l += GRAM_NT) phys[l] = z_phys(s, M, l);
-  constexpr int QMAX = (2 * NMAX * NMAX + GRAM_NT - 1) / GRAM_NT;
-  double2 acc[QMAX];
+  C* buf = reinterpret_cast<C*>(smem_raw);  // [2 buffers][Z, AZ][2nb columns][ROWS]
+  const int tsz = 2 * nb * ROWS;            // one matrix of one buffer
+  __shared__ int phys[NMAX + 1];
+  __shared__ unsigned char bi_of[NMAX * NMAX / 4 + NMAX], bj_of[NMAX * NMAX / 4 + NMAX];
+  for (int l = threadIdx.x; l < 2 * nb; l += GRAM_NT) phys[l] = l < n ? z_phys(s, M, l) : -1;
+  if (threadIdx.x == 0) {
+    int q = 0;
+    for (int i = 0; i < nb; ++i)
+      for (int j = i; j < nb; ++j) { bi_of[q] = (unsigned char)i; bj_of[q] = (unsigned char)j; ++q; }
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  C acc[IPW][4];
 #pragma unroll
-  for (int i = 0; i < QMAX; ++i) acc[i] = make_double2(0, 0);
-  const int nq = 2 * n * n;
+  for (int i = 0; i < IPW; ++i)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) acc[i][e] = mk<C>(0, 0);
   const long long n2 = d.n2;
-  const C* Y = d.Y[par];
-  const C* AY = d.AY[par];
-  const long long ntile = (n2 + GRAM_ROWS - 1) / GRAM_ROWS;
+  const C* __restrict__ Y = d.Y[par];
+  const C* __restrict__ AY = d.AY[par];
+  const long long ntile = (n2 + ROWS - 1) / ROWS;
   __syncthreads();
-  for (long long tile = blockIdx.x; tile < ntile; tile += nchunk) {
-    const long long r0 = tile * GRAM_ROWS;
-    for (int e = threadIdx.x; e < n * GRAM_ROWS; e += GRAM_NT) {
-      const int l = e / GRAM_ROWS, r = e % GRAM_ROWS;
+  auto stage = [&](long long tile, int b) {
+    C* Zs = buf + (size_t)b * 2 * tsz;
+    C* AZs = Zs + tsz;
+    const long long r0 = tile * ROWS;
+    for (int e = threadIdx.x; e < tsz; e += GRAM_NT) {
+      const int l = e / ROWS, r = e % ROWS;
       const long long row = r0 + r;
-      const size_t off = (size_t)phys[l] * n2 + row;
-      const bool ok = row < n2;
-      Zs[l * GRAM_ROWS + r] = ok ? Y[off] : mk<C>(0, 0);
-      AZs[l * GRAM_ROWS + r] = ok ? AY[off] : mk<C>(0, 0);
+      if (row < n2 && phys[l] >= 0) {
+        const size_t off = (size_t)phys[l] * n2 + row;
+        if constexpr (sizeof(C) == 16) { cp_async16(Zs + e, Y + off); cp_async16(AZs + e, AY + off); }
+        else { cp_async8(Zs + e, Y + off); cp_async8(AZs + e, AY + off); }
+      } else {
+        Zs[e] = mk<C>(0, 0);
+        AZs[e] = mk<C>(0, 0);
+      }
     }
+    cp_async_commit();
+  };
+  int it = 0;
+  if (blockIdx.x < ntile) stage(blockIdx.x, 0);
+  for (long long tile = blockIdx.x; tile < ntile; tile += nchunk, ++it) {
+    if (tile + nchunk < ntile) stage(tile + nchunk, (it + 1) & 1);
+    else cp_async_commit();  // empty group keeps the wait count uniform
+    cp_async_wait_prev();
     __syncthreads();
+    const C* Zs = buf + (size_t)(it & 1) * 2 * tsz;
+    const C* AZs = Zs + tsz;
 #pragma unroll
-    for (int i = 0; i < QMAX; ++i) {
-      const int q = threadIdx.x + i * GRAM_NT;
-      if (q < nq) {
-        const int which = q / (n * n), ab = q % (n * n), a = ab / n, b = ab % n;
-        const C* za = Zs + a * GRAM_ROWS;
-        const C* zb = (which ? AZs : Zs) + b * GRAM_ROWS;
-        double sr = 0, si = 0;
-#pragma unroll 8
-        for (int r = 0; r < GRAM_ROWS; ++r) {
-          const C x = za[r], y = zb[r];
-          // conj(x)·y
-          sr += (double)x.x * y.x + (double)x.y * y.y;
-          si += (double)x.x * y.y - (double)x.y * y.x;
+    for (int i = 0; i < IPW; ++i) {
+      const int itm = item0 + warp * IPW + i;
+      if (itm < 2 * nblk) {
+        const int which = itm / nblk, q = itm % nblk;
+        const C* za = Zs + 2 * bi_of[q] * ROWS;
+        const C* zb = (which ? AZs : Zs) + 2 * bj_of[q] * ROWS;
+#pragma unroll
+        for (int k = 0; k < ROWS / 32; ++k) {
+          const int r = lane + 32 * k;
+          const C a0 = za[r], a1 = za[ROWS + r], b0 = zb[r], b1 = zb[ROWS + r];
+          // conj(a)·b
+          acc[i][0] = acc[i][0] + cmul(cconj(a0), b0);
+          acc[i][1] = acc[i][1] + cmul(cconj(a0), b1);
+          acc[i][2] = acc[i][2] + cmul(cconj(a1), b0);
+          acc[i][3] = acc[i][3] + cmul(cconj(a1), b1);
         }
-        acc[i].x += sr;
-        acc[i].y += si;
       }
     }
     __syncthreads();
   }
   double2* out = d.gram_part + (size_t)blockIdx.x * (2 * NMAX * NMAX);
 #pragma unroll
-  for (int i = 0; i < QMAX; ++i) {
-    const int q = threadIdx.x + i * GRAM_NT;
-    if (q < nq) {
-      const int which = q / (n * n), ab = q % (n * n), a = ab / n, b = ab % n;
-      out[which * NMAX * NMAX + a * NMAX + b] = acc[i];
+  for (int i = 0; i < IPW; ++i) {
+    const int itm = item0 + warp * IPW + i;
+    if (itm >= 2 * nblk) continue;  // warp-uniform
+    const int which = itm / nblk, q = itm % nblk;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      double re = (double)acc[i][e].x, im = (double)acc[i][e].y;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        re += __shfl_xor_sync(0xffffffffu, re, o);
+        im += __shfl_xor_sync(0xffffffffu, im, o);
+      }
+      const int a = 2 * bi_of[q] + (e >> 1), bcol = 2 * bj_of[q] + (e & 1);
+      if (lane == 0 && a < n && bcol < n) out[which * NMAX * NMAX + a * NMAX + bcol] = make_double2(re, im);
     }
   }
 }
@@ -168,7 +228,9 @@ __global__ void __launch_bounds__(RR_NT) k_rr(TrackState* const* __restrict__ st
 // ---------------------------------------------------------------------------------
 // Update: X ← ZC, AX ← AZC, P ← ZCP, AP ← AZCP into the other parity, then
 // R = AX − XΛ, W = P̂_diag R (or R when the MPB preconditioner follows), ‖R‖² partials.
-template <typename T>
+// One thread per vector row (coalesced column reads straight from global memory), the
+// coefficients broadcast from shared memory, MB ≥ M register accumulators per output.
+template <typename T, int MB>
 __global__ void __launch_bounds__(UPD_NT) k_update(const TrackDesc<T>* __restrict__ D, int par, int nchunk,
                                                    int prec_diag) {
   using C = cplx<T>;
@@ -178,108 +240,96 @@ __global__ void __launch_bounds__(UPD_NT) k_update(const TrackDesc<T>* __restric
   const int M = d.M;
   const int n = M + s.nWa + s.nP;
   const int nPn = s.nP_next;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* Zs = reinterpret_cast<C*>(smem_raw);          // [l][r]
-  C* AZs = Zs + (size_t)n * UPD_ROWS;
-  C* Cs = AZs + (size_t)n * UPD_ROWS;               // [l][m], m < M
-  C* CPs = Cs + (size_t)n * MMAX;                   // [l][m], m < nPn
+  __shared__ C Cs[NMAX][MB];
+  __shared__ C CPs[NMAX][MB];
   __shared__ int phys[NMAX];
-  __shared__ T lam[MMAX];
-  __shared__ double rsum[UPD_NT / 32][MMAX];
+  __shared__ T lam[MB];
+  __shared__ double rsum[UPD_NT / 32][MB];
   for (int l = threadIdx.x; l < n; l += UPD_NT) phys[l] = z_phys(s, M, l);
-  for (int e = threadIdx.x; e < n * M; e += UPD_NT) {
-    const int l = e / M, m = e % M;
-    const double2 c = d.coef[l * MMAX + m];
-    Cs[l * MMAX + m] = mk<C>((T)c.x, (T)c.y);
+  for (int e = threadIdx.x; e < n * MB; e += UPD_NT) {
+    const int l = e / MB, m = e % MB;
+    const double2 c = m < M ? d.coef[l * MMAX + m] : make_double2(0, 0);
+    const double2 cp = m < nPn ? d.coef[NMAX * MMAX + l * MMAX + m] : make_double2(0, 0);
+    Cs[l][m] = mk<C>((T)c.x, (T)c.y);
+    CPs[l][m] = mk<C>((T)cp.x, (T)cp.y);
   }
-  for (int e = threadIdx.x; e < n * nPn; e += UPD_NT) {
-    const int l = e / nPn, m = e % nPn;
-    const double2 c = d.coef[NMAX * MMAX + l * MMAX + m];
-    CPs[l * MMAX + m] = mk<C>((T)c.x, (T)c.y);
-  }
-  for (int m = threadIdx.x; m < M; m += UPD_NT) lam[m] = (T)s.lam[m];
+  for (int m = threadIdx.x; m < MB; m += UPD_NT) lam[m] = m < M ? (T)s.lam[m] : T(0);
   if (blockIdx.x == 0 && threadIdx.x == 0) d.st->cur_par = par ^ 1;
-  const long long n2 = d.n2;
-  const C* Y = d.Y[par];
-  const C* AY = d.AY[par];
-  C* Yo = d.Y[par ^ 1];
-  C* AYo = d.AY[par ^ 1];
-  const T k = (T)s.k;
-  // each thread owns fixed (row-in-tile, column) slots: e = tid + j·NT → r = e % ROWS
-  constexpr int SLOTS = (MMAX * UPD_ROWS + UPD_NT - 1) / UPD_NT;
-  double racc[SLOTS];
-#pragma unroll
-  for (int i = 0; i < SLOTS; ++i) racc[i] = 0;
-  const long long ntile = (n2 + UPD_ROWS - 1) / UPD_ROWS;
   __syncthreads();
-  for (long long tile = blockIdx.x; tile < ntile; tile += nchunk) {
-    const long long r0 = tile * UPD_ROWS;
-    for (int e = threadIdx.x; e < n * UPD_ROWS; e += UPD_NT) {
-      const int l = e / UPD_ROWS, r = e % UPD_ROWS;
-      const long long row = r0 + r;
+  const long long n2 = d.n2;
+  const C* __restrict__ Y = d.Y[par];
+  const C* __restrict__ AY = d.AY[par];
+  C* __restrict__ Yo = d.Y[par ^ 1];
+  C* __restrict__ AYo = d.AY[par ^ 1];
+  const T k = (T)s.k;
+  double racc[MB];
+#pragma unroll
+  for (int m = 0; m < MB; ++m) racc[m] = 0;
+  for (long long row = (long long)blockIdx.x * UPD_NT + threadIdx.x; row < n2; row += (long long)nchunk * UPD_NT) {
+    C x[MB], ax[MB];
+#pragma unroll
+    for (int m = 0; m < MB; ++m) { x[m] = mk<C>(0, 0); ax[m] = mk<C>(0, 0); }
+#pragma unroll 4
+    for (int l = 0; l < n; ++l) {
       const size_t off = (size_t)phys[l] * n2 + row;
-      const bool ok = row < n2;
-      Zs[l * UPD_ROWS + r] = ok ? Y[off] : mk<C>(0, 0);
-      AZs[l * UPD_ROWS + r] = ok ? AY[off] : mk<C>(0, 0);
-    }
-    __syncthreads();
-    // X, AX, W and ‖R‖²
+      const C z = Y[off], az = AY[off];
 #pragma unroll
-    for (int i = 0; i < SLOTS; ++i) {
-      const int e = threadIdx.x + i * UPD_NT;
-      if (e < M * UPD_ROWS) {
-        const int r = e % UPD_ROWS, m = e / UPD_ROWS;
-        const long long row = r0 + r;
-        if (row < n2) {
-          C x = mk<C>(0, 0), ax = mk<C>(0, 0);
-          for (int l = 0; l < n; ++l) {
-            const C c = Cs[l * MMAX + m];
-            x = x + cmul(Zs[l * UPD_ROWS + r], c);
-            ax = ax + cmul(AZs[l * UPD_ROWS + r], c);
-          }
-          const C res = ax - x * lam[m];
-          racc[i] += (double)res.x * res.x + (double)res.y * res.y;
-          C w = res;
-          if (prec_diag) {
-            const long long p = row >> 1;
-            const int ix = (int)(p % d.Nx), iy = (int)(p / d.Nx);
-            const T gx = T(freq_index(ix, d.Nx)) * (T)d.inv_dx, gy = T(freq_index(iy, d.Ny)) * (T)d.inv_dy;
-            w = res * (T(d.eps_mean) / (gx * gx + gy * gy + k * k));
-          }
-          Yo[(size_t)m * n2 + row] = x;
-          AYo[(size_t)m * n2 + row] = ax;
-          Yo[(size_t)(M + m) * n2 + row] = w;
+      for (int m = 0; m < MB; ++m) {
+        if (m < M) {
+          const C c = Cs[l][m];
+          x[m] = x[m] + cmul(z, c);
+          ax[m] = ax[m] + cmul(az, c);
         }
       }
     }
-    // P, AP
-    for (int e = threadIdx.x; e < nPn * UPD_ROWS; e += UPD_NT) {
-      const int r = e % UPD_ROWS, m = e / UPD_ROWS;
-      const long long row = r0 + r;
-      if (row < n2) {
-        C p = mk<C>(0, 0), ap = mk<C>(0, 0);
-        for (int l = 0; l < n; ++l) {
-          const C c = CPs[l * MMAX + m];
-          p = p + cmul(Zs[l * UPD_ROWS + r], c);
-          ap = ap + cmul(AZs[l * UPD_ROWS + r], c);
-        }
-        Yo[(size_t)(2 * M + m) * n2 + row] = p;
-        AYo[(size_t)(2 * M + m) * n2 + row] = ap;
+    T pscale = T(1);
+    if (prec_diag) {
+      const long long p = row >> 1;
+      const int ix = (int)(p % d.Nx), iy = (int)(p / d.Nx);
+      const T gx = T(freq_index(ix, d.Nx)) * (T)d.inv_dx, gy = T(freq_index(iy, d.Ny)) * (T)d.inv_dy;
+      pscale = T(d.eps_mean) / (gx * gx + gy * gy + k * k);
+    }
+#pragma unroll
+    for (int m = 0; m < MB; ++m) {
+      if (m < M) {
+        const C res = ax[m] - x[m] * lam[m];
+        racc[m] += (double)res.x * res.x + (double)res.y * res.y;
+        Yo[(size_t)m * n2 + row] = x[m];
+        AYo[(size_t)m * n2 + row] = ax[m];
+        Yo[(size_t)(M + m) * n2 + row] = res * pscale;
       }
     }
-    __syncthreads();
+    if (nPn > 0) {
+#pragma unroll
+      for (int m = 0; m < MB; ++m) { x[m] = mk<C>(0, 0); ax[m] = mk<C>(0, 0); }
+#pragma unroll 4
+      for (int l = M; l < n; ++l) {  // the X rows of CP are zero
+        const size_t off = (size_t)phys[l] * n2 + row;
+        const C z = Y[off], az = AY[off];
+#pragma unroll
+        for (int m = 0; m < MB; ++m) {
+          if (m < nPn) {
+            const C c = CPs[l][m];
+            x[m] = x[m] + cmul(z, c);
+            ax[m] = ax[m] + cmul(az, c);
+          }
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < MB; ++m) {
+        if (m < nPn) {
+          Yo[(size_t)(2 * M + m) * n2 + row] = x[m];
+          AYo[(size_t)(2 * M + m) * n2 + row] = ax[m];
+        }
+      }
+    }
   }
-  // reduce ‖R‖² per column: slots of a thread share m = (tid + i·NT)/ROWS
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  for (int m = 0; m < M; ++m) {
-    double v = 0;
+  const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
 #pragma unroll
-    for (int i = 0; i < SLOTS; ++i) {
-      const int e = threadIdx.x + i * UPD_NT;
-      if (e < M * UPD_ROWS && e / UPD_ROWS == m) v += racc[i];
-    }
+  for (int m = 0; m < MB; ++m) {
+    double v = racc[m];
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (l == 0) rsum[w][m] = v;
+    if (ln == 0) rsum[w][m] = v;
   }
   __syncthreads();
   if (threadIdx.x < M) {
@@ -290,7 +340,8 @@ __global__ void __launch_bounds__(UPD_NT) k_update(const TrackDesc<T>* __restric
 }
 
 // ---------------------------------------------------------------------------------
-// Control (after the update) and Newton (after the HMkH pass): one thread per track.
+// Control (after the update; one warp per track) and Newton (after the HMkH pass; one
+// thread per track).
 __global__ void k_control(TrackState* const* __restrict__ states, double* const* __restrict__ res_parts,
                           int ntracks, IterParams prm);
 __global__ void k_newton(TrackState* const* __restrict__ states, double* const* __restrict__ hmkh_parts,

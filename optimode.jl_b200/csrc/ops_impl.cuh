@@ -24,7 +24,7 @@ using PassKernel = void (*)(const OpUnit<T>*, const cplx<T>*);
 template <typename T>
 static cudaError_t launch_pass(PassKernel<T> kern, dim3 g, int nt, size_t smem, cudaStream_t st,
                                const OpUnit<T>* units, const cplx<T>* tw) {
-  if (smem > 48 * 1024) {
+  if (smem > 32 * 1024) {  // the default limit counts static shared memory too
     cudaError_t e = ensure_smem(reinterpret_cast<const void*>(kern), smem);
     if (e != cudaSuccess) return e;
   }

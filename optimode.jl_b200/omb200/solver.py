@@ -24,13 +24,14 @@ class B200Solver:
 
     * ``precision``: ``"mixed"`` (FP32 iterations, FP64 polish to the tolerance),
       ``"fp64"`` or ``"fp32"`` (tolerance clamped to the FP32 floor).
-    * ``preconditioner``: ``"mpb"`` (``_P!``, two FFT pairs) or ``"diag"`` (⟨ε⟩/|k+G|²).
+    * ``preconditioner``: ``"diag"`` (⟨ε⟩/|k+G|², the default: fewer iterations than the
+      MPB-style one on the benchmark ridges and no FFTs) or ``"mpb"`` (``_P!``, two FFT pairs).
     * ``newton``: ``"inner"`` (Newton steps inside the iteration, one track per band) or
       ``"outer"`` (the reference loop: bands in turn, a converged block eigensolve per step).
     """
 
     precision: str = "mixed"
-    preconditioner: str = "mpb"
+    preconditioner: str = "diag"
     newton: str = "inner"
     device: int = 0
     maxiter: int = 300

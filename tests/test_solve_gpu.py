@@ -117,9 +117,10 @@ def test_batch_matches_single(omb, case):
 def test_warm_start_guess(omb, case):
     grid, ei, km_ref, kv_ref = case
     g = omb.Grid(6.0, 4.0, 24, 16)
-    (km, _), info = omb.solve_k_batch([{"omega": OMEGA0, "eps_inv": ei, "grid": g, "nev": 2,
-                                        "kguess": km_ref[0], "Hguess": kv_ref}], return_info=True)
+    ret, info = omb.solve_k_batch([{"omega": OMEGA0, "eps_inv": ei, "grid": g, "nev": 2,
+                                    "kguess": km_ref[0], "Hguess": kv_ref}], return_info=True)
+    km = ret[0][0]
     assert np.allclose(km, km_ref, rtol=1e-9)
-    (_, _), info0 = omb.solve_k_batch([{"omega": OMEGA0, "eps_inv": ei, "grid": g, "nev": 2}],
-                                      return_info=True)
+    _, info0 = omb.solve_k_batch([{"omega": OMEGA0, "eps_inv": ei, "grid": g, "nev": 2}],
+                                 return_info=True)
     assert info[0]["iterations"].sum() < info0[0]["iterations"].sum()
