@@ -203,7 +203,7 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
     import omb200
-    solver = omb200.B200Solver(precision="mixed", preconditioner="mpb", newton="inner", device=local)
+    solver = omb200.B200Solver(precision="mixed", preconditioner="diag", newton="inner", device=local)
     g, probs = workload(args.instances, seed=rank)
     batch = omb200.Batch(probs, solver)
 

@@ -102,11 +102,13 @@ typedef struct {
   int32_t max_eigsolves;  /* Newton steps per band                            (60)   */
   int32_t maxiter;        /* eigensolver iterations per band and phase        (300)  */
   int32_t precision;      /* OMB_PREC_MIXED / OMB_PREC_FP64 / OMB_PREC_FP32   (MIXED)*/
-  int32_t preconditioner; /* OMB_OP_P (MPB-style) or OMB_OP_P_DIAG           (P)    */
+  int32_t preconditioner; /* OMB_OP_P_DIAG or OMB_OP_P (MPB-style)          (DIAG) */
   int32_t newton;         /* OMB_NEWTON_INNER or OMB_NEWTON_OUTER             (INNER)*/
   int32_t canonicalize;   /* 1: rotate each eigenvector so the largest E component is
                              real and positive (fields.jl:258-260)           (1)    */
   uint64_t seed;          /* random start blocks                              (0)    */
+  int32_t guard_bands;    /* extra block columns beyond the wanted bands of a
+                             Newton track (OMB_NEWTON_INNER)                  (1)    */
 } omb_options;
 
 /* One solve_k problem: the lowest `nev` guided modes of one cell at frequency ω. */

@@ -43,6 +43,8 @@ static int options_from(const omb_options* o, SolveOptions& so) {
   so.prec_diag = o->preconditioner == OMB_OP_P_DIAG;
   so.newton_mode = o->newton == OMB_NEWTON_OUTER ? MODE_NEWTON_OUTER : MODE_NEWTON_INNER;
   so.seed = o->seed;
+  if (o->guard_bands < 0 || o->guard_bands > 4) return fail(OMB_ERR_INVALID_ARG, "guard_bands must be in 0..4");
+  so.guard = o->guard_bands;
   return OMB_OK;
 }
 
@@ -75,6 +77,7 @@ int omb_options_default(omb_options* o) {
   o->newton = OMB_NEWTON_INNER;
   o->canonicalize = 1;
   o->seed = 0;
+  o->guard_bands = 1;
   return OMB_OK;
 }
 
@@ -94,7 +97,8 @@ int omb_batch_create(omb_ctx* ctx, const omb_instance* inst, int n_inst, const o
   b->guesses.resize(n_inst);
   for (int i = 0; i < n_inst; ++i) {
     omb_instance& I = b->inst[i];
-    if (I.nev <= 0 || I.nev > MMAX - 2) return fail(OMB_ERR_INVALID_ARG, "nev must be in 1..10");
+    if (I.nev <= 0 || I.nev + b->so.guard > MMAX)
+      return fail(OMB_ERR_INVALID_ARG, "nev + guard_bands must be in 2..12");
     if (!(I.omega > 0) || !std::isfinite(I.omega)) return fail(OMB_ERR_INVALID_ARG, "omega must be finite and positive");
     if (I.nguess < 0 || (I.nguess > 0 && !I.Hguess)) return fail(OMB_ERR_INVALID_ARG, "bad Hguess/nguess");
     rc = upload_problem(ctx, &I.grid, I.epsinv, b->probs[i]);
@@ -128,7 +132,7 @@ int omb_batch_run(omb_batch* b) {
       // one Newton track per band: block = bands 0..b plus one guard column
       for (int band = 0; band < I.nev; ++band) {
         TrackSpec ts;
-        ts.prob = i; ts.band = band; ts.nbands = 1; ts.M = band + 2; ts.need = band + 1;
+        ts.prob = i; ts.band = band; ts.nbands = 1; ts.M = band + 1 + b->so.guard; ts.need = band + 1;
         ts.mode = MODE_NEWTON_INNER;
         ts.omega2 = I.omega * I.omega; ts.k0 = k0;
         ts.guess = I.Hguess; ts.nguess = I.nguess;

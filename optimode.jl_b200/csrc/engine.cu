@@ -119,7 +119,8 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
       yoff_[t] = ytot;
       ytot += 12 * (size_t)tracks_[t].M * n2;
       soff_[t] = stot;
-      stot += 2 * (size_t)tracks_[t].M * 3 * P.N();
+      // the A pass covers up to [X | W | P] (3M columns) right after a Newton step
+      stot += 3 * (size_t)tracks_[t].M * 3 * P.N();
     }
     OMB_CU(Y.alloc(ytot, st));
     OMB_CU(Sc.alloc(stot, st));
@@ -262,7 +263,7 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
     k_newton<<<cb, 128, 0, st>>>(d_state_ptrs_.p, d_hmkh_ptrs_.p, d_hmkh_nb_.p, nt_, prm);
     if (!ok("k_newton", cudaGetLastError())) return e;
     for (const Group& g : groups_)
-      if (!ok("operator pass", launch_op<T>(OP_M, d_uA[par].p + g.off, g.n, g.Nx, g.Ny, 2 * g.Mmax, ctx_->tw, st))) return e;
+      if (!ok("operator pass", launch_op<T>(OP_M, d_uA[par].p + g.off, g.n, g.Nx, g.Ny, 3 * g.Mmax, ctx_->tw, st))) return e;
     k_gram<T><<<dim3(gram_chunks_, nt_, item_chunks), GRAM_NT, sm_gram, st>>>(d_descs.p, par, gram_chunks_);
     if (!ok("k_gram", cudaGetLastError())) return e;
     k_rr<<<nt_, RR_NT, sm_rr, st>>>(d_state_ptrs_.p, d_gram_ptrs_.p, d_coef_ptrs_.p, nt_, prm);
@@ -370,7 +371,7 @@ int Engine::run() {
 
   // FP32 noise floor of the residual of a unit vector: ~ ε₃₂·√‖M̂‖ (FFT round-off scales
   // with the field's norm, the curl epilogue with |k+G|)
-  const double tauA = std::max(opt_.tol, 64.0 * 5.96e-8 * std::sqrt(normA));
+  const double tauA = std::max(opt_.tol, 16.0 * 5.96e-8 * std::sqrt(normA));
   // result store: one FP64 vector per finished band
   store_off_.assign(nt_, 0);
   snaps_.assign(nt_, {});

@@ -18,6 +18,7 @@ struct SolveOptions {
   bool prec_diag = false;
   int newton_mode = MODE_NEWTON_INNER;
   uint64_t seed = 0;
+  int guard = 1;  // extra block columns of a Newton track
 };
 
 // One eigensolve unit: a Newton band track (solve_k) or a fixed-k block (solve_ω²).

@@ -347,13 +347,13 @@ __global__ void k_newton(TrackState* const* __restrict__ states, double* const* 
   if (!(s.k > 0)) { finish(s, TS_NAN); return; }
   if (prm.last_phase && maxres < prm.tol && fabs(dk) < prm.k_tol) { finish(s, TS_CONVERGED); return; }
   if (s.newton_steps >= prm.max_newton) { finish(s, prm.last_phase ? TS_MAXITER : TS_PHASE_DONE); return; }
-  // k moved: recompute AX (and AW) at the new k, restart the P direction and locking
+  // k moved: recompute AX, AW and AP at the new k (keeping the P direction keeps LOBPCG's
+  // momentum across Newton steps) and restart locking
   const int M = s.M;
-  s.nP = 0;
   s.nlocked = 0;
   s.nWa = M;
   s.op_col0 = 0;
-  s.op_ncol = 2 * M;
+  s.op_ncol = 2 * M + s.nP;
   s.pw_ncol = 0;
   s.resid_best = 1e300;
   s.stall = 0;

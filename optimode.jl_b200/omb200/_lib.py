@@ -131,7 +131,7 @@ class c_options(ctypes.Structure):
                 ("max_eigsolves", ctypes.c_int32), ("maxiter", ctypes.c_int32),
                 ("precision", ctypes.c_int32), ("preconditioner", ctypes.c_int32),
                 ("newton", ctypes.c_int32), ("canonicalize", ctypes.c_int32),
-                ("seed", ctypes.c_uint64)]
+                ("seed", ctypes.c_uint64), ("guard_bands", ctypes.c_int32)]
 
 
 class c_instance(ctypes.Structure):

@@ -36,6 +36,7 @@ class B200Solver:
     device: int = 0
     maxiter: int = 300
     seed: int = 0
+    guard_bands: int = 1
 
     def options(self, k_tol=1e-8, eig_tol=1e-8, max_eigsolves=60, maxiter=None, canonicalize=True):
         o = _lib.c_options()
@@ -49,6 +50,7 @@ class B200Solver:
         o.newton = _NEWTON[self.newton]
         o.canonicalize = 1 if canonicalize else 0
         o.seed = int(self.seed)
+        o.guard_bands = int(self.guard_bands)
         return o
 
 
