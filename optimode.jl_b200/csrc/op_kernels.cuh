@@ -90,6 +90,7 @@ __global__ void __launch_bounds__(NT) k_row_in(const OpUnit<T>* __restrict__ uni
   load_tw(tw, tw_g, NX);
   const T k = (T)(*U.k_dev);
   const C* __restrict__ H = U.in + (size_t)(col + unit_col0(U)) * U.in_cs;
+#pragma unroll
   for (int q = threadIdx.x; q < ROWS * NX; q += NT) {
     const int r = q / NX, ix = q - r * NX, iy = row0 + r;
     C d0 = mk<C>(0, 0), d1 = d0, d2 = d0;
@@ -123,6 +124,7 @@ __global__ void __launch_bounds__(NT) k_row_in(const OpUnit<T>* __restrict__ uni
   __syncthreads();
   fft_lines<C, NX, INV, 3 * ROWS, NT>(s, LS, tw);
   C* __restrict__ D = U.scr + (size_t)col * U.scr_cs;
+#pragma unroll
   for (int q = threadIdx.x; q < ROWS * NX; q += NT) {
     const int r = q / NX, ix = q - r * NX, iy = row0 + r;
     if (iy < Ny) {
@@ -153,6 +155,7 @@ __global__ void __launch_bounds__(NT) k_col(const OpUnit<T>* __restrict__ units,
   const size_t N = (size_t)Nx * NY;
   load_tw(tw, tw_g, NY);
   C* __restrict__ D = U.scr + (size_t)col * U.scr_cs;
+#pragma unroll
   for (int q = threadIdx.x; q < 3 * NY * TX; q += NT) {
     const int t = q % TX, rest = q / TX, iy = rest % NY, c = rest / NY, ix = ix0 + t;
     s[(c * TX + t) * LS + iy] = (ix < Nx) ? D[c * N + (size_t)iy * Nx + ix] : mk<C>(0, 0);
@@ -160,6 +163,7 @@ __global__ void __launch_bounds__(NT) k_col(const OpUnit<T>* __restrict__ units,
   __syncthreads();
   if constexpr (S1 != CS_NONE) fft_lines<C, NY, S1 == CS_INV, 3 * TX, NT>(s, LS, tw);
   if constexpr (PW != PW_NONE) {
+#pragma unroll
     for (int q = threadIdx.x; q < TX * NY; q += NT) {
       const int t = q % TX, iy = q / TX, ix = ix0 + t;
       if (ix < Nx) {
@@ -184,6 +188,7 @@ __global__ void __launch_bounds__(NT) k_col(const OpUnit<T>* __restrict__ units,
     __syncthreads();
   }
   if constexpr (S2 != CS_NONE) fft_lines<C, NY, S2 == CS_INV, 3 * TX, NT>(s, LS, tw);
+#pragma unroll
   for (int q = threadIdx.x; q < 3 * NY * TX; q += NT) {
     const int t = q % TX, rest = q / TX, iy = rest % NY, c = rest / NY, ix = ix0 + t;
     if (ix < Nx) D[c * N + (size_t)iy * Nx + ix] = s[(c * TX + t) * LS + iy];
@@ -210,6 +215,7 @@ __global__ void __launch_bounds__(NT) k_row_out(const OpUnit<T>* __restrict__ un
   const size_t N = (size_t)NX * Ny;
   load_tw(tw, tw_g, NX);
   const C* __restrict__ D = U.scr + (size_t)col * U.scr_cs;
+#pragma unroll
   for (int q = threadIdx.x; q < ROWS * NX; q += NT) {
     const int r = q / NX, ix = q - r * NX, iy = row0 + r;
     const bool ok = iy < Ny;
@@ -224,6 +230,7 @@ __global__ void __launch_bounds__(NT) k_row_out(const OpUnit<T>* __restrict__ un
   const int c0 = unit_col0(U);
   C* __restrict__ O = U.out + (size_t)(col + c0) * U.out_cs;
   double accr = 0.0, acci = 0.0;
+#pragma unroll
   for (int q = threadIdx.x; q < ROWS * NX; q += NT) {
     const int r = q / NX, ix = q - r * NX, iy = row0 + r;
     if (iy >= Ny) continue;

@@ -1,0 +1,163 @@
+# B200Solver: the libomb200 backend for MaxwellEigenmodes' solve_ω² / solve_k.
+#
+# Drop this file into lib/MaxwellEigenmodes/src/solvers/ (include it after gpu.jl) and set
+# OMB200_LIB to the path of libomb200.so.  It adds one concrete AbstractEigensolver with the
+# same method set and keyword contract as GPUSolver (src/solvers/gpu.jl:37-49, 201-242);
+# every device step runs in the C library (include/omb200.h) through `ccall`.
+
+export B200Solver, solve_k_batch
+
+const OMB200_LIB = get(ENV, "OMB200_LIB", "libomb200.so")
+
+# ---- C structs (layouts match include/omb200.h) ------------------------------------
+struct OmbGrid
+    Nx::Int32
+    Ny::Int32
+    Dx::Float64
+    Dy::Float64
+end
+
+struct OmbOptions
+    k_tol::Float64
+    eig_tol::Float64
+    max_eigsolves::Int32
+    maxiter::Int32
+    precision::Int32
+    preconditioner::Int32
+    newton::Int32
+    canonicalize::Int32
+    seed::UInt64
+    guard_bands::Int32
+end
+
+struct OmbInstance
+    grid::OmbGrid
+    omega::Float64
+    epsinv::Ptr{Float64}
+    nev::Int32
+    kguess::Float64
+    Hguess::Ptr{Float64}
+    nguess::Int32
+end
+
+struct OmbResult
+    kmags::Ptr{Float64}
+    evecs::Ptr{Float64}
+    residuals::Ptr{Float64}
+    dw2dk::Ptr{Float64}
+    status::Ptr{Int32}
+    iterations::Ptr{Int32}
+    newton_steps::Ptr{Int32}
+end
+
+const _PREC = Dict(:fp32 => Int32(0), :fp64 => Int32(1), :mixed => Int32(2))
+const _PRECOND = Dict(:mpb => Int32(1), :diag => Int32(2))
+const _NEWTON = Dict(:inner => Int32(0), :outer => Int32(1))
+
+"""
+    B200Solver(; precision=:mixed, preconditioner=:diag, newton=:inner, device=0,
+               maxiter=300, guard_bands=1, logger=NullLogger())
+
+NVIDIA B200 (sm_100a) backend: batched device LOBPCG with Newton steps on k inside the
+iteration, FP32 iterations polished in FP64 to the requested tolerance.
+"""
+struct B200Solver{L<:AbstractLogger} <: AbstractEigensolver{L}
+    logger::L
+    device::Int
+    precision::Symbol
+    preconditioner::Symbol
+    newton::Symbol
+    maxiter::Int
+    guard_bands::Int
+end
+
+B200Solver(; precision=:mixed, preconditioner=:diag, newton=:inner, device=0, maxiter=300,
+    guard_bands=1, logger=NullLogger()) =
+    B200Solver(logger, device, precision, preconditioner, newton, maxiter, guard_bands)
+
+const _OMB_CTX = Dict{Int,Ptr{Cvoid}}()
+
+function _omb_check(rc)
+    rc == 0 && return nothing
+    msg = unsafe_string(ccall((:omb_last_error, OMB200_LIB), Cstring, ()))
+    error("libomb200 (B200Solver) failed with status $rc: $msg")
+end
+
+function _omb_ctx(s::B200Solver)
+    get!(_OMB_CTX, s.device) do
+        h = Ref{Ptr{Cvoid}}(C_NULL)
+        _omb_check(ccall((:omb_ctx_create, OMB200_LIB), Cint, (Cint, Ref{Ptr{Cvoid}}), s.device, h))
+        h[]
+    end
+end
+
+function _omb_options(s::B200Solver; k_tol=1e-8, eig_tol=1e-8, max_eigsolves=60, maxiter=s.maxiter)
+    OmbOptions(k_tol, eig_tol, max_eigsolves, maxiter, _PREC[s.precision], _PRECOND[s.preconditioner],
+        _NEWTON[s.newton], Int32(1), UInt64(0), Int32(s.guard_bands))
+end
+
+_omb_grid(g::Grid{2}) = OmbGrid(g.Nx, g.Ny, g.Δx, g.Δy)
+
+"""
+    solve_k_batch(ωs, ε⁻¹s, grids, s::B200Solver; nevs, k_tol, eig_tol, ...) -> Vector{(kmags, evecs)}
+
+Solve many independent cross-sections in one device run (new API: the reference callers
+loop over `solve_k`).
+"""
+function solve_k_batch(ωs, ε⁻¹s, grids, s::B200Solver; nevs=fill(1, length(ωs)), max_eigsolves=60,
+    maxiter=s.maxiter, k_tol=1e-8, eig_tol=1e-8, kguesses=nothing, Hguesses=nothing)
+    n = length(ωs)
+    eps = [convert(Array{Float64,4}, e) for e in ε⁻¹s]
+    kmags = [zeros(Float64, nevs[i]) for i in 1:n]
+    evecs = [zeros(ComplexF64, 2 * grids[i].Nx * grids[i].Ny, nevs[i]) for i in 1:n]
+    status = [zeros(Int32, nevs[i]) for i in 1:n]
+    guesses = [Hguesses === nothing ? nothing : reduce(hcat, Hguesses[i]) for i in 1:n]
+    GC.@preserve eps kmags evecs status guesses begin
+        insts = [OmbInstance(_omb_grid(grids[i]), ωs[i], pointer(eps[i]), nevs[i],
+            kguesses === nothing ? 0.0 : Float64(first(kguesses[i])),
+            guesses[i] === nothing ? Ptr{Float64}(C_NULL) : Ptr{Float64}(pointer(guesses[i])),
+            guesses[i] === nothing ? 0 : size(guesses[i], 2)) for i in 1:n]
+        res = [OmbResult(pointer(kmags[i]), Ptr{Float64}(pointer(evecs[i])), C_NULL, C_NULL,
+            pointer(status[i]), C_NULL, C_NULL) for i in 1:n]
+        opt = Ref(_omb_options(s; k_tol, eig_tol, max_eigsolves, maxiter))
+        rc = ccall((:omb_solve_k, OMB200_LIB), Cint,
+            (Ptr{Cvoid}, Ptr{OmbInstance}, Cint, Ref{OmbOptions}, Ptr{OmbResult}),
+            _omb_ctx(s), insts, n, opt, res)
+        _omb_check(rc)
+    end
+    return [(kmags[i], [evecs[i][:, j] for j in 1:nevs[i]]) for i in 1:n]
+end
+
+# solve_k(ω, ε⁻¹, grid, solver; ...) with the reference's keyword set (src/solve.jl:182-196)
+function solve_k(ω::T0, ε⁻¹::AbstractArray{T0,4}, grid::Grid{2,T0}, s::B200Solver; nev=1,
+    max_eigsolves=60, maxiter=s.maxiter, k_tol=1e-8, eig_tol=1e-8, log=false, kguess=nothing,
+    Hguess=nothing, f_filter=nothing, overwrite=false) where {T0<:Real}
+    hg = Hguess === nothing ? nothing : [Hguess isa AbstractMatrix ? collect(eachcol(Hguess)) :
+                                         (eltype(Hguess) <: Number ? [Hguess] : collect(Hguess))]
+    out = solve_k_batch([Float64(ω)], [ε⁻¹], [grid], s; nevs=[nev], max_eigsolves, maxiter, k_tol,
+        eig_tol, kguesses=kguess === nothing ? nothing : [kguess], Hguesses=hg)
+    return out[1]
+end
+
+# solve_ω²(ms, solver; nev, maxiter, tol): writes ms.H⃗ and ms.ω² like gpu.jl:201-211
+function solve_ω²(ms::ModeSolver{2,T}, s::B200Solver; nev=1, maxiter=s.maxiter, tol=1e-8, log=false,
+    f_filter=nothing) where {T<:Real}
+    n2 = size(ms.H⃗, 1)
+    evals = zeros(Float64, nev)
+    evecs = zeros(ComplexF64, n2, nev)
+    eps = convert(Array{Float64,4}, ms.M̂.ε⁻¹)
+    guess = convert(Matrix{ComplexF64}, ms.H⃗)
+    opt = Ref(_omb_options(s; eig_tol=tol, maxiter))
+    GC.@preserve eps evals evecs guess begin
+        rc = ccall((:omb_solve_omega2, OMB200_LIB), Cint,
+            (Ptr{Cvoid}, Ref{OmbGrid}, Cdouble, Ptr{Float64}, Cint, Ptr{Float64}, Cint, Ref{OmbOptions},
+             Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Int32}),
+            _omb_ctx(s), Ref(_omb_grid(ms.grid)), ms.M̂.k⃗[3], eps, nev, Ptr{Float64}(pointer(guess)),
+            min(nev, size(guess, 2)), opt, evals, Ptr{Float64}(pointer(evecs)), C_NULL, C_NULL)
+        _omb_check(rc)
+    end
+    evecs_out = [evecs[:, j] for j in 1:nev]
+    ms.H⃗[:, 1:nev] .= evecs
+    ms.ω²[1:nev] .= complex.(evals)
+    return evals, evecs_out
+end

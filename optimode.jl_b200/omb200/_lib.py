@@ -197,3 +197,4 @@ def _declare_batch(lib):
 EXPORTS = EXPORTS + ("omb_batch_create", "omb_batch_run", "omb_batch_results", "omb_batch_stats",
                      "omb_batch_destroy", "omb_profile_apply")
 _DECLARERS.append(_declare_batch)
+
