@@ -87,6 +87,23 @@ int omb_HMkH(omb_ctx* ctx, int precision, const omb_grid* grid, double k,
 int omb_efield(omb_ctx* ctx, int precision, const omb_grid* grid, double k,
                const double* epsinv, const double* H, double* E);
 
+/* Allocation-free FP32 Hout = M̂(k) Hin on caller-owned device memory.  No counterpart in
+ * the reference: it exists for callers that cannot allocate device memory when they need
+ * the operator — code inside a CUDA stream capture (allocations are not capturable), host
+ * frameworks that own the device pool and forbid foreign cudaMalloc/cudaFree, and hot
+ * loops that must not pay allocation latency.  It allocates nothing: its scratch is a
+ * fixed static device array (6 MiB) held by every GPU that loads the library until exit.
+ *   d_epsinv : device Float32 (3, 3, Nx, Ny), symmetric per pixel
+ *   d_H_in, d_H_out : device ComplexF32 (2, Nx, Ny), ncol columns each
+ *   stream   : a cudaStream_t, or NULL for the legacy default stream
+ * Limit: Nx·Ny·ncol ≤ OMB_NOALLOC_MAX_PIXEL_COLUMNS, else OMB_ERR_INVALID_ARG.  All calls
+ * share the scratch, so calls that overlap on the GPU race; the first call on a device
+ * sets up the scratch address and twiddle tables (blocking) and must precede any stream
+ * capture. */
+#define OMB_NOALLOC_MAX_PIXEL_COLUMNS 262144
+int omb_apply_M_noalloc(int32_t Nx, int32_t Ny, double Dx, double Dy, double k, const float* d_epsinv,
+                        int32_t ncol, const void* d_H_in, void* d_H_out, void* stream);
+
 /* ---------------------------------------------------------------------------------
  * Eigensolves
  * --------------------------------------------------------------------------------- */

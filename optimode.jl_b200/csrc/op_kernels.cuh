@@ -33,6 +33,7 @@ template <typename T> struct OpUnit {
   const float2* e32b;     // (xz, yz)         FP32
   const double2* e64;     // 3 double2 per pixel: (xx,yy), (zz,xy), (xz,yz)
   const T* eave;          // 3/tr(ε⁻¹) per pixel
+  const T* e9;            // ε⁻¹ in the reference's (3, 3, Nx, Ny) layout (PW_EPS9 only)
   const double* k_dev;    // wavevector magnitude (device, so the solver can update it)
   double* partial;        // per-(column, row-block) partial sums for RO_KXCT_DOT
   const int* ncol_dev;    // optional device-side column count
@@ -46,7 +47,7 @@ template <typename T> struct OpUnit {
 enum RowIn : int { RI_KXTC = 0, RI_KXINV = 1, RI_ZXTC = 2, RI_LOAD3 = 3 };
 enum RowOut : int { RO_KXCT = 0, RO_KXINVCT = 1, RO_STORE3 = 2, RO_KXCT_DOT = 3 };
 enum ColStep : int { CS_NONE = 0, CS_FWD = 1, CS_INV = 2 };
-enum ColPw : int { PW_NONE = 0, PW_EPS = 1, PW_EAVE = 2 };
+enum ColPw : int { PW_NONE = 0, PW_EPS = 1, PW_EAVE = 2, PW_EPS9 = 3 };
 
 template <typename T> __device__ __forceinline__ void load_eps(const OpUnit<T>& U, size_t p, T e[6]);
 template <> __device__ __forceinline__ void load_eps<float>(const OpUnit<float>& U, size_t p, float e[6]) {
@@ -172,9 +173,15 @@ __global__ void __launch_bounds__(NT) k_col(const OpUnit<T>* __restrict__ units,
         C* a1 = &s[(1 * TX + t) * LS + iy];
         C* a2 = &s[(2 * TX + t) * LS + iy];
         const C d0 = *a0, d1 = *a1, d2 = *a2;
-        if constexpr (PW == PW_EPS) {
+        if constexpr (PW == PW_EPS || PW == PW_EPS9) {
           T e[6];
-          load_eps<T>(U, p, e);
+          if constexpr (PW == PW_EPS) {
+            load_eps<T>(U, p, e);
+          } else {  // the reference's (3, 3, Nx, Ny) column-major layout, 9 entries per pixel
+            const T* m = U.e9 + 9 * p;
+            e[0] = m[0]; e[1] = m[4]; e[2] = m[8];
+            e[3] = T(0.5) * (m[1] + m[3]); e[4] = T(0.5) * (m[2] + m[6]); e[5] = T(0.5) * (m[5] + m[7]);
+          }
           // symmetric ε⁻¹ = [[xx, xy, xz], [xy, yy, yz], [xz, yz, zz]]
           *a0 = d0 * e[0] + d1 * e[3] + d2 * e[4];
           *a1 = d0 * e[3] + d1 * e[1] + d2 * e[5];

@@ -198,3 +198,13 @@ EXPORTS = EXPORTS + ("omb_batch_create", "omb_batch_run", "omb_batch_results", "
                      "omb_batch_destroy", "omb_profile_apply")
 _DECLARERS.append(_declare_batch)
 
+
+def _declare_noalloc(lib):
+    f = lib.omb_apply_M_noalloc
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                  ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+
+
+EXPORTS = EXPORTS + ("omb_apply_M_noalloc",)
+_DECLARERS.append(_declare_noalloc)
