@@ -171,6 +171,22 @@ int omb_solve_omega2(omb_ctx* ctx, const omb_grid* grid, double k, const double*
                      const double* Hguess, int nguess, const omb_options* opt, double* evals,
                      double* evecs, double* residuals, int32_t* status);
 
+/* Adjoint pull-back of one solve_k result: cotangents (k̄, ē) of (kmags, evecs) → ω̄ and
+ * ε̄⁻¹ (and optionally ε̄ = ∂/∂ε).  Replaces the pullback closure of
+ * rrule(solve_k, ω, ε⁻¹, grid, solver) (lib/MaxwellEigenmodes/src/solve.jl:213-289; GPU
+ * variant src/solvers/gpu.jl:292-365).  kmags/evecs are solve_k's outputs (nev values,
+ * nev columns (2, Nx, Ny) ComplexF64); kbar is NULL (zero) or nev values; evbar is NULL
+ * (zero) or nev columns, an all-zero column standing for an AbstractZero band.
+ * epsinv_bar receives (3, 3, Nx, Ny) with the summed (i,j)+(j,i) off-diagonal sensitivity
+ * mirrored into both slots (the ε⁻¹_bar convention, src/grads/solve.jl:490-515); eps_bar,
+ * if non-NULL, receives the same pulled through ε⁻¹ = inv(ε) per pixel
+ * (−Yᵀ ε̄⁻¹ Yᵀ, src/grads/linalg.jl:40-47).  iterations (NULL or nev) receives the adjoint
+ * solver's iteration count per band. */
+int omb_pullback(omb_ctx* ctx, const omb_grid* grid, double omega, const double* epsinv, int nev,
+                 const double* kmags, const double* evecs, const double* kbar, const double* evbar,
+                 const omb_options* opt, double* omega_bar, double* epsinv_bar, double* eps_bar,
+                 int32_t* iterations);
+
 /* ---------------------------------------------------------------------------------
  * Staged batches: the same solve as omb_solve_k split into its host→device, device and
  * device→host parts, so the device part can run (and be timed) with its inputs resident.

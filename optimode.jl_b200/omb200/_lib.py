@@ -208,3 +208,14 @@ def _declare_noalloc(lib):
 
 EXPORTS = EXPORTS + ("omb_apply_M_noalloc",)
 _DECLARERS.append(_declare_noalloc)
+
+
+def _declare_pullback(lib):
+    f = lib.omb_pullback
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_void_p, ctypes.POINTER(c_grid), ctypes.c_double, _dp, ctypes.c_int, _dp, _dp,
+                  _dp, _dp, ctypes.POINTER(c_options), _dp, _dp, _dp, _ip]
+
+
+EXPORTS = EXPORTS + ("omb_pullback",)
+_DECLARERS.append(_declare_pullback)
