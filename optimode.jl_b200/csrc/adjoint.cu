@@ -416,7 +416,7 @@ extern "C" int omb_pullback(omb_ctx* ctx, const omb_grid* grid, double omega, co
       OMB_CU(cudaGetLastError());
       MinresState s0{};
       s0.shift = omega * omega;
-      s0.rtol = 1e-11;
+      s0.rtol = 1e-12;
       s0.maxit = 4 * std::max(O.maxiter, 300);
       OMB_CU(cudaMemcpyAsync(S.p, &s0, sizeof(s0), cudaMemcpyHostToDevice, st));
       k_minres_init<<<nb, ADJ_NT, 0, st>>>(V, eb.p, part.p);

@@ -161,3 +161,37 @@ function solve_ω²(ms::ModeSolver{2,T}, s::B200Solver; nev=1, maxiter=s.maxiter
     ms.ω²[1:nev] .= complex.(evals)
     return evals, evecs_out
 end
+
+# rrule(solve_k, ...) for B200Solver: same contract as src/solve.jl:213-289 — the pullback
+# returns (NoTangent(), ω̄, ε̄⁻¹, NoTangent(), NoTangent()); AbstractZero cotangents (whole
+# tuple or per band) become NULL / all-zero columns.
+function ChainRulesCore.rrule(::typeof(solve_k), ω::T0, ε⁻¹::AbstractArray{T0,4}, grid::Grid{2,T0},
+    s::B200Solver; nev=1, max_eigsolves=60, maxiter=s.maxiter, k_tol=1e-8, eig_tol=1e-8, log=false,
+    kguess=nothing, Hguess=nothing, f_filter=nothing, overwrite=false) where {T0<:Real}
+    kmags, evecs = solve_k(ω, ε⁻¹, grid, s; nev, max_eigsolves, maxiter, k_tol, eig_tol, kguess, Hguess)
+    eps = convert(Array{Float64,4}, ε⁻¹)
+    function b200_solve_k_pullback(ΔΩ)
+        ΔΩ isa AbstractZero && return (NoTangent(), 0.0, zero(eps), NoTangent(), NoTangent())
+        k̄mags, ēvecs = ΔΩ
+        kbar = k̄mags isa AbstractZero ? nothing : [k isa AbstractZero ? 0.0 : Float64(k) for k in k̄mags]
+        n2 = length(first(evecs))
+        ebar = ēvecs isa AbstractZero ? nothing :
+               reduce(hcat, [e isa AbstractZero ? zeros(ComplexF64, n2) : ComplexF64.(e) for e in ēvecs])
+        V = reduce(hcat, evecs)
+        ω̄ = Ref(0.0)
+        ε̄⁻¹ = zeros(Float64, size(eps))
+        opt = Ref(_omb_options(s; k_tol, eig_tol, max_eigsolves, maxiter))
+        GC.@preserve eps kmags V kbar ebar ε̄⁻¹ begin
+            rc = ccall((:omb_pullback, OMB200_LIB), Cint,
+                (Ptr{Cvoid}, Ref{OmbGrid}, Cdouble, Ptr{Float64}, Cint, Ptr{Float64}, Ptr{Float64},
+                 Ptr{Float64}, Ptr{Float64}, Ref{OmbOptions}, Ref{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Int32}),
+                _omb_ctx(s), Ref(_omb_grid(grid)), Float64(ω), eps, nev, kmags, Ptr{Float64}(pointer(V)),
+                kbar === nothing ? Ptr{Float64}(C_NULL) : pointer(kbar),
+                ebar === nothing ? Ptr{Float64}(C_NULL) : Ptr{Float64}(pointer(ebar)),
+                opt, ω̄, ε̄⁻¹, C_NULL, C_NULL)
+            _omb_check(rc)
+        end
+        return (NoTangent(), ω̄[], ε̄⁻¹, NoTangent(), NoTangent())
+    end
+    return ((kmags, evecs), b200_solve_k_pullback)
+end

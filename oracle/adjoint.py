@@ -3,9 +3,12 @@
 Restates ``ME/src/solve.jl:213-289`` (the generic ``rrule(solve_k)``), ``eig_adjt``
 (``ME/src/grads/solve.jl:96-113``), the 2D ``ε⁻¹_bar`` (``ME/src/grads/solve.jl:490-515``),
 ``∇ₖmag_m_n`` (``ME/src/maxwell.jl:560-566``) and the ``sliceinv_3x3`` pull-back
-(``ME/src/grads/linalg.jl:40-47``).  The adjoint linear system is solved to a tight
-tolerance with preconditioned GMRES (the reference's ``my_linsolve``,
-``ME/src/grads/solve.jl:56-66``, uses IterativeSolvers ``gmres`` with ``Pl = P̂``).
+(``ME/src/grads/linalg.jl:40-47``).  The adjoint linear system (the reference's
+``my_linsolve``, ``ME/src/grads/solve.jl:56-66``: IterativeSolvers ``gmres`` with ``Pl = P̂``)
+is solved to rounding here, by a different route on purpose: exactly through the dense
+eigendecomposition of the deflated operator when the system is small, otherwise by MINRES
+on the deflated system with a symmetric positive-definite preconditioner, and in both cases
+the true residual is checked.  Every converged solver returns the same λ.
 """
 
 from __future__ import annotations
@@ -15,27 +18,49 @@ import scipy.sparse.linalg as spla
 
 from .maxwell import Grid, Operator, bfft2, eid, fft2, kx_tc
 
+DENSE_MAX = 4096
 
-def _linsolve(apply_A, b: np.ndarray, apply_P=None, rtol: float = 1e-13, maxiter: int = 2000):
+
+def _deflated_solve(apply_A, x: np.ndarray, b: np.ndarray, apply_P=None, rtol: float = 1e-13):
+    """λ ⟂ x with (A)λ = b on x⊥, b ⟂ x, for Hermitian A (already shifted)."""
     n = b.shape[0]
-    A = spla.LinearOperator((n, n), matvec=apply_A, dtype=np.complex128)
-    Mp = spla.LinearOperator((n, n), matvec=apply_P, dtype=np.complex128) if apply_P else None
-    x, _ = spla.gmres(A, b, M=Mp, rtol=rtol, atol=0.0, restart=60, maxiter=maxiter)
-    return x
+    proj = lambda v: v - x * np.vdot(x, v)
+    if n <= DENSE_MAX:
+        Am = np.stack([apply_A(c) for c in np.eye(n, dtype=np.complex128)], axis=1)
+        Am = 0.5 * (Am + Am.conj().T)
+        Q = np.eye(n, dtype=np.complex128) - np.outer(x, x.conj())
+        w, V = np.linalg.eigh(Q @ Am @ Q)
+        c = V.conj().T @ b
+        # the deflated direction x has eigenvalue 0 and carries no part of b
+        keep = np.abs(c) > 0
+        scale = np.max(np.abs(w))
+        keep &= np.abs(w) > 1e-13 * scale
+        lam = V[:, keep] @ (c[keep] / w[keep])
+    else:
+        Aop = spla.LinearOperator((n, n), matvec=lambda v: proj(apply_A(proj(v))), dtype=np.complex128)
+        Mop = spla.LinearOperator((n, n), matvec=lambda v: proj(apply_P(proj(v))), dtype=np.complex128) \
+            if apply_P else None
+        lam, info = spla.minres(Aop, b, M=Mop, rtol=rtol, maxiter=50 * n)
+    lam = proj(lam)
+    r = np.linalg.norm(proj(apply_A(lam)) - b) / np.linalg.norm(b)
+    if not r < 1e-9:
+        raise RuntimeError(f"adjoint solve did not converge (relative residual {r:.2e})")
+    return lam
 
 
 def eig_adjt(A, alpha: float, x: np.ndarray, alpha_bar: float, x_bar, P=None,
              rtol: float = 1e-13) -> np.ndarray:
     """Adjoint vector λ = λₓ + ᾱ x, (A − αI) λₓ = x̄ − x⟨x, x̄⟩, λₓ ⟂ x.
 
-    ``A`` is a dense matrix or a callable; ``P`` an optional preconditioner callable.
+    ``A`` is a dense matrix or a callable; ``P`` an optional symmetric positive-definite
+    preconditioner callable (used by the iterative route only).
     """
     if x_bar is None or not np.any(x_bar):
         return np.zeros_like(x) if alpha_bar == 0 else alpha_bar * x
     apply = (lambda v: A @ v - alpha * v) if isinstance(A, np.ndarray) else (lambda v: A(v) - alpha * v)
+    x = np.asarray(x, dtype=np.complex128)
     b = x_bar - x * np.vdot(x, x_bar)
-    lx = _linsolve(apply, b, P, rtol=rtol)
-    lx = lx - x * np.vdot(x, lx)
+    lx = _deflated_solve(apply, x, b, P, rtol=rtol)
     return lx + alpha_bar * x
 
 
@@ -65,7 +90,7 @@ def grad_k_mag_m_n(magbar, mbar, nbar, mag, m, n) -> float:
 
 
 def solve_k_pullback(omega: float, epsinv, grid: Grid, kmags, evecs, kbar=None, evbar=None,
-                     precond: str = "mpb", rtol: float = 1e-13):
+                     precond: str = "diag", rtol: float = 1e-14):
     """Pull (k̄, ē) back to (ω̄, ε̄⁻¹) for the modes ``(kmags, evecs)`` of ``solve_k``.
 
     ``kbar``/``evbar`` may be ``None`` (a zero cotangent) as a whole or per band.
