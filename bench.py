@@ -171,9 +171,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
-    ap.add_argument("--case", default="full", choices=["full", "apply", "solve1"],
-                    help="apply / solve1: one operator-apply timing or one single-instance solve "
-                         "(small, self-contained runs for profiling)")
+    ap.add_argument("--case", default="full", choices=["full", "apply", "solve1", "batch"],
+                    help="apply / solve1 / batch: one operator-apply timing, one single-instance "
+                         "solve, or one batched solve of --instances cells (small, self-contained "
+                         "runs for profiling)")
     ap.add_argument("--apply-cells", type=int, default=64)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -183,7 +184,7 @@ def main():
         return run_reference(args, rank)
     if args.case != "full":
         import omb200
-        g, probs = workload(1)
+        g, probs = workload(args.instances if args.case == "batch" else 1)
         if args.case == "apply":
             t = omb200.profile_apply("M", 1.3, probs[0]["eps_inv"], g, NEV, args.apply_cells, reps=args.steps)
             print(json.dumps({"case": "apply", "seconds_per_apply": t, "cells": args.apply_cells, "ncol": NEV}))
@@ -191,8 +192,8 @@ def main():
             b = omb200.Batch(probs, omb200.B200Solver(device=local))
             b.run()
             _, info = b.results(return_info=True, raise_on_failure=False)
-            print(json.dumps({"case": "solve1", **{k: v for k, v in b.stats().items()},
-                              "iterations": info[0]["iterations"].tolist()}))
+            print(json.dumps({"case": args.case, **{k: v for k, v in b.stats().items()},
+                              "iterations": [i["iterations"].tolist() for i in info]}))
             b.close()
         return
 
