@@ -46,7 +46,7 @@ cudaError_t ensure_smem(const void* func, size_t bytes) {
 }
 
 int row_blocks(int Nx, int Ny) {
-  const int rows = rows_for(Nx);
+  const int rows = plan2_a(Nx) ? l2_rows(Nx) : rows_for(Nx);
   return (Ny + rows - 1) / rows;
 }
 
@@ -141,24 +141,33 @@ static int make_twiddles(omb_ctx* ctx) {
 #define OMB_CASE(n) lens.push_back(n);
   OMB_FFT_SIZES(OMB_CASE)
 #undef OMB_CASE
+  // per length L: [exp(-2πi m/L), m < L | TW1 | TW3], the last two for the two-level plan
+  // L = A·B: TW1[k1·B + n2] = W^{n2·k1}, TW3[m2·A + k1] = W^{m2·k1}
   size_t tot = 0;
-  for (int L : lens) tot += L;
+  for (int L : lens) tot += 3 * (size_t)L;
   std::vector<double2> h64(tot);
   std::vector<float2> h32(tot);
   size_t off = 0;
   const double two_pi = 6.283185307179586476925286766559;
+  auto w_of = [&](int m, int L) {
+    m %= L;
+    double c = std::cos(-two_pi * (double)m / (double)L), s = std::sin(-two_pi * (double)m / (double)L);
+    if (m == 0) { c = 1; s = 0; }
+    if (4 * m == L) { c = 0; s = -1; }
+    if (2 * m == L) { c = -1; s = 0; }
+    if (4 * m == 3 * L) { c = 0; s = 1; }
+    return make_double2(c, s);
+  };
   for (int L : lens) {
-    for (int m = 0; m < L; ++m) {
-      // reduce the angle to [0, π/4]-symmetric evaluation for accuracy
-      const double a = -two_pi * (double)m / (double)L;
-      double c = std::cos(a), s = std::sin(a);
-      if (4 * m == L) { c = 0; s = -1; }
-      if (2 * m == L) { c = -1; s = 0; }
-      if (4 * m == 3 * L) { c = 0; s = 1; }
-      h64[off + m] = make_double2(c, s);
-      h32[off + m] = make_float2((float)c, (float)s);
-    }
-    off += L;
+    for (int m = 0; m < L; ++m) h64[off + m] = w_of(m, L);
+    const int A = plan2_a(L), B = A ? L / A : 0;
+    for (int k1 = 0; k1 < A; ++k1)
+      for (int n2 = 0; n2 < B; ++n2) {
+        h64[off + L + k1 * B + n2] = w_of(n2 * k1, L);
+        h64[off + 2 * L + n2 * A + k1] = w_of(n2 * k1, L);
+      }
+    for (int m = 0; m < 3 * L; ++m) h32[off + m] = make_float2((float)h64[off + m].x, (float)h64[off + m].y);
+    off += 3 * (size_t)L;
   }
   void* mem = nullptr;
   OMB_CU(cudaMalloc(&mem, tot * (sizeof(double2) + sizeof(float2))));
@@ -170,7 +179,7 @@ static int make_twiddles(omb_ctx* ctx) {
   for (int L : lens) {
     ctx->tw.f64[L] = d64 + off;
     ctx->tw.f32[L] = d32 + off;
-    off += L;
+    off += 3 * (size_t)L;
   }
   ctx->tw_mem = mem;
   return OMB_OK;

@@ -44,16 +44,17 @@ __host__ __device__ __forceinline__ int freq_index(int i, int n) { return (i < (
 
 // Transverse polarisation basis at one plane wave, kpg = k ẑ − G with G = (gx, gy, 0):
 // mag = |kpg|, n̂ = ẑ×kpg/|ẑ×kpg| (ŷ when kpg ∥ ẑ), m̂ = n̂×kpg/|n̂×kpg|.
-template <typename T> struct Basis { T mag, mx, my, mz, nx, ny; };
+template <typename T> struct Basis { T mag, imag, mx, my, mz, nx, ny; };  // imag = 1/mag
 
 template <typename T>
 __host__ __device__ __forceinline__ Basis<T> basis_at(T k, T gx, T gy) {
   Basis<T> b;
   T p2 = gx * gx + gy * gy;
   b.mag = sqrt(p2 + k * k);
+  const T im = T(1) / b.mag;
+  b.imag = im;
   if (p2 > T(0)) {
     T ip = T(1) / sqrt(p2);
-    T im = T(1) / b.mag;
     b.nx = gy * ip; b.ny = -gx * ip;
     b.mx = -gx * k * ip * im; b.my = -gy * k * ip * im; b.mz = -p2 * ip * im;
   } else {

@@ -1,6 +1,7 @@
 // Size/mode dispatch for the fused operator passes.  Included once per precision.
 #pragma once
 
+#include "op_kernels_2l.cuh"
 #include "ops.h"
 
 namespace omb {
@@ -35,29 +36,54 @@ static cudaError_t launch_pass(PassKernel<T> kern, dim3 g, int nt, size_t smem, 
 template <typename T, int NX>
 static cudaError_t row_in_nx(int mode, const OpUnit<T>* u, int nunits, int Ny, int maxcol,
                              const cplx<T>* tw, cudaStream_t st) {
-  constexpr int ROWS = rows_for(NX);
-  const size_t sm = (NX + 3 * ROWS * (NX + 1)) * sizeof(cplx<T>);
-  const dim3 g((Ny + ROWS - 1) / ROWS, maxcol, nunits);
-  switch (mode) {
-    case RI_KXTC: return launch_pass<T>(k_row_in<T, NX, ROWS, NT_ROW, RI_KXTC, false>, g, NT_ROW, sm, st, u, tw);
-    case RI_KXINV: return launch_pass<T>(k_row_in<T, NX, ROWS, NT_ROW, RI_KXINV, true>, g, NT_ROW, sm, st, u, tw);
-    case RI_ZXTC: return launch_pass<T>(k_row_in<T, NX, ROWS, NT_ROW, RI_ZXTC, false>, g, NT_ROW, sm, st, u, tw);
-    default: return cudaErrorInvalidValue;
+  if constexpr (plan2_a(NX) != 0) {  // two-level register FFT
+    constexpr int G = l2_rows(NX), NT = l2_row_threads(NX);
+    const size_t sm = (size_t)3 * G * l2_row_lstr<cplx<T>, NX>() * sizeof(cplx<T>);
+    const dim3 g((Ny + G - 1) / G, maxcol, nunits);
+    switch (mode) {
+      case RI_KXTC: return launch_pass<T>(k_row_in2<T, NX, RI_KXTC, false>, g, NT, sm, st, u, tw);
+      case RI_KXINV: return launch_pass<T>(k_row_in2<T, NX, RI_KXINV, true>, g, NT, sm, st, u, tw);
+      case RI_ZXTC: return launch_pass<T>(k_row_in2<T, NX, RI_ZXTC, false>, g, NT, sm, st, u, tw);
+      default: return cudaErrorInvalidValue;
+    }
+  } else {
+    constexpr int ROWS = rows_for(NX);
+    const size_t sm = (NX + 3 * ROWS * (NX + 1)) * sizeof(cplx<T>);
+    const dim3 g((Ny + ROWS - 1) / ROWS, maxcol, nunits);
+    switch (mode) {
+      case RI_KXTC: return launch_pass<T>(k_row_in<T, NX, ROWS, NT_ROW, RI_KXTC, false>, g, NT_ROW, sm, st, u, tw);
+      case RI_KXINV: return launch_pass<T>(k_row_in<T, NX, ROWS, NT_ROW, RI_KXINV, true>, g, NT_ROW, sm, st, u, tw);
+      case RI_ZXTC: return launch_pass<T>(k_row_in<T, NX, ROWS, NT_ROW, RI_ZXTC, false>, g, NT_ROW, sm, st, u, tw);
+      default: return cudaErrorInvalidValue;
+    }
   }
 }
 
 template <typename T, int NX>
 static cudaError_t row_out_nx(int mode, const OpUnit<T>* u, int nunits, int Ny, int maxcol,
                               const cplx<T>* tw, cudaStream_t st) {
-  constexpr int ROWS = rows_for(NX);
-  const size_t sm = (NX + 3 * ROWS * (NX + 1)) * sizeof(cplx<T>);
-  const dim3 g((Ny + ROWS - 1) / ROWS, maxcol, nunits);
-  switch (mode) {
-    case RO_KXCT: return launch_pass<T>(k_row_out<T, NX, ROWS, NT_ROW, RO_KXCT, true>, g, NT_ROW, sm, st, u, tw);
-    case RO_KXINVCT: return launch_pass<T>(k_row_out<T, NX, ROWS, NT_ROW, RO_KXINVCT, false>, g, NT_ROW, sm, st, u, tw);
-    case RO_STORE3: return launch_pass<T>(k_row_out<T, NX, ROWS, NT_ROW, RO_STORE3, true>, g, NT_ROW, sm, st, u, tw);
-    case RO_KXCT_DOT: return launch_pass<T>(k_row_out<T, NX, ROWS, NT_ROW, RO_KXCT_DOT, true>, g, NT_ROW, sm, st, u, tw);
-    default: return cudaErrorInvalidValue;
+  if constexpr (plan2_a(NX) != 0) {  // two-level register FFT
+    constexpr int G = l2_rows(NX), NT = l2_row_threads(NX);
+    const size_t sm = (size_t)3 * G * l2_row_lstr<cplx<T>, NX>() * sizeof(cplx<T>);
+    const dim3 g((Ny + G - 1) / G, maxcol, nunits);
+    switch (mode) {
+      case RO_KXCT: return launch_pass<T>(k_row_out2<T, NX, RO_KXCT, true>, g, NT, sm, st, u, tw);
+      case RO_KXINVCT: return launch_pass<T>(k_row_out2<T, NX, RO_KXINVCT, false>, g, NT, sm, st, u, tw);
+      case RO_STORE3: return launch_pass<T>(k_row_out2<T, NX, RO_STORE3, true>, g, NT, sm, st, u, tw);
+      case RO_KXCT_DOT: return launch_pass<T>(k_row_out2<T, NX, RO_KXCT_DOT, true>, g, NT, sm, st, u, tw);
+      default: return cudaErrorInvalidValue;
+    }
+  } else {
+    constexpr int ROWS = rows_for(NX);
+    const size_t sm = (NX + 3 * ROWS * (NX + 1)) * sizeof(cplx<T>);
+    const dim3 g((Ny + ROWS - 1) / ROWS, maxcol, nunits);
+    switch (mode) {
+      case RO_KXCT: return launch_pass<T>(k_row_out<T, NX, ROWS, NT_ROW, RO_KXCT, true>, g, NT_ROW, sm, st, u, tw);
+      case RO_KXINVCT: return launch_pass<T>(k_row_out<T, NX, ROWS, NT_ROW, RO_KXINVCT, false>, g, NT_ROW, sm, st, u, tw);
+      case RO_STORE3: return launch_pass<T>(k_row_out<T, NX, ROWS, NT_ROW, RO_STORE3, true>, g, NT_ROW, sm, st, u, tw);
+      case RO_KXCT_DOT: return launch_pass<T>(k_row_out<T, NX, ROWS, NT_ROW, RO_KXCT_DOT, true>, g, NT_ROW, sm, st, u, tw);
+      default: return cudaErrorInvalidValue;
+    }
   }
 }
 
@@ -67,16 +93,30 @@ enum ColMode : int { CM_M = 0, CM_P = 1, CM_E = 2, CM_FWD = 3, CM_EPSINV = 4 };
 template <typename T, int NY>
 static cudaError_t col_ny(int mode, const OpUnit<T>* u, int nunits, int Nx, int maxcol,
                           const cplx<T>* tw, cudaStream_t st) {
-  constexpr int TX = tx_for<T>(NY);
-  const size_t sm = (NY + 3 * TX * (NY + 1)) * sizeof(cplx<T>);
-  const dim3 g((Nx + TX - 1) / TX, maxcol, nunits);
-  switch (mode) {
-    case CM_M: return launch_pass<T>(k_col<T, NY, TX, NT_COL, CS_FWD, PW_EPS, CS_INV>, g, NT_COL, sm, st, u, tw);
-    case CM_P: return launch_pass<T>(k_col<T, NY, TX, NT_COL, CS_INV, PW_EAVE, CS_FWD>, g, NT_COL, sm, st, u, tw);
-    case CM_E: return launch_pass<T>(k_col<T, NY, TX, NT_COL, CS_FWD, PW_EPS, CS_NONE>, g, NT_COL, sm, st, u, tw);
-    case CM_FWD: return launch_pass<T>(k_col<T, NY, TX, NT_COL, CS_FWD, PW_NONE, CS_NONE>, g, NT_COL, sm, st, u, tw);
-    case CM_EPSINV: return launch_pass<T>(k_col<T, NY, TX, NT_COL, CS_NONE, PW_EPS, CS_INV>, g, NT_COL, sm, st, u, tw);
-    default: return cudaErrorInvalidValue;
+  if constexpr (plan2_a(NY) != 0) {  // two-level register FFT
+    constexpr int TX = l2_tx<T>(NY), NT = l2_col_threads<T>(NY);
+    const size_t sm = (size_t)3 * TX * l2_col_lstr<cplx<T>, NY, TX>() * sizeof(cplx<T>);
+    const dim3 g((Nx + TX - 1) / TX, maxcol, nunits);
+    switch (mode) {
+      case CM_M: return launch_pass<T>(k_col2<T, NY, CS_FWD, PW_EPS, CS_INV>, g, NT, sm, st, u, tw);
+      case CM_P: return launch_pass<T>(k_col2<T, NY, CS_INV, PW_EAVE, CS_FWD>, g, NT, sm, st, u, tw);
+      case CM_E: return launch_pass<T>(k_col2<T, NY, CS_FWD, PW_EPS, CS_NONE>, g, NT, sm, st, u, tw);
+      case CM_FWD: return launch_pass<T>(k_col2<T, NY, CS_FWD, PW_NONE, CS_NONE>, g, NT, sm, st, u, tw);
+      case CM_EPSINV: return launch_pass<T>(k_col2<T, NY, CS_NONE, PW_EPS, CS_INV>, g, NT, sm, st, u, tw);
+      default: return cudaErrorInvalidValue;
+    }
+  } else {
+    constexpr int TX = tx_for<T>(NY);
+    const size_t sm = (NY + 3 * TX * (NY + 1)) * sizeof(cplx<T>);
+    const dim3 g((Nx + TX - 1) / TX, maxcol, nunits);
+    switch (mode) {
+      case CM_M: return launch_pass<T>(k_col<T, NY, TX, NT_COL, CS_FWD, PW_EPS, CS_INV>, g, NT_COL, sm, st, u, tw);
+      case CM_P: return launch_pass<T>(k_col<T, NY, TX, NT_COL, CS_INV, PW_EAVE, CS_FWD>, g, NT_COL, sm, st, u, tw);
+      case CM_E: return launch_pass<T>(k_col<T, NY, TX, NT_COL, CS_FWD, PW_EPS, CS_NONE>, g, NT_COL, sm, st, u, tw);
+      case CM_FWD: return launch_pass<T>(k_col<T, NY, TX, NT_COL, CS_FWD, PW_NONE, CS_NONE>, g, NT_COL, sm, st, u, tw);
+      case CM_EPSINV: return launch_pass<T>(k_col<T, NY, TX, NT_COL, CS_NONE, PW_EPS, CS_INV>, g, NT_COL, sm, st, u, tw);
+      default: return cudaErrorInvalidValue;
+    }
   }
 }
 
