@@ -42,9 +42,6 @@ Engine::Engine(omb_ctx* ctx, std::vector<Problem>* problems, std::vector<TrackSp
     }
     groups_.push_back(g);
   }
-  const int target = 4 * std::max(ctx_->num_sms, 1);
-  gram_chunks_ = std::max(4, std::min(32, (target + nt_ - 1) / std::max(nt_, 1)));
-  upd_chunks_ = std::max(4, std::min(256, (2 * target + nt_ - 1) / std::max(nt_, 1)));
 }
 
 Engine::~Engine() { cudaStreamSynchronize(ctx_->stream); }
@@ -170,8 +167,10 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
     d.AY[1] = base + 9 * M * n2;
     d.st = d_states_.p + t;
     d.coef = coef_.p + (size_t)t * 2 * NMAX * MMAX;
-    d.gram_part = gram_part_.p + (size_t)t * 32 * 2 * NMAX * NMAX;
-    d.res_part = res_part_.p + (size_t)t * 256 * MMAX;
+    if constexpr (std::is_same<T, float>::value) d.coefT = coef32_.p + (size_t)t * 2 * NMAX * MMAX;
+    else d.coefT = d.coef;
+    d.gram_acc = gram_acc_.p + (size_t)t * 2 * NMAX * NMAX;
+    d.res_acc = res_acc_.p + (size_t)t * MMAX;
     d.hmkh_part = hmkh_part_.p + (size_t)t * 2 * 512;
     d.n2 = n2; d.Nx = P.Nx; d.Ny = P.Ny; d.M = M;
     d.hmkh_nb = row_blocks(P.Nx, P.Ny);
@@ -236,19 +235,32 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
   prm.max_newton = opt_.max_newton;
   prm.last_phase = last ? 1 : 0;
   prm.prec_diag = opt_.prec_diag ? 1 : 0;
-  prm.gram_chunks = gram_chunks_;
-  prm.upd_chunks = upd_chunks_;
 
   int Mmax = 1;
   for (const auto& ts : tracks_) Mmax = std::max(Mmax, ts.M);
   const int nmax = 3 * Mmax;
-  const int nbmax = (nmax + 1) / 2;
-  const size_t sm_gram = gram_smem<T>(nbmax);
-  const int item_chunks = (2 * (nbmax * (nbmax + 1) / 2) + gram_ipc<T>() - 1) / gram_ipc<T>();
+  // Gram: as many ring stages as fit in ≈200 KB (2..8); update: a fixed ring
+  const int rg = GramCfg<T>::rows(nmax);
+  const size_t gstage = GramCfg<T>::stage_elems(nmax, rg) * sizeof(cplx<T>);
+  const size_t gred = GramCfg<T>::red_entries(nmax) * sizeof(double2);
+  const int gstages = (int)std::max<size_t>(2, std::min<size_t>(8, (200 * 1024 - 128 - gred) / gstage));
+  const size_t sm_gram = 128 + gstages * gstage + gred;
+  const size_t sm_upd = UpdCfg<T>::smem;
   const size_t sm_rr = 4 * (size_t)NMAX * NMAX * sizeof(double2);
   OMB_CU(set_smem(k_gram<T>, sm_gram));
-  auto update_kernel = Mmax <= 4 ? k_update<T, 4> : (Mmax <= 8 ? k_update<T, 8> : k_update<T, MMAX>);
+  auto update_kernel = Mmax <= 2 ? k_update<T, 2>
+                       : Mmax <= 4 ? k_update<T, 4>
+                       : Mmax <= 6 ? k_update<T, 6>
+                       : Mmax <= 8 ? k_update<T, 8> : k_update<T, MMAX>;
+  OMB_CU(set_smem(update_kernel, sm_upd));
   OMB_CU(set_smem(k_rr, sm_rr));
+  int occ_g = 0, occ_u = 0;
+  OMB_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_g, k_gram<T>, GramCfg<T>::NT, sm_gram));
+  OMB_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_u, update_kernel, UpdCfg<T>::NT, sm_upd));
+  const int grid_g = std::max(1, occ_g) * ctx_->num_sms;
+  const int grid_u = std::max(1, occ_u) * ctx_->num_sms;
+  OMB_CU(gram_acc_.zero());
+  OMB_CU(res_acc_.zero());
   const int cb = (nt_ + 127) / 128;
 
   const char* step = "";
@@ -264,11 +276,15 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
     if (!ok("k_newton", cudaGetLastError())) return e;
     for (const Group& g : groups_)
       if (!ok("operator pass", launch_op<T>(OP_M, d_uA[par].p + g.off, g.n, g.Nx, g.Ny, 3 * g.Mmax, ctx_->tw, st))) return e;
-    k_gram<T><<<dim3(gram_chunks_, nt_, item_chunks), GRAM_NT, sm_gram, st>>>(d_descs.p, par, gram_chunks_);
+    k_live_prefix<<<1, 1024, 0, st>>>(d_state_ptrs_.p, d_n2_.p, nt_, rg, UpdCfg<T>::R, d_pre_.p,
+                                      d_pre_.p + nt_ + 1);
+    if (!ok("k_live_prefix", cudaGetLastError())) return e;
+    k_gram<T><<<grid_g, GramCfg<T>::NT, sm_gram, st>>>(d_descs.p, d_pre_.p, nt_, par, nmax, rg, gstages, d_err_.p);
     if (!ok("k_gram", cudaGetLastError())) return e;
-    k_rr<<<nt_, RR_NT, sm_rr, st>>>(d_state_ptrs_.p, d_gram_ptrs_.p, d_coef_ptrs_.p, nt_, prm);
+    k_rr<<<nt_, RR_NT, sm_rr, st>>>(d_state_ptrs_.p, d_gram_ptrs_.p, d_coef_ptrs_.p, d_coef32_ptrs_.p, nt_, prm);
     if (!ok("k_rr", cudaGetLastError())) return e;
-    update_kernel<<<dim3(upd_chunks_, nt_), UPD_NT, 0, st>>>(d_descs.p, par, upd_chunks_, prm.prec_diag);
+    update_kernel<<<grid_u, UpdCfg<T>::NT, sm_upd, st>>>(d_descs.p, d_pre_.p + nt_ + 1, nt_, par, prm.prec_diag,
+                                                          d_err_.p);
     if (!ok("k_update", cudaGetLastError())) return e;
     k_control<<<(nt_ + 3) / 4, 128, 0, st>>>(d_state_ptrs_.p, d_res_ptrs_.p, nt_, prm);
     ok("k_control", cudaGetLastError());
@@ -314,6 +330,11 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
   cudaGraphDestroy(graph);
   if (rc_out) return rc_out;
   rc_out = download_states();
+  if (rc_out) return rc_out;
+  int perr = 0;
+  OMB_CU(cudaMemcpy(&perr, d_err_.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (perr != PIPE_OK)
+    return fail(OMB_ERR_CUDA, "streaming kernel pipeline wait timed out (code " + std::to_string(perr) + ")");
   last_prec_ = std::is_same<T, float>::value ? 0 : 1;
   return rc_out;
 }
@@ -337,27 +358,39 @@ int Engine::run() {
   }
   OMB_CU(d_states_.alloc(nt_, st));
   OMB_CU(coef_.alloc((size_t)nt_ * 2 * NMAX * MMAX, st));
-  OMB_CU(gram_part_.alloc((size_t)nt_ * 32 * 2 * NMAX * NMAX, st));
-  OMB_CU(res_part_.alloc((size_t)nt_ * 256 * MMAX, st));
+  OMB_CU(coef32_.alloc((size_t)nt_ * 2 * NMAX * MMAX, st));
+  OMB_CU(gram_acc_.alloc((size_t)nt_ * 2 * NMAX * NMAX, st));
+  OMB_CU(res_acc_.alloc((size_t)nt_ * MMAX, st));
   OMB_CU(hmkh_part_.alloc((size_t)nt_ * 2 * 512, st));
-  OMB_CU(gram_part_.zero());
-  OMB_CU(res_part_.zero());
+  OMB_CU(coef_.zero());
+  OMB_CU(coef32_.zero());
+  OMB_CU(d_pre_.alloc(2 * ((size_t)nt_ + 1), st));
+  OMB_CU(d_err_.alloc(1, st));
+  OMB_CU(d_err_.zero());
   std::vector<TrackState*> sp(nt_);
   std::vector<double2*> gp(nt_), cp(nt_);
+  std::vector<float2*> cp32(nt_);
   std::vector<double*> rp(nt_), hp(nt_);
   std::vector<int> hnb(nt_);
+  std::vector<long long> n2s(nt_);
   for (int t = 0; t < nt_; ++t) {
     const Problem& P = (*probs_)[tracks_[t].prob];
     sp[t] = d_states_.p + t;
-    gp[t] = gram_part_.p + (size_t)t * 32 * 2 * NMAX * NMAX;
+    gp[t] = gram_acc_.p + (size_t)t * 2 * NMAX * NMAX;
     cp[t] = coef_.p + (size_t)t * 2 * NMAX * MMAX;
-    rp[t] = res_part_.p + (size_t)t * 256 * MMAX;
+    cp32[t] = coef32_.p + (size_t)t * 2 * NMAX * MMAX;
+    rp[t] = res_acc_.p + (size_t)t * MMAX;
     hp[t] = hmkh_part_.p + (size_t)t * 2 * 512;
     hnb[t] = row_blocks(P.Nx, P.Ny);
+    n2s[t] = 2 * (long long)P.N();
   }
   OMB_CU(d_state_ptrs_.alloc(nt_, st));
   OMB_CU(d_gram_ptrs_.alloc(nt_, st));
   OMB_CU(d_coef_ptrs_.alloc(nt_, st));
+  OMB_CU(d_coef32_ptrs_.alloc(nt_, st));
+  OMB_CU(d_n2_.alloc(nt_, st));
+  OMB_CU(cudaMemcpyAsync(d_coef32_ptrs_.p, cp32.data(), nt_ * sizeof(void*), cudaMemcpyHostToDevice, st));
+  OMB_CU(cudaMemcpyAsync(d_n2_.p, n2s.data(), nt_ * sizeof(long long), cudaMemcpyHostToDevice, st));
   OMB_CU(d_res_ptrs_.alloc(nt_, st));
   OMB_CU(d_hmkh_ptrs_.alloc(nt_, st));
   OMB_CU(d_hmkh_nb_.alloc(nt_, st));

@@ -75,13 +75,17 @@ class Engine {
 
   DevBuf<TrackState> d_states_;
   std::vector<TrackState> host_states_;
-  DevBuf<double2> coef_, gram_part_;
-  DevBuf<double> res_part_, hmkh_part_;
+  DevBuf<double2> coef_, gram_acc_;
+  DevBuf<float2> coef32_;
+  DevBuf<double> res_acc_, hmkh_part_;
   DevBuf<TrackState*> d_state_ptrs_;
   DevBuf<double2*> d_gram_ptrs_, d_coef_ptrs_;
+  DevBuf<float2*> d_coef32_ptrs_;
   DevBuf<double*> d_res_ptrs_, d_hmkh_ptrs_;
   DevBuf<int> d_hmkh_nb_;
-  int gram_chunks_ = 8, upd_chunks_ = 8;
+  DevBuf<long long> d_n2_;
+  DevBuf<int> d_pre_;   // live-tile prefixes: Gram tiles [0, nt], update tiles [nt+1, 2nt+1]
+  DevBuf<int> d_err_;   // first pipeline error of the streaming kernels (0: none)
 
   // block buffers of the current precision (Y/AY per parity, scratch)
   DevBuf<float2> y32_, s32_;

@@ -3,9 +3,40 @@
 
 namespace omb {
 
+__global__ void k_live_prefix(TrackState* const* __restrict__ states, const long long* __restrict__ n2,
+                              int ntracks, int rg, int ru, int* __restrict__ pre_g, int* __restrict__ pre_u) {
+  // one CTA of 1024 threads: inclusive scans of the live tracks' tile counts
+  __shared__ int sg[1024], su[1024];
+  __shared__ int carry[2];
+  const int tid = threadIdx.x;
+  if (tid == 0) { carry[0] = carry[1] = 0; pre_g[0] = 0; pre_u[0] = 0; }
+  __syncthreads();
+  for (int base = 0; base < ntracks; base += 1024) {
+    const int t = base + tid;
+    int vg = 0, vu = 0;
+    if (t < ntracks && !states[t]->done) {
+      vg = (int)((n2[t] + rg - 1) / rg);
+      vu = (int)((n2[t] + ru - 1) / ru);
+    }
+    sg[tid] = vg; su[tid] = vu;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+      const int ag = tid >= off ? sg[tid - off] : 0, au = tid >= off ? su[tid - off] : 0;
+      __syncthreads();
+      sg[tid] += ag; su[tid] += au;
+      __syncthreads();
+    }
+    if (t < ntracks) { pre_g[t + 1] = carry[0] + sg[tid]; pre_u[t + 1] = carry[1] + su[tid]; }
+    __syncthreads();
+    if (tid == 1023) { carry[0] += sg[1023]; carry[1] += su[1023]; }
+    __syncthreads();
+  }
+}
+
 __global__ void __launch_bounds__(RR_NT) k_rr(TrackState* const* __restrict__ states,
-                                               double2* const* __restrict__ gram_parts,
-                                               double2* const* __restrict__ coefs, int ntracks,
+                                               double2* const* __restrict__ gram_accs,
+                                               double2* const* __restrict__ coefs,
+                                               float2* const* __restrict__ coefs32, int ntracks,
                                                IterParams prm) {
   const int t = blockIdx.x;
   if (t >= ntracks) return;
@@ -27,24 +58,22 @@ __global__ void __launch_bounds__(RR_NT) k_rr(TrackState* const* __restrict__ st
   __shared__ int keep[NMAX];
   __shared__ int rank;
   const int tid = threadIdx.x, nt = blockDim.x;
-  const double2* part = gram_parts[t];
-  // 1. sum the per-chunk partial Gram matrices (upper triangles) and mirror them
+  double2* acc = gram_accs[t];
+  // 1. the summed Gram matrices (upper triangles), mirrored; then clear the accumulators
   for (int e = tid; e < 2 * n * n; e += nt) {
     const int which = e / (n * n), ab = e % (n * n), a = ab / n, b = ab % n;
     if (a > b) continue;
-    double2 g = make_double2(0, 0);
-    const double2* pc = part + which * NMAX * NMAX + a * NMAX + b;
-#pragma unroll 4
-    for (int c = 0; c < prm.gram_chunks; ++c) {
-      const double2 x = pc[(size_t)c * (2 * NMAX * NMAX)];
-      g.x += x.x; g.y += x.y;
-    }
+    double2 g = acc[which * NMAX * NMAX + a * NMAX + b];
     double2* Mx = which ? S : G;
     if (a == b) g.y = 0;
     Mx[a * ld + b] = g;
     Mx[b * ld + a] = make_double2(g.x, -g.y);
   }
   __syncthreads();
+  for (int e = tid; e < 2 * n * n; e += nt) {
+    const int which = e / (n * n), ab = e % (n * n), a = ab / n, b = ab % n;
+    if (a <= b) acc[which * NMAX * NMAX + a * NMAX + b] = make_double2(0, 0);
+  }
   // 2. unit-diagonal scaling
   for (int a = tid; a < n; a += nt) {
     const double g = G[a * ld + a].x;
@@ -56,6 +85,7 @@ __global__ void __launch_bounds__(RR_NT) k_rr(TrackState* const* __restrict__ st
     const double f = dsc[a] * dsc[b];
     G[a * ld + b].x *= f; G[a * ld + b].y *= f;
     S[a * ld + b].x *= f; S[a * ld + b].y *= f;
+    B[a * ld + b] = G[a * ld + b];  // the SVQB path needs it after the Cholesky attempt
   }
   __syncthreads();
   // 3. Basis of the Gram metric.  Fast path: Cholesky Gs = L Lᴴ, then the projected
@@ -136,20 +166,10 @@ __global__ void __launch_bounds__(RR_NT) k_rr(TrackState* const* __restrict__ st
     Ev = V;
     Av = B;
   } else {
-    // SVQB: rebuild the scaled Gram matrix (the Cholesky attempt overwrote it)
+    // SVQB: restore the scaled Gram matrix (the Cholesky attempt overwrote it)
     for (int e = tid; e < n * n; e += nt) {
       const int a = e / n, b = e % n;
-      if (a > b) continue;
-      double2 g = make_double2(0, 0);
-      const double2* pc = part + a * NMAX + b;
-      for (int c = 0; c < prm.gram_chunks; ++c) {
-        const double2 x = pc[(size_t)c * (2 * NMAX * NMAX)];
-        g.x += x.x; g.y += x.y;
-      }
-      const double f = dsc[a] * dsc[b];
-      if (a == b) g.y = 0;
-      G[a * ld + b] = make_double2(g.x * f, g.y * f);
-      G[b * ld + a] = make_double2(g.x * f, -g.y * f);
+      G[a * ld + b] = B[a * ld + b];
     }
     __syncthreads();
     jacobi_eigh(G, V, n, ld, rot, red);
@@ -208,6 +228,7 @@ __global__ void __launch_bounds__(RR_NT) k_rr(TrackState* const* __restrict__ st
   sort_diag(Av, r, ld, order);
   // 5. coefficients of the new X in the Z columns, Ritz values
   double2* coef = coefs[t];
+  float2* coef32 = coefs32[t];
   if (chol_ok) {
     // C = D L⁻ᴴ U[:, order[:M]] (column-parallel back substitution; S is free scratch)
     for (int m = tid; m < M; m += nt) {
@@ -225,6 +246,7 @@ __global__ void __launch_bounds__(RR_NT) k_rr(TrackState* const* __restrict__ st
       for (int i = 0; i < n; ++i) {
         const double2 y = S[i * ld + m];
         coef[i * MMAX + m] = make_double2(y.x * dsc[i], y.y * dsc[i]);
+        coef32[i * MMAX + m] = make_float2((float)(y.x * dsc[i]), (float)(y.y * dsc[i]));
       }
     }
   } else {
@@ -238,6 +260,7 @@ __global__ void __launch_bounds__(RR_NT) k_rr(TrackState* const* __restrict__ st
         acc.y += a.x * b.y + a.y * b.x;
       }
       coef[l * MMAX + m] = make_double2(acc.x * dsc[l], acc.y * dsc[l]);
+      coef32[l * MMAX + m] = make_float2((float)(acc.x * dsc[l]), (float)(acc.y * dsc[l]));
     }
   }
   for (int m = tid; m < M; m += nt) s.lam[m] = Av[order[m] * ld + order[m]].x;
@@ -246,7 +269,9 @@ __global__ void __launch_bounds__(RR_NT) k_rr(TrackState* const* __restrict__ st
   const int nPn = (s.nWa + s.nP > 0) ? (M - s.nlocked) : 0;
   for (int e = tid; e < n * nPn; e += nt) {
     const int l = e / nPn, mp = e % nPn;
-    coef[NMAX * MMAX + l * MMAX + mp] = (l < M) ? make_double2(0, 0) : coef[l * MMAX + (s.nlocked + mp)];
+    const double2 c = (l < M) ? make_double2(0, 0) : coef[l * MMAX + (s.nlocked + mp)];
+    coef[NMAX * MMAX + l * MMAX + mp] = c;
+    coef32[NMAX * MMAX + l * MMAX + mp] = make_float2((float)c.x, (float)c.y);
   }
   if (tid == 0) { s.nP_next = nPn; s.rr_n = n; s.rr_rank = r; }
 }
@@ -257,24 +282,19 @@ __device__ __forceinline__ void finish(TrackState& s, int status) {
   s.op_ncol = 0; s.pw_ncol = 0; s.hmkh_ncol = 0;
 }
 
-__global__ void k_control(TrackState* const* __restrict__ states, double* const* __restrict__ res_parts,
+__global__ void k_control(TrackState* const* __restrict__ states, double* const* __restrict__ res_accs,
                           int ntracks, IterParams prm) {
   const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (t >= ntracks) return;
   TrackState& s = *states[t];
   if (s.done) return;
-  const int M = s.M;
-  const double* rp = res_parts[t];
-  // the warp sums the per-chunk ‖R‖² partials, lane 0 runs the control logic
-  double rs[MMAX];
-  for (int m = 0; m < M; ++m) {
-    double v = 0;
-    for (int c = lane; c < prm.upd_chunks; c += 32) v += rp[(size_t)c * MMAX + m];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    rs[m] = v;
-  }
   if (lane != 0) return;
+  const int M = s.M;
+  // ‖R‖² summed by k_update; cleared for the next iteration
+  double* ra = res_accs[t];
+  double rs[MMAX];
+  for (int m = 0; m < M; ++m) { rs[m] = ra[m]; ra[m] = 0.0; }
   bool bad = false;
   for (int m = 0; m < M; ++m) {
     s.resid[m] = sqrt(rs[m]);

@@ -24,14 +24,13 @@
 #pragma once
 
 #include "op_kernels.cuh"
+#include "pipe.cuh"
 #include "smallmat.cuh"
 
 namespace omb {
 
 constexpr int MMAX = 12;         // block columns per track
 constexpr int NMAX = 3 * MMAX;   // Rayleigh–Ritz basis size
-constexpr int GRAM_NT = 256;
-constexpr int UPD_NT = 256;
 constexpr int RR_NT = 128;
 
 enum TrackStatus : int {
@@ -64,8 +63,9 @@ template <typename T> struct TrackDesc {
   cplx<T>* AY[2];       // [AX | AW | AP]
   TrackState* st;
   double2* coef;        // C (NMAX×MMAX) then CP (NMAX×MMAX), row-major [l][m]
-  double2* gram_part;   // [gram_chunks][2·NMAX·NMAX]
-  double* res_part;     // [upd_chunks][MMAX]
+  const cplx<T>* coefT; // the same coefficients in the block's precision
+  double2* gram_acc;    // G then S (NMAX×NMAX each, upper triangles), summed by k_gram
+  double* res_acc;      // ‖R‖² per block column, summed by k_update
   double* hmkh_part;    // row_out partial sums of the HMkH pass
   long long n2;         // vector length (2·Nx·Ny complex)
   int Nx, Ny, M, hmkh_nb;
@@ -78,7 +78,7 @@ struct IterParams {
   double tau_phase;    // phase-A exit residual (FP32 floor) — equals tol in the last phase
   double dk_phase;     // phase-A exit Newton step
   double gram_drop;    // relative Gram eigenvalue floor
-  int maxiter, max_newton, last_phase, prec_diag, gram_chunks, upd_chunks;
+  int maxiter, max_newton, last_phase, prec_diag;
 };
 
 __device__ __forceinline__ int z_phys(const TrackState& s, int M, int l) {
@@ -89,260 +89,446 @@ __device__ __forceinline__ int z_phys(const TrackState& s, int M, int l) {
 }
 
 // ---------------------------------------------------------------------------------
-// Gram: partial G = ZᴴZ and S = ZᴴAZ, upper triangles only, per CTA row slice.
-// The n columns (padded to even) are cut into 2×2 output blocks; each warp owns
-// gram_ipw blocks and its lanes stride the rows of a staged tile, so shared-memory reads
-// are consecutive (conflict-free) and every lane keeps 4 complex accumulators per block.
-// Tiles are staged with double-buffered cp.async copies (the next tile's loads are in
-// flight while the current one is reduced).  Lane partials are reduced in FP64 at the end.
-// Grid: (row chunks, tracks, block chunks).
-template <typename T> __host__ __device__ constexpr int gram_ipw() { return sizeof(T) == 4 ? 6 : 4; }
-template <typename T> __host__ __device__ constexpr int gram_ipc() { return (GRAM_NT / 32) * gram_ipw<T>(); }
-template <typename T> __host__ __device__ constexpr int gram_rows() { return sizeof(T) == 4 ? 128 : 64; }
-template <typename T> __host__ __device__ constexpr size_t gram_smem(int nbmax) {
-  return 2 /*buffers*/ * 2 /*Z, AZ*/ * (size_t)(2 * nbmax) * gram_rows<T>() * sizeof(cplx<T>);
-}
+// Streaming kernels: the tall-skinny Gram products and the Rayleigh–Ritz update.
+//
+// Both stream the row tiles of the live tracks through shared memory with bulk copies
+// (one producer warp, a ring of `stages` buffers guarded by full/empty mbarriers) while
+// the consumer warps compute.  The rows of all live tracks form one sequence of tiles
+// (k_live_prefix counts them after the Newton step of the iteration); CTA b of a 1D grid
+// of X takes tiles [b·T/X, (b+1)·T/X), so the work stays spread over every SM however
+// few tracks are left.  Per-track sums leave each CTA through FP64 atomics into the
+// track's accumulators, which k_rr (Gram) and k_control (‖R‖²) read and clear.
 
-__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src));
+// Tile sequence of one CTA: tiles of R rows of the live tracks, in track order.
+struct TileWalk {
+  const int* pre;      // prefix of tile counts over tracks (pre[t+1] − pre[t] tiles of track t)
+  int ntracks, t;      // current track
+  long long i, end;    // current global tile, one past the last
+  int R;
+  __device__ __forceinline__ void start(const int* pre_, int ntracks_, int R_) {
+    pre = pre_; ntracks = ntracks_; R = R_;
+    const long long T = pre[ntracks];
+    i = (long long)blockIdx.x * T / gridDim.x;
+    end = (long long)(blockIdx.x + 1) * T / gridDim.x;
+    // first track whose tile range contains i (skips tracks with no tiles)
+    int lo = 0, hi = ntracks - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (pre[mid + 1] > i) hi = mid; else lo = mid + 1;
+    }
+    t = lo;
+  }
+  __device__ __forceinline__ bool valid() const { return i < end; }
+  __device__ __forceinline__ long long row0() const { return (i - pre[t]) * (long long)R; }
+  __device__ __forceinline__ void next() {
+    ++i;
+    while (t < ntracks - 1 && pre[t + 1] <= i) ++t;
+  }
+  // is the current tile the last of its track within this CTA's range?
+  __device__ __forceinline__ bool last_of_track() const { return i + 1 >= end || pre[t + 1] <= i + 1; }
+};
+
+// Live-tile prefixes for the Gram (rows per tile rg) and update (ru) kernels.
+__global__ void k_live_prefix(TrackState* const* __restrict__ states, const long long* __restrict__ n2,
+                              int ntracks, int rg, int ru, int* __restrict__ pre_g, int* __restrict__ pre_u);
+
+// ---- Gram ---------------------------------------------------------------------------
+// G = ZᴴZ and S = ZᴴAZ (upper triangles).  The outputs are cut into 4×4 blocks (items);
+// items·SPLIT ≤ 512 consumer threads, each thread owns one item and every SPLIT-th row of
+// a tile (16 complex accumulators), and the SPLIT threads of an item are adjacent lanes,
+// so their partial sums meet in a shuffle reduction (FP64) before the atomics.
+template <typename T> struct GramCfg {
+  static constexpr int NCW = 15;                                 // consumer warps
+  static constexpr int NT = (NCW + 1) * 32;                      // + the producer warp (16 warps: 128 regs)
+  static constexpr int PAD = 16 / (int)sizeof(cplx<T>);          // column pad: 16 bytes
+  // Z columns at [0, n), AZ columns at [n4, n4 + n) with n4 = 4·⌈n/4⌉: the 4×4 blocks read
+  // up to column 2·n4 − 1, so a stage holds 2·4·⌈nmax/4⌉ columns of R + PAD elements
+  static __host__ __device__ constexpr int n4(int n) { return (n + 3) / 4 * 4; }
+  static __host__ __device__ constexpr size_t stage_elems(int nmax, int R) { return (size_t)2 * n4(nmax) * (R + PAD); }
+  // rows per tile: the largest multiple of 64 (≤ 256 FP32, ≤ 128 FP64) whose stage fits in ≈95 KB
+  static __host__ int rows(int nmax) {
+    const int cap = sizeof(T) == 4 ? 256 : 128;
+    int R = (int)(95 * 1024 / (2 * n4(nmax) * sizeof(cplx<T>))) - PAD;
+    R = R / 64 * 64;
+    return R < 64 ? 64 : (R > cap ? cap : R);
+  }
+  // FP64 reduction buffer after the ring: 16 entries per item
+  static __host__ __device__ constexpr int red_entries(int nmax) {
+    return 2 * ((nmax + 3) / 4) * ((nmax + 3) / 4 + 1) / 2 * 16;
+  }
+};
+
+// Named barrier over the first `count` threads of the CTA (the consumer warps).
+__device__ __forceinline__ void bar_sync_count(int id, int count) {
+  asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(count) : "memory");
 }
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src));
+// Item q of a track with nb4 column blocks: matrix (0: G, 1: S) and block (bi ≤ bj).
+__device__ __forceinline__ void gram_item(int q, int nblk, int nb4, int& which, int& bi, int& bj) {
+  which = q / nblk;
+  int r = q - which * nblk;
+  bi = 0;
+  while (r >= nb4 - bi) { r -= nb4 - bi; ++bi; }
+  bj = bi + r;
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::); }
 
 template <typename T>
-__global__ void __launch_bounds__(GRAM_NT) k_gram(const TrackDesc<T>* __restrict__ D, int par, int nchunk) {
+__global__ void __launch_bounds__(GramCfg<T>::NT, 1)
+    k_gram(const TrackDesc<T>* __restrict__ D, const int* __restrict__ pre, int ntracks, int par, int nmax,
+           int R, int stages, int* __restrict__ err) {
   using C = cplx<T>;
-  constexpr int IPW = gram_ipw<T>();
-  constexpr int ROWS = gram_rows<T>();
-  const TrackDesc<T>& d = D[blockIdx.y];
-  const TrackState& s = *d.st;
-  if (s.done) return;
-  const int M = d.M;
-  const int n = M + s.nWa + s.nP;
-  const int nb = (n + 1) / 2;
-  const int nblk = nb * (nb + 1) / 2;
-  const int item0 = blockIdx.z * gram_ipc<T>();
-  if (item0 >= 2 * nblk) return;
+  using Cfg = GramCfg<T>;
+  const int CS = R + Cfg::PAD;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* buf = reinterpret_cast<C*>(smem_raw);  // [2 buffers][Z, AZ][2nb columns][ROWS]
-  const int tsz = 2 * nb * ROWS;            // one matrix of one buffer
-  __shared__ int phys[NMAX + 1];
-  __shared__ unsigned char bi_of[NMAX * NMAX / 4 + NMAX], bj_of[NMAX * NMAX / 4 + NMAX];
-  for (int l = threadIdx.x; l < 2 * nb; l += GRAM_NT) phys[l] = l < n ? z_phys(s, M, l) : -1;
-  if (threadIdx.x == 0) {
-    int q = 0;
-    for (int i = 0; i < nb; ++i)
-      for (int j = i; j < nb; ++j) { bi_of[q] = (unsigned char)i; bj_of[q] = (unsigned char)j; ++q; }
-  }
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw);
+  uint64_t* empty = full + 8;
+  C* stage0 = reinterpret_cast<C*>(smem_raw + 128);
+  const size_t sel = Cfg::stage_elems(nmax, R);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  C acc[IPW][4];
-#pragma unroll
-  for (int i = 0; i < IPW; ++i)
-#pragma unroll
-    for (int e = 0; e < 4; ++e) acc[i][e] = mk<C>(0, 0);
-  const long long n2 = d.n2;
-  const C* __restrict__ Y = d.Y[par];
-  const C* __restrict__ AY = d.AY[par];
-  const long long ntile = (n2 + ROWS - 1) / ROWS;
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < stages; ++q) { mbar_init(&full[q], 1); mbar_init(&empty[q], Cfg::NCW); }
+    mbar_init_fence();
+  }
   __syncthreads();
-  auto stage = [&](long long tile, int b) {
-    C* Zs = buf + (size_t)b * 2 * tsz;
-    C* AZs = Zs + tsz;
-    const long long r0 = tile * ROWS;
-    for (int e = threadIdx.x; e < tsz; e += GRAM_NT) {
-      const int l = e / ROWS, r = e % ROWS;
-      const long long row = r0 + r;
-      if (row < n2 && phys[l] >= 0) {
-        const size_t off = (size_t)phys[l] * n2 + row;
-        if constexpr (sizeof(C) == 16) { cp_async16(Zs + e, Y + off); cp_async16(AZs + e, AY + off); }
-        else { cp_async8(Zs + e, Y + off); cp_async8(AZs + e, AY + off); }
-      } else {
-        Zs[e] = mk<C>(0, 0);
-        AZs[e] = mk<C>(0, 0);
+  TileWalk w;
+  w.start(pre, ntracks, R);
+  if (warp == Cfg::NCW) {
+    // ---- producer: one bulk copy per column segment of the tile
+    int q = 0, fills[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t ph = 0;
+    bool ok = true;
+    for (; w.valid() && ok; w.next()) {
+      const TrackDesc<T>& d = D[w.t];
+      const TrackState& s = *d.st;
+      const int M = d.M, n = M + s.nWa + s.nP;
+      const long long r0 = w.row0();
+      const int rows = (int)min((long long)R, d.n2 - r0);
+      if (lane == 0) {
+        ok = mbar_wait(&empty[q], ph ^ 1);
+        if (ok) mbar_arrive_expect_tx(&full[q], (uint32_t)(2 * n * rows * sizeof(C)));
+        else pipe_fail(err, PIPE_EMPTY_TIMEOUT);
       }
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) break;
+      C* st = stage0 + (size_t)q * sel;
+      const int nz = Cfg::n4(n);
+      for (int c = lane; c < 2 * n; c += 32) {
+        const int l = c < n ? c : c - n;
+        const C* src = (c < n ? d.Y[par] : d.AY[par]) + (size_t)z_phys(s, M, l) * d.n2 + r0;
+        bulk_g2s(st + (size_t)(c < n ? c : nz + l) * CS, src, (uint32_t)(rows * sizeof(C)), &full[q]);
+      }
+      fills[q]++;
+      if (++q == stages) { q = 0; ph ^= 1; }
     }
-    cp_async_commit();
-  };
-  int it = 0;
-  if (blockIdx.x < ntile) stage(blockIdx.x, 0);
-  for (long long tile = blockIdx.x; tile < ntile; tile += nchunk, ++it) {
-    if (tile + nchunk < ntile) stage(tile + nchunk, (it + 1) & 1);
-    else cp_async_commit();  // empty group keeps the wait count uniform
-    cp_async_wait_prev();
-    __syncthreads();
-    const C* Zs = buf + (size_t)(it & 1) * 2 * tsz;
-    const C* AZs = Zs + tsz;
+    // leave no copy in flight: the last fill of every stage has landed
+    if (lane == 0)
+      for (int k = 0; k < stages; ++k)
+        if (fills[k] > 0 && !mbar_wait(&full[k], (uint32_t)((fills[k] - 1) & 1))) pipe_fail(err, PIPE_DRAIN_TIMEOUT);
+    return;
+  }
+  // ---- consumers: thread (item, sub) accumulates one 4×4 block over rows sub, sub+split, …
+  constexpr int NC = Cfg::NCW * 32;
+  const int tid = threadIdx.x;
+  double2* red = reinterpret_cast<double2*>(smem_raw + 128 + (size_t)stages * sel * sizeof(C));
+  for (int e = tid; e < Cfg::red_entries(nmax); e += NC) red[e] = make_double2(0, 0);
+  bar_sync_count(1, NC);
+  int q = 0;
+  uint32_t ph = 0;
+  bool failed = false;
+  C acc[4][4];
+  int cur = -1, items = 0, split = 1, nblk = 0, nb4 = 1, n = 0, item = 0, sub = 0, which = 0, bi = 0, bj = 0;
+  bool active = false;
+  for (; w.valid(); w.next()) {
+    const TrackDesc<T>& d = D[w.t];
+    if (w.t != cur) {  // new track: its item layout
+      cur = w.t;
+      const TrackState& s = *d.st;
+      n = d.M + s.nWa + s.nP;
+      nb4 = (n + 3) / 4;
+      nblk = nb4 * (nb4 + 1) / 2;
+      items = 2 * nblk;
+      split = max(1, NC / items);
+      item = tid / split;
+      sub = tid - item * split;
+      active = item < items;
+      gram_item(active ? item : 0, nblk, nb4, which, bi, bj);
 #pragma unroll
-    for (int i = 0; i < IPW; ++i) {
-      const int itm = item0 + warp * IPW + i;
-      if (itm < 2 * nblk) {
-        const int which = itm / nblk, q = itm % nblk;
-        const C* za = Zs + 2 * bi_of[q] * ROWS;
-        const C* zb = (which ? AZs : Zs) + 2 * bj_of[q] * ROWS;
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int k = 0; k < ROWS / 32; ++k) {
-          const int r = lane + 32 * k;
-          const C a0 = za[r], a1 = za[ROWS + r], b0 = zb[r], b1 = zb[ROWS + r];
-          // conj(a)·b
-          acc[i][0] = acc[i][0] + cmul(cconj(a0), b0);
-          acc[i][1] = acc[i][1] + cmul(cconj(a0), b1);
-          acc[i][2] = acc[i][2] + cmul(cconj(a1), b0);
-          acc[i][3] = acc[i][3] + cmul(cconj(a1), b1);
+        for (int j = 0; j < 4; ++j) acc[i][j] = mk<C>(0, 0);
+    }
+    const int rows = (int)min((long long)R, d.n2 - w.row0());
+    bool ok = failed ? false : mbar_wait(&full[q], ph);
+    ok = __all_sync(0xffffffffu, ok);
+    if (!ok && !failed) { pipe_fail(err, PIPE_FULL_TIMEOUT); failed = true; }
+    if (!failed) {
+      if (active) {
+        const C* st = stage0 + (size_t)q * sel;
+        const C* za = st + (size_t)(4 * bi) * CS;
+        const C* zb = st + (size_t)((which ? Cfg::n4(n) : 0) + 4 * bj) * CS;
+#pragma unroll 2
+        for (int r = sub; r < rows; r += split) {
+          C a[4], b[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) { a[i] = za[i * CS + r]; b[i] = zb[i * CS + r]; }
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {  // conj(a)·b
+              acc[i][j].x += a[i].x * b[j].x + a[i].y * b[j].y;
+              acc[i][j].y += a[i].x * b[j].y - a[i].y * b[j].x;
+            }
         }
       }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[q]);
     }
-    __syncthreads();
-  }
-  double2* out = d.gram_part + (size_t)blockIdx.x * (2 * NMAX * NMAX);
+    if (++q == stages) { q = 0; ph ^= 1; }
+    if (w.last_of_track()) {
+      // the split partial sums of each item meet in shared memory (FP64), then one global
+      // atomic per matrix entry
+      if (active) {
 #pragma unroll
-  for (int i = 0; i < IPW; ++i) {
-    const int itm = item0 + warp * IPW + i;
-    if (itm >= 2 * nblk) continue;  // warp-uniform
-    const int which = itm / nblk, q = itm % nblk;
+        for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      double re = (double)acc[i][e].x, im = (double)acc[i][e].y;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        re += __shfl_xor_sync(0xffffffffu, re, o);
-        im += __shfl_xor_sync(0xffffffffu, im, o);
+          for (int j = 0; j < 4; ++j) {
+            atomicAdd(&red[item * 16 + i * 4 + j].x, (double)acc[i][j].x);
+            atomicAdd(&red[item * 16 + i * 4 + j].y, (double)acc[i][j].y);
+          }
       }
-      const int a = 2 * bi_of[q] + (e >> 1), bcol = 2 * bj_of[q] + (e & 1);
-      if (lane == 0 && a < n && bcol < n) out[which * NMAX * NMAX + a * NMAX + bcol] = make_double2(re, im);
+      bar_sync_count(1, NC);
+      for (int e = tid; e < items * 16; e += NC) {
+        int wh, ei, ej;
+        gram_item(e >> 4, nblk, nb4, wh, ei, ej);
+        const int a = 4 * ei + ((e >> 2) & 3), b = 4 * ej + (e & 3);
+        const double2 v = red[e];
+        if (!failed && a < n && b < n && a <= b) {
+          double2* g = d.gram_acc + (size_t)wh * NMAX * NMAX + (size_t)a * NMAX + b;
+          atomicAdd(&g->x, v.x);
+          atomicAdd(&g->y, v.y);
+        }
+        red[e] = make_double2(0, 0);
+      }
+      bar_sync_count(1, NC);
+      cur = -1;
     }
   }
 }
 
-// ---------------------------------------------------------------------------------
-// Rayleigh–Ritz: one CTA per track.
-__global__ void __launch_bounds__(RR_NT) k_rr(TrackState* const* __restrict__ states,
-                                               double2* const* __restrict__ gram_parts,
-                                               double2* const* __restrict__ coefs, int ntracks,
-                                               IterParams prm);
+// ---- Update -----------------------------------------------------------------------
+// X ← ZC, AX ← AZC, P ← ZCP, AP ← AZCP into the other parity, then R = AX − XΛ,
+// W = P̂_diag R (or R when the MPB preconditioner follows) and ‖R‖².  One consumer thread
+// per tile row; a stage holds LG columns of Z and AZ for the tile plus the matching rows
+// of C and CP (in the block's precision), so the coefficients follow the tile's track.
+static_assert(MMAX == 12, "k_update dispatches M = 1..12");
+template <typename T> struct UpdCfg {
+  // rows per tile = consumer threads; with the producer warp 16 warps (FP32, 128 registers)
+  // or 9 warps (FP64, whose M ≤ 6 tile bodies need ≈170 registers)
+  static constexpr int R = sizeof(T) == 4 ? 480 : 256;
+  static constexpr int LG = sizeof(T) == 4 ? 4 : 2;      // columns per stage
+  static constexpr int NCW = R / 32;
+  static constexpr int NT = (NCW + 1) * 32;
+  static constexpr int STAGES = 6;
+  // stage: Z[LG][R], AZ[LG][R], C[LG][MMAX], CP[LG][MMAX]
+  static constexpr size_t stage_elems = (size_t)2 * LG * R + (size_t)2 * LG * MMAX;
+  static constexpr size_t smem = 128 + STAGES * stage_elems * sizeof(cplx<T>);
+};
 
-// ---------------------------------------------------------------------------------
-// Update: X ← ZC, AX ← AZC, P ← ZCP, AP ← AZCP into the other parity, then
-// R = AX − XΛ, W = P̂_diag R (or R when the MPB preconditioner follows), ‖R‖² partials.
-// One thread per vector row (coalesced column reads straight from global memory), the
-// coefficients broadcast from shared memory, MB ≥ M register accumulators per output.
-template <typename T, int MB>
-__global__ void __launch_bounds__(UPD_NT) k_update(const TrackDesc<T>* __restrict__ D, int par, int nchunk,
-                                                   int prec_diag) {
+// One tile of the update for a track with M block columns (compile-time, so the column
+// loops unroll without per-column branches).  Entries of CP beyond nP_next may be stale;
+// they only reach P columns that are not stored.
+template <typename T, int M, int MB>
+__device__ __forceinline__ void update_tile(const TrackDesc<T>& d, const TrackState& s, long long r0, int rows,
+                                            int par, int prec_diag, const cplx<T>* stage0, uint64_t* full,
+                                            uint64_t* empty, int& q, uint32_t& ph, bool& failed,
+                                            double (&racc)[MB], int* err) {
   using C = cplx<T>;
-  const TrackDesc<T>& d = D[blockIdx.y];
-  const TrackState& s = *d.st;
-  if (s.done) return;
-  const int M = d.M;
-  const int n = M + s.nWa + s.nP;
-  const int nPn = s.nP_next;
-  __shared__ C Cs[NMAX][MB];
-  __shared__ C CPs[NMAX][MB];
-  __shared__ int phys[NMAX];
-  __shared__ T lam[MB];
-  __shared__ double rsum[UPD_NT / 32][MB];
-  for (int l = threadIdx.x; l < n; l += UPD_NT) phys[l] = z_phys(s, M, l);
-  for (int e = threadIdx.x; e < n * MB; e += UPD_NT) {
-    const int l = e / MB, m = e % MB;
-    const double2 c = m < M ? d.coef[l * MMAX + m] : make_double2(0, 0);
-    const double2 cp = m < nPn ? d.coef[NMAX * MMAX + l * MMAX + m] : make_double2(0, 0);
-    Cs[l][m] = mk<C>((T)c.x, (T)c.y);
-    CPs[l][m] = mk<C>((T)cp.x, (T)cp.y);
-  }
-  for (int m = threadIdx.x; m < MB; m += UPD_NT) lam[m] = m < M ? (T)s.lam[m] : T(0);
-  if (blockIdx.x == 0 && threadIdx.x == 0) d.st->cur_par = par ^ 1;
-  __syncthreads();
-  const long long n2 = d.n2;
-  const C* __restrict__ Y = d.Y[par];
-  const C* __restrict__ AY = d.AY[par];
-  C* __restrict__ Yo = d.Y[par ^ 1];
-  C* __restrict__ AYo = d.AY[par ^ 1];
-  const T k = (T)s.k;
-  double racc[MB];
+  using Cfg = UpdCfg<T>;
+  constexpr int R = Cfg::R, LG = Cfg::LG, S = Cfg::STAGES;
+  const int r = threadIdx.x, lane = r & 31;
+  const int n = M + s.nWa + s.nP, nPn = s.nP_next;
+  C x[M], ax[M], p[M], ap[M];
 #pragma unroll
-  for (int m = 0; m < MB; ++m) racc[m] = 0;
-  for (long long row = (long long)blockIdx.x * UPD_NT + threadIdx.x; row < n2; row += (long long)nchunk * UPD_NT) {
-    C x[MB], ax[MB];
+  for (int m = 0; m < M; ++m) x[m] = ax[m] = p[m] = ap[m] = mk<C>(0, 0);
+  for (int l0 = 0; l0 < n; l0 += LG) {
+    bool ok = failed ? false : mbar_wait(&full[q], ph);
+    ok = __all_sync(0xffffffffu, ok);
+    if (!ok && !failed) { pipe_fail(err, PIPE_FULL_TIMEOUT); failed = true; }
+    if (!failed) {
+      const C* st = stage0 + (size_t)q * Cfg::stage_elems;
+      const C* Cs = st + 2 * LG * R;
+      const C* CPs = Cs + LG * MMAX;
+      if (r < rows) {
 #pragma unroll
-    for (int m = 0; m < MB; ++m) { x[m] = mk<C>(0, 0); ax[m] = mk<C>(0, 0); }
-#pragma unroll 4
-    for (int l = 0; l < n; ++l) {
-      const size_t off = (size_t)phys[l] * n2 + row;
-      const C z = Y[off], az = AY[off];
+        for (int j = 0; j < LG; ++j) {
+          if (l0 + j < n) {
+            const C z = st[j * R + r], az = st[(LG + j) * R + r];
 #pragma unroll
-      for (int m = 0; m < MB; ++m) {
-        if (m < M) {
-          const C c = Cs[l][m];
-          x[m] = x[m] + cmul(z, c);
-          ax[m] = ax[m] + cmul(az, c);
+            for (int m = 0; m < M; ++m) {
+              const C c = Cs[j * MMAX + m];
+              x[m] = x[m] + cmul(z, c);
+              ax[m] = ax[m] + cmul(az, c);
+            }
+            if (l0 + j >= M) {  // the X rows of CP are zero
+#pragma unroll
+              for (int m = 0; m < M; ++m) {
+                const C c = CPs[j * MMAX + m];
+                p[m] = p[m] + cmul(z, c);
+                ap[m] = ap[m] + cmul(az, c);
+              }
+            }
+          }
         }
       }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[q]);
     }
+    if (++q == S) { q = 0; ph ^= 1; }
+  }
+  if (failed) return;
+  if (r0 == 0 && r == 0) d.st->cur_par = par ^ 1;
+  if (r < rows) {
+    const long long row = r0 + r, n2 = d.n2;
+    C* __restrict__ Yo = d.Y[par ^ 1];
+    C* __restrict__ AYo = d.AY[par ^ 1];
     T pscale = T(1);
     if (prec_diag) {
-      const long long p = row >> 1;
-      const int ix = (int)(p % d.Nx), iy = (int)(p / d.Nx);
+      const long long pix = row >> 1;
+      const int ix = (int)(pix % d.Nx), iy = (int)(pix / d.Nx);
+      const T k = (T)s.k;
       const T gx = T(freq_index(ix, d.Nx)) * (T)d.inv_dx, gy = T(freq_index(iy, d.Ny)) * (T)d.inv_dy;
       pscale = T(d.eps_mean) / (gx * gx + gy * gy + k * k);
     }
 #pragma unroll
-    for (int m = 0; m < MB; ++m) {
-      if (m < M) {
-        const C res = ax[m] - x[m] * lam[m];
-        racc[m] += (double)res.x * res.x + (double)res.y * res.y;
-        Yo[(size_t)m * n2 + row] = x[m];
-        AYo[(size_t)m * n2 + row] = ax[m];
-        Yo[(size_t)(M + m) * n2 + row] = res * pscale;
-      }
+    for (int m = 0; m < M; ++m) {
+      const C res = ax[m] - x[m] * (T)s.lam[m];
+      racc[m] += (double)res.x * res.x + (double)res.y * res.y;
+      Yo[(size_t)m * n2 + row] = x[m];
+      AYo[(size_t)m * n2 + row] = ax[m];
+      Yo[(size_t)(M + m) * n2 + row] = res * pscale;
     }
-    if (nPn > 0) {
 #pragma unroll
-      for (int m = 0; m < MB; ++m) { x[m] = mk<C>(0, 0); ax[m] = mk<C>(0, 0); }
-#pragma unroll 4
-      for (int l = M; l < n; ++l) {  // the X rows of CP are zero
-        const size_t off = (size_t)phys[l] * n2 + row;
-        const C z = Y[off], az = AY[off];
-#pragma unroll
-        for (int m = 0; m < MB; ++m) {
-          if (m < nPn) {
-            const C c = CPs[l][m];
-            x[m] = x[m] + cmul(z, c);
-            ax[m] = ax[m] + cmul(az, c);
-          }
-        }
-      }
-#pragma unroll
-      for (int m = 0; m < MB; ++m) {
-        if (m < nPn) {
-          Yo[(size_t)(2 * M + m) * n2 + row] = x[m];
-          AYo[(size_t)(2 * M + m) * n2 + row] = ax[m];
-        }
+    for (int m = 0; m < M; ++m) {
+      if (m < nPn) {
+        Yo[(size_t)(2 * M + m) * n2 + row] = p[m];
+        AYo[(size_t)(2 * M + m) * n2 + row] = ap[m];
       }
     }
   }
-  const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
-#pragma unroll
-  for (int m = 0; m < MB; ++m) {
-    double v = racc[m];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (ln == 0) rsum[w][m] = v;
+}
+
+// MB: the largest block size of the launch (the tile bodies for M ≤ MB are compiled in).
+template <typename T, int MB>
+__global__ void __launch_bounds__(UpdCfg<T>::NT, 1)
+    k_update(const TrackDesc<T>* __restrict__ D, const int* __restrict__ pre, int ntracks, int par,
+             int prec_diag, int* __restrict__ err) {
+  using C = cplx<T>;
+  using Cfg = UpdCfg<T>;
+  constexpr int R = Cfg::R, LG = Cfg::LG, S = Cfg::STAGES;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw);
+  uint64_t* empty = full + 8;
+  C* stage0 = reinterpret_cast<C*>(smem_raw + 128);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < S; ++q) { mbar_init(&full[q], 1); mbar_init(&empty[q], Cfg::NCW); }
+    mbar_init_fence();
   }
   __syncthreads();
-  if (threadIdx.x < M) {
-    double v = 0;
-    for (int i = 0; i < UPD_NT / 32; ++i) v += rsum[i][threadIdx.x];
-    d.res_part[(size_t)blockIdx.x * MMAX + threadIdx.x] = v;
+  TileWalk w;
+  w.start(pre, ntracks, R);
+  if (warp == Cfg::NCW) {
+    // ---- producer
+    int q = 0, fills[S] = {};
+    uint32_t ph = 0;
+    bool ok = true;
+    for (; w.valid() && ok; w.next()) {
+      const TrackDesc<T>& d = D[w.t];
+      const TrackState& s = *d.st;
+      if (s.done) continue;  // finished in k_rr after the tiles were counted
+      const int M = d.M, n = M + s.nWa + s.nP;
+      const long long r0 = w.row0();
+      const int rows = (int)min((long long)R, d.n2 - r0);
+      for (int l0 = 0; l0 < n && ok; l0 += LG) {
+        const int nl = min(LG, n - l0);
+        if (lane == 0) {
+          ok = mbar_wait(&empty[q], ph ^ 1);
+          if (ok)
+            mbar_arrive_expect_tx(&full[q], (uint32_t)((2 * nl * rows + 2 * nl * MMAX) * sizeof(C)));
+          else
+            pipe_fail(err, PIPE_EMPTY_TIMEOUT);
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) break;
+        C* st = stage0 + (size_t)q * Cfg::stage_elems;
+        if (lane < 2 * nl) {
+          const int j = lane % nl, l = l0 + j;
+          const C* src = (lane < nl ? d.Y[par] : d.AY[par]) + (size_t)z_phys(s, M, l) * d.n2 + r0;
+          bulk_g2s(st + (size_t)(lane < nl ? j : LG + j) * R, src, (uint32_t)(rows * sizeof(C)), &full[q]);
+        } else if (lane == 2 * LG) {
+          bulk_g2s(st + 2 * LG * R, d.coefT + (size_t)l0 * MMAX, (uint32_t)(nl * MMAX * sizeof(C)), &full[q]);
+        } else if (lane == 2 * LG + 1) {
+          bulk_g2s(st + 2 * LG * R + LG * MMAX, d.coefT + (size_t)NMAX * MMAX + (size_t)l0 * MMAX,
+                   (uint32_t)(nl * MMAX * sizeof(C)), &full[q]);
+        }
+        fills[q]++;
+        if (++q == S) { q = 0; ph ^= 1; }
+      }
+    }
+    if (lane == 0)
+      for (int k = 0; k < S; ++k)
+        if (fills[k] > 0 && !mbar_wait(&full[k], (uint32_t)((fills[k] - 1) & 1))) pipe_fail(err, PIPE_DRAIN_TIMEOUT);
+    return;
+  }
+  // ---- consumers: thread r owns row row0 + r of each tile
+  int q = 0;
+  uint32_t ph = 0;
+  bool failed = false;
+  double racc[MB];
+#pragma unroll
+  for (int m = 0; m < MB; ++m) racc[m] = 0;
+  for (; w.valid(); w.next()) {
+    const TrackDesc<T>& d = D[w.t];
+    const TrackState& s = *d.st;
+    if (s.done) continue;
+    const long long r0 = w.row0();
+    const int rows = (int)min((long long)R, d.n2 - r0);
+    switch (d.M) {
+#define OMB_UPD_CASE(MM)                                                                                \
+  case MM:                                                                                              \
+    if constexpr (MM <= MB)                                                                             \
+      update_tile<T, (MM <= MB ? MM : 1), MB>(d, s, r0, rows, par, prec_diag, stage0, full, empty, q, ph, \
+                                              failed, racc, err);                                       \
+    break;
+      OMB_UPD_CASE(1) OMB_UPD_CASE(2) OMB_UPD_CASE(3) OMB_UPD_CASE(4) OMB_UPD_CASE(5) OMB_UPD_CASE(6)
+      OMB_UPD_CASE(7) OMB_UPD_CASE(8) OMB_UPD_CASE(9) OMB_UPD_CASE(10) OMB_UPD_CASE(11) OMB_UPD_CASE(12)
+#undef OMB_UPD_CASE
+      default: break;
+    }
+    if (w.last_of_track()) {
+#pragma unroll
+      for (int m = 0; m < MB; ++m) {
+        double v = racc[m];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0 && m < d.M && !failed) atomicAdd(d.res_acc + m, v);
+        racc[m] = 0;
+      }
+    }
   }
 }
 
 // ---------------------------------------------------------------------------------
+// Rayleigh–Ritz: one CTA per track.  Reads the track's Gram accumulators (and clears
+// them for the next iteration); writes C, CP in FP64 and in FP32 (coef32).
+__global__ void __launch_bounds__(RR_NT) k_rr(TrackState* const* __restrict__ states,
+                                               double2* const* __restrict__ gram_accs,
+                                               double2* const* __restrict__ coefs,
+                                               float2* const* __restrict__ coefs32, int ntracks,
+                                               IterParams prm);
+
+// ---------------------------------------------------------------------------------
 // Control (after the update; one warp per track) and Newton (after the HMkH pass; one
 // thread per track).
-__global__ void k_control(TrackState* const* __restrict__ states, double* const* __restrict__ res_parts,
+__global__ void k_control(TrackState* const* __restrict__ states, double* const* __restrict__ res_accs,
                           int ntracks, IterParams prm);
 __global__ void k_newton(TrackState* const* __restrict__ states, double* const* __restrict__ hmkh_parts,
                          const int* __restrict__ hmkh_nb, int ntracks, IterParams prm);
