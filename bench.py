@@ -189,7 +189,7 @@ def main():
             t = omb200.profile_apply("M", 1.3, probs[0]["eps_inv"], g, NEV, args.apply_cells, reps=args.steps)
             print(json.dumps({"case": "apply", "seconds_per_apply": t, "cells": args.apply_cells, "ncol": NEV}))
         else:
-            b = omb200.Batch(probs, omb200.B200Solver(device=local))
+            b = omb200.Batch(probs, omb200.B200Solver(device=local, warm_start="sweep"))
             b.run()
             _, info = b.results(return_info=True, raise_on_failure=False)
             print(json.dumps({"case": args.case, **{k: v for k, v in b.stats().items()},
@@ -204,7 +204,9 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
     import omb200
-    solver = omb200.B200Solver(precision="mixed", preconditioner="diag", newton="inner", device=local)
+    # batched + warm-start: each ridge's ω values form a sweep (OMB_WARM_SWEEP)
+    solver = omb200.B200Solver(precision="mixed", preconditioner="diag", newton="inner", device=local,
+                               warm_start="sweep")
     g, probs = workload(args.instances, seed=rank)
     batch = omb200.Batch(probs, solver)
 
@@ -307,6 +309,8 @@ def main():
                                    f"{len(probs)} instances per GPU (widths {list(WIDTHS)} x omega)",
                        "instances_per_gpu": len(probs), "nev": NEV, "grid": [NX, NY],
                        "precision": "mixed (FP32 iterations, FP64 polish)", "tol": 1e-8, "k_tol": 1e-8,
+                       "warm_start": "per-ridge omega sweep: the instance nearest the mean omega is solved first, "
+                                     "the others start from its device-resident eigenvectors and a first-order k",
                        "l2": "working set per step is GBs (inputs larger than L2)",
                        "parallelism": f"instances sharded, {world} rank(s)"},
             "converged_modes_per_step": converged_all, "modes_per_step": len(probs) * NEV * world,

@@ -113,6 +113,15 @@ int omb_apply_M_noalloc(int32_t Nx, int32_t Ny, double Dx, double Dy, double k, 
 #define OMB_NEWTON_OUTER 1 /* the reference loop: bands one after another, a full block
                               eigensolve per Newton step (the plain baseline)            */
 
+/* Warm starts across the instances of one batch (no counterpart in the reference, whose
+ * callers pass each solve's result as the next one's kguess/Hguess by hand) */
+#define OMB_WARM_NONE 0  /* every instance starts from its own guesses or at random      */
+#define OMB_WARM_SWEEP 1 /* instances sharing one epsinv array (same pointer) and grid form
+                            a frequency sweep: the one nearest the group's mean ω is solved
+                            first, the others start from its eigenvectors (on the device)
+                            with k_b + (ω − ω_a)·2ω_a/(∂ω²/∂k)_b per band; instances with
+                            their own Hguess or kguess_bands keep them                  */
+
 typedef struct {
   double k_tol;           /* Newton tolerance on |Δk|                       (1e-8) */
   double eig_tol;         /* residual ‖M̂h − ω²h‖ of a unit eigenvector       (1e-8) */
@@ -126,6 +135,7 @@ typedef struct {
   uint64_t seed;          /* random start blocks                              (0)    */
   int32_t guard_bands;    /* extra block columns beyond the wanted bands of a
                              Newton track (OMB_NEWTON_INNER)                  (1)    */
+  int32_t warm_start;     /* OMB_WARM_NONE or OMB_WARM_SWEEP                  (NONE) */
 } omb_options;
 
 /* One solve_k problem: the lowest `nev` guided modes of one cell at frequency ω. */
@@ -137,6 +147,7 @@ typedef struct {
   double kguess;           /* Newton start; ≤ 0 → k_guess(ω, ε⁻¹) = ω/√(min diag ε⁻¹) */
   const double* Hguess;    /* NULL or `nguess` warm-start columns (2, Nx, Ny)        */
   int32_t nguess;
+  const double* kguess_bands; /* NULL or nev per-band Newton starts (override kguess) */
 } omb_instance;
 
 /* Caller-owned outputs of one instance; any pointer but kmags may be NULL. */

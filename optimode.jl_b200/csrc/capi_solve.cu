@@ -8,14 +8,18 @@
 #include "engine.h"
 
 struct omb_batch {
+  struct Who { int inst, band0, eng, track; };  // a track's instance, first band, engine, index
   omb_ctx* ctx = nullptr;
   std::vector<omb_instance> inst;
-  std::vector<std::vector<double>> guesses;  // copies of the warm starts
+  std::vector<const double*> src_eps;          // the caller's ε⁻¹ pointers (sweep groups)
+  std::vector<std::vector<double>> guesses;    // copies of the warm starts
+  std::vector<std::vector<double>> kbands;     // copies of the per-band k guesses
   std::vector<omb::Problem> probs;
   omb::SolveOptions so;
   bool canon = true;
-  std::unique_ptr<omb::Engine> engine;
-  std::vector<std::pair<int, int>> who;  // track → (instance, first band)
+  int warm = OMB_WARM_NONE;
+  std::vector<std::unique_ptr<omb::Engine>> engines;  // one per stage
+  std::vector<Who> who;
   int64_t h2d = 0, d2h = 0;
   double run_seconds = 0;
 };
@@ -45,7 +49,56 @@ static int options_from(const omb_options* o, SolveOptions& so) {
   so.seed = o->seed;
   if (o->guard_bands < 0 || o->guard_bands > 4) return fail(OMB_ERR_INVALID_ARG, "guard_bands must be in 0..4");
   so.guard = o->guard_bands;
+  if (o->warm_start != OMB_WARM_NONE && o->warm_start != OMB_WARM_SWEEP)
+    return fail(OMB_ERR_INVALID_ARG, "warm_start must be OMB_WARM_NONE or OMB_WARM_SWEEP");
   return OMB_OK;
+}
+
+// Tracks of one instance.  k0[b] is band b's Newton start; gdev (optional) holds device
+// FP64 start columns for the block (bands 0..ngdev−1 of a solved neighbour).
+static void add_tracks(omb_batch* b, int i, const std::vector<double>& k0, const double2* const* gdev, int ngdev,
+                       int eng, std::vector<TrackSpec>& tracks) {
+  const omb_instance& I = b->inst[i];
+  auto fill = [&](TrackSpec& ts) {
+    ts.omega2 = I.omega * I.omega;
+    ts.guess = I.Hguess; ts.nguess = I.nguess;
+    if (!I.Hguess && gdev) {
+      ts.nguess_dev = std::min(ngdev, MMAX);
+      for (int c = 0; c < ts.nguess_dev; ++c) ts.guess_dev[c] = gdev[c];
+    }
+  };
+  if (b->so.newton_mode == MODE_NEWTON_INNER) {
+    // one Newton track per band: block = bands 0..b plus the guard columns
+    for (int band = 0; band < I.nev; ++band) {
+      TrackSpec ts;
+      ts.prob = i; ts.band = band; ts.nbands = 1; ts.M = band + 1 + b->so.guard; ts.need = band + 1;
+      ts.mode = MODE_NEWTON_INNER;
+      ts.k0 = k0[band];
+      fill(ts);
+      b->who.push_back({i, band, eng, (int)tracks.size()});
+      tracks.push_back(ts);
+    }
+  } else {
+    // the reference loop: bands in turn on one block of nev columns
+    TrackSpec ts;
+    ts.prob = i; ts.band = 0; ts.nbands = I.nev; ts.M = I.nev; ts.need = I.nev;
+    ts.mode = MODE_NEWTON_OUTER;
+    ts.k0 = k0[0];
+    fill(ts);
+    b->who.push_back({i, 0, eng, (int)tracks.size()});
+    tracks.push_back(ts);
+  }
+}
+
+// Newton starts of instance i from its own guesses (kguess_bands, kguess) or k_guess(ω, ε⁻¹).
+static std::vector<double> own_k0(const omb_batch* b, int i) {
+  const omb_instance& I = b->inst[i];
+  const double base = I.kguess > 0 ? I.kguess : I.omega * std::sqrt(1.0 / b->probs[i].min_diag);
+  std::vector<double> k0(I.nev, base);
+  if (!b->kbands[i].empty())
+    for (int j = 0; j < I.nev; ++j)
+      if (b->kbands[i][j] > 0) k0[j] = b->kbands[i][j];
+  return k0;
 }
 
 static int status_code(int ts) {
@@ -78,6 +131,7 @@ int omb_options_default(omb_options* o) {
   o->canonicalize = 1;
   o->seed = 0;
   o->guard_bands = 1;
+  o->warm_start = OMB_WARM_NONE;
   return OMB_OK;
 }
 
@@ -93,8 +147,11 @@ int omb_batch_create(omb_ctx* ctx, const omb_instance* inst, int n_inst, const o
   b->ctx = ctx;
   OMB_CU(cudaSetDevice(ctx->device));
   b->inst.assign(inst, inst + n_inst);
+  b->warm = opt ? opt->warm_start : OMB_WARM_NONE;
   b->probs.resize(n_inst);
   b->guesses.resize(n_inst);
+  b->kbands.resize(n_inst);
+  b->src_eps.resize(n_inst);
   for (int i = 0; i < n_inst; ++i) {
     omb_instance& I = b->inst[i];
     if (I.nev <= 0 || I.nev + b->so.guard > MMAX)
@@ -112,6 +169,11 @@ int omb_batch_create(omb_ctx* ctx, const omb_instance* inst, int n_inst, const o
       I.Hguess = b->guesses[i].data();
       b->h2d += (int64_t)(n * sizeof(double));
     }
+    if (I.kguess_bands) {
+      b->kbands[i].assign(I.kguess_bands, I.kguess_bands + I.nev);
+      I.kguess_bands = b->kbands[i].data();
+    }
+    b->src_eps[i] = I.epsinv;
     I.epsinv = nullptr;  // uploaded; the caller's array is not kept
   }
   *out = b.release();
@@ -122,40 +184,86 @@ int omb_batch_run(omb_batch* b) {
   if (!b) return fail(OMB_ERR_INVALID_ARG, "batch is NULL");
   omb_ctx* ctx = b->ctx;
   OMB_CU(cudaSetDevice(ctx->device));
-  std::vector<TrackSpec> tracks;
   b->who.clear();
+  b->engines.clear();
   const int n_inst = (int)b->inst.size();
-  for (int i = 0; i < n_inst; ++i) {
-    const omb_instance& I = b->inst[i];
-    const double k0 = I.kguess > 0 ? I.kguess : I.omega * std::sqrt(1.0 / b->probs[i].min_diag);
-    if (b->so.newton_mode == MODE_NEWTON_INNER) {
-      // one Newton track per band: block = bands 0..b plus one guard column
-      for (int band = 0; band < I.nev; ++band) {
-        TrackSpec ts;
-        ts.prob = i; ts.band = band; ts.nbands = 1; ts.M = band + 1 + b->so.guard; ts.need = band + 1;
-        ts.mode = MODE_NEWTON_INNER;
-        ts.omega2 = I.omega * I.omega; ts.k0 = k0;
-        ts.guess = I.Hguess; ts.nguess = I.nguess;
-        tracks.push_back(ts);
-        b->who.push_back({i, band});
+  // sweep groups: same ε⁻¹ pointer, grid and band count, no warm start of their own
+  std::vector<int> anchor(n_inst, -1);  // stage-2 instance → its stage-1 neighbour
+  if (b->warm == OMB_WARM_SWEEP) {
+    std::vector<std::vector<int>> groups;
+    std::vector<int> gid(n_inst, -1);
+    for (int i = 0; i < n_inst; ++i) {
+      const omb_instance& I = b->inst[i];
+      if (I.nguess > 0 || !b->kbands[i].empty()) continue;
+      for (size_t g = 0; g < groups.size() && gid[i] < 0; ++g) {
+        const omb_instance& J = b->inst[groups[g][0]];
+        if (b->src_eps[groups[g][0]] == b->src_eps[i] && J.grid.Nx == I.grid.Nx && J.grid.Ny == I.grid.Ny &&
+            J.grid.Dx == I.grid.Dx && J.grid.Dy == I.grid.Dy && J.nev == I.nev)
+          gid[i] = (int)g;
       }
-    } else {
-      // the reference loop: bands in turn on one block of nev columns
-      TrackSpec ts;
-      ts.prob = i; ts.band = 0; ts.nbands = I.nev; ts.M = I.nev; ts.need = I.nev;
-      ts.mode = MODE_NEWTON_OUTER;
-      ts.omega2 = I.omega * I.omega; ts.k0 = k0;
-      ts.guess = I.Hguess; ts.nguess = I.nguess;
-      tracks.push_back(ts);
-      b->who.push_back({i, 0});
+      if (gid[i] < 0) { gid[i] = (int)groups.size(); groups.push_back({i}); }
+      else groups[gid[i]].push_back(i);
+    }
+    for (const auto& g : groups) {
+      if (g.size() < 2) continue;
+      double mean = 0;
+      for (int i : g) mean += b->inst[i].omega;
+      mean /= (double)g.size();
+      int a = g[0];
+      for (int i : g)
+        if (std::fabs(b->inst[i].omega - mean) < std::fabs(b->inst[a].omega - mean)) a = i;
+      for (int i : g)
+        if (i != a) anchor[i] = a;
     }
   }
   cudaEvent_t e0, e1;
   OMB_CU(cudaEventCreate(&e0));
   OMB_CU(cudaEventCreate(&e1));
   OMB_CU(cudaEventRecord(e0, ctx->stream));
-  b->engine.reset(new Engine(ctx, &b->probs, tracks, b->so));
-  int rc = b->engine->run();
+  // stage 1: every instance without a neighbour to start from
+  std::vector<TrackSpec> tracks;
+  for (int i = 0; i < n_inst; ++i)
+    if (anchor[i] < 0) add_tracks(b, i, own_k0(b, i), nullptr, 0, 0, tracks);
+  b->engines.emplace_back(new Engine(ctx, &b->probs, tracks, b->so));
+  int rc = b->engines[0]->run();
+  // stage 2: the rest of each sweep group, from its anchor's eigenvectors and k
+  if (!rc) {
+    std::vector<TrackSpec> tracks2;
+    const Engine& E0 = *b->engines[0];
+    std::vector<std::vector<int>> first(n_inst);  // anchor → stage-1 who entries per band
+    for (size_t w = 0; w < b->who.size(); ++w) {
+      const auto& h = b->who[w];
+      auto& f = first[h.inst];
+      if (f.empty()) f.assign(b->inst[h.inst].nev, -1);
+      f[h.band0] = (int)w;
+    }
+    for (int i = 0; i < n_inst; ++i) {
+      const int a = anchor[i];
+      if (a < 0) continue;
+      const omb_instance& I = b->inst[i];
+      const double wa = b->inst[a].omega;
+      std::vector<double> k0(I.nev);
+      const double2* gdev[MMAX] = {};
+      const bool inner = b->so.newton_mode == MODE_NEWTON_INNER;
+      for (int j = 0; j < I.nev; ++j) {
+        // band j of the anchor: its own track (inner) or result j of its single track
+        const auto& h = b->who[first[a][inner ? j : 0]];
+        const int rb = inner ? 0 : j;
+        const TrackState& s = E0.result_state(h.track, rb);
+        const double dw2dk = 2.0 * s.hmkh;
+        double k = s.k * I.omega / wa;  // constant n_eff
+        if (dw2dk > 0 && std::isfinite(dw2dk) && std::isfinite(s.k))
+          k = s.k + (I.omega - wa) * 2.0 * wa / dw2dk;  // first order in ω: dk/dω = 2ω/(∂ω²/∂k)
+        k0[j] = (k > 0 && std::isfinite(k)) ? k : own_k0(b, i)[j];
+        if (j < MMAX) gdev[j] = E0.result_dev(h.track, rb);
+      }
+      add_tracks(b, i, k0, gdev, I.nev, 1, tracks2);
+    }
+    if (!tracks2.empty()) {
+      b->engines.emplace_back(new Engine(ctx, &b->probs, tracks2, b->so));
+      rc = b->engines[1]->run();
+    }
+  }
   cudaEventRecord(e1, ctx->stream);
   cudaEventSynchronize(e1);
   float ms = 0;
@@ -168,13 +276,14 @@ int omb_batch_run(omb_batch* b) {
 
 int omb_batch_results(omb_batch* b, omb_result* out) {
   if (!b || !out) return fail(OMB_ERR_INVALID_ARG, "batch and out must be non-NULL");
-  if (!b->engine) return fail(OMB_ERR_INVALID_ARG, "omb_batch_run has not been called");
+  if (b->engines.empty()) return fail(OMB_ERR_INVALID_ARG, "omb_batch_run has not been called");
   OMB_CU(cudaSetDevice(b->ctx->device));
-  Engine& E = *b->engine;
   bool all_ok = true;
   b->d2h = 0;
-  for (size_t t = 0; t < b->who.size(); ++t) {
-    const int i = b->who[t].first, band0 = b->who[t].second;
+  for (size_t w = 0; w < b->who.size(); ++w) {
+    const int i = b->who[w].inst, band0 = b->who[w].band0;
+    Engine& E = *b->engines[b->who[w].eng];
+    const int t = b->who[w].track;
     const omb_instance& I = b->inst[i];
     omb_result& r = out[i];
     if (!r.kmags) return fail(OMB_ERR_INVALID_ARG, "result kmags is NULL");
@@ -182,7 +291,7 @@ int omb_batch_results(omb_batch* b, omb_result* out) {
     const int nb = b->so.newton_mode == MODE_NEWTON_INNER ? 1 : I.nev;
     for (int rb = 0; rb < nb; ++rb) {
       const int band = band0 + rb;
-      const TrackState& s = E.result_state((int)t, rb);
+      const TrackState& s = E.result_state(t, rb);
       r.kmags[band] = s.k;
       if (r.residuals) r.residuals[band] = s.resid[band];
       if (r.dw2dk) r.dw2dk[band] = 2.0 * s.hmkh;
@@ -193,13 +302,13 @@ int omb_batch_results(omb_batch* b, omb_result* out) {
       all_ok = all_ok && s.status == TS_CONVERGED;
       if (r.evecs) {
         double* v = r.evecs + 2 * n2 * band;
-        int rc = E.fetch_result((int)t, rb, v);
+        int rc = E.fetch_result(t, rb, v);
         if (rc) return rc;
         b->d2h += (int64_t)(2 * n2 * sizeof(double));
         if (b->canon) {
           long long idx;
           double re, im;
-          rc = E.result_efield_argmax((int)t, rb, &idx, &re, &im);
+          rc = E.result_efield_argmax(t, rb, &idx, &re, &im);
           if (rc) return rc;
           b->d2h += 24;
           const std::complex<double> ph = std::polar(1.0, -std::atan2(im, re));
@@ -218,12 +327,17 @@ int omb_batch_results(omb_batch* b, omb_result* out) {
 
 int omb_batch_stats(const omb_batch* b, omb_stats* out) {
   if (!b || !out) return fail(OMB_ERR_INVALID_ARG, "batch and out must be non-NULL");
-  out->graph_launches = b->engine ? b->engine->graph_launches() : 0;
-  out->kernel_launches = b->engine ? b->engine->kernel_launches() : 0;
+  out->graph_launches = 0;
+  out->kernel_launches = 0;
+  out->max_iterations = 0;
+  for (const auto& e : b->engines) {
+    out->graph_launches += e->graph_launches();
+    out->kernel_launches += e->kernel_launches();
+    out->max_iterations = std::max<int32_t>(out->max_iterations, e->max_iterations());
+  }
   out->h2d_bytes = b->h2d;
   out->d2h_bytes = b->d2h;
   out->tracks = (int32_t)b->who.size();
-  out->max_iterations = b->engine ? b->engine->max_iterations() : 0;
   out->run_seconds = b->run_seconds;
   return OMB_OK;
 }

@@ -84,6 +84,18 @@ template <typename T> int Engine::init_block(int phase) {
           OMB_CU(cudaGetLastError());
         }
         OMB_CU(cudaStreamSynchronize(st));
+      } else if (ts.nguess_dev > 0) {
+        // device-resident FP64 columns from an earlier engine
+        for (int c = 0; c < std::min(ts.nguess_dev, ts.M); ++c) {
+          if (!ts.guess_dev[c]) continue;
+          if constexpr (std::is_same<T, double>::value) {
+            OMB_CU(cudaMemcpyAsync(X + (size_t)c * n2, ts.guess_dev[c], n2 * sizeof(double2),
+                                   cudaMemcpyDeviceToDevice, st));
+          } else {
+            k_c64_to_c32<<<blocks_for(n2), 256, 0, st>>>(ts.guess_dev[c], X + (size_t)c * n2, n2);
+            OMB_CU(cudaGetLastError());
+          }
+        }
       }
     } else {
       // previous phase ran in FP32: promote its X

@@ -34,6 +34,8 @@ struct TrackSpec {
   double omega2 = 0, k0 = 0;
   const double* guess = nullptr;  // host, interleaved complex, nguess columns of length n2
   int nguess = 0;
+  const double2* guess_dev[MMAX] = {};  // or device FP64 columns (another engine's results)
+  int nguess_dev = 0;
 };
 
 class Engine {
@@ -46,6 +48,10 @@ class Engine {
   // column of the block, or block column b for solve_ω²) and the argmax of its E field.
   const TrackState& result_state(int t, int b) const { return snaps_[t][b]; }
   int fetch_result(int t, int b, double* out);
+  // device address of result b of track t (FP64, n2 complex); valid while the engine lives
+  const double2* result_dev(int t, int b) const {
+    return store_.p + store_off_[t] + (size_t)b * 2 * (*probs_)[tracks_[t].prob].N();
+  }
   int fetch_block_column(int t, int col, double* out);
   int result_efield_argmax(int t, int b, long long* idx, double* re, double* im);
   int64_t graph_launches() const { return launches_; }

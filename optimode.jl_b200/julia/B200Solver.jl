@@ -28,6 +28,7 @@ struct OmbOptions
     canonicalize::Int32
     seed::UInt64
     guard_bands::Int32
+    warm_start::Int32
 end
 
 struct OmbInstance
@@ -38,6 +39,7 @@ struct OmbInstance
     kguess::Float64
     Hguess::Ptr{Float64}
     nguess::Int32
+    kguess_bands::Ptr{Float64}
 end
 
 struct OmbResult
@@ -53,13 +55,16 @@ end
 const _PREC = Dict(:fp32 => Int32(0), :fp64 => Int32(1), :mixed => Int32(2))
 const _PRECOND = Dict(:mpb => Int32(1), :diag => Int32(2))
 const _NEWTON = Dict(:inner => Int32(0), :outer => Int32(1))
+const _WARM = Dict(:none => Int32(0), :sweep => Int32(1))
 
 """
     B200Solver(; precision=:mixed, preconditioner=:diag, newton=:inner, device=0,
-               maxiter=300, guard_bands=1, logger=NullLogger())
+               maxiter=300, guard_bands=1, warm_start=:none, logger=NullLogger())
 
 NVIDIA B200 (sm_100a) backend: batched device LOBPCG with Newton steps on k inside the
-iteration, FP32 iterations polished in FP64 to the requested tolerance.
+iteration, FP32 iterations polished in FP64 to the requested tolerance.  `warm_start=:sweep`
+makes `solve_k_batch` start the instances that share one ε⁻¹ array from the solved instance
+nearest their mean ω (a frequency sweep).
 """
 struct B200Solver{L<:AbstractLogger} <: AbstractEigensolver{L}
     logger::L
@@ -69,11 +74,12 @@ struct B200Solver{L<:AbstractLogger} <: AbstractEigensolver{L}
     newton::Symbol
     maxiter::Int
     guard_bands::Int
+    warm_start::Symbol
 end
 
 B200Solver(; precision=:mixed, preconditioner=:diag, newton=:inner, device=0, maxiter=300,
-    guard_bands=1, logger=NullLogger()) =
-    B200Solver(logger, device, precision, preconditioner, newton, maxiter, guard_bands)
+    guard_bands=1, warm_start=:none, logger=NullLogger()) =
+    B200Solver(logger, device, precision, preconditioner, newton, maxiter, guard_bands, warm_start)
 
 const _OMB_CTX = Dict{Int,Ptr{Cvoid}}()
 
@@ -93,7 +99,7 @@ end
 
 function _omb_options(s::B200Solver; k_tol=1e-8, eig_tol=1e-8, max_eigsolves=60, maxiter=s.maxiter)
     OmbOptions(k_tol, eig_tol, max_eigsolves, maxiter, _PREC[s.precision], _PRECOND[s.preconditioner],
-        _NEWTON[s.newton], Int32(1), UInt64(0), Int32(s.guard_bands))
+        _NEWTON[s.newton], Int32(1), UInt64(0), Int32(s.guard_bands), _WARM[s.warm_start])
 end
 
 _omb_grid(g::Grid{2}) = OmbGrid(g.Nx, g.Ny, g.Δx, g.Δy)
@@ -107,7 +113,9 @@ loop over `solve_k`).
 function solve_k_batch(ωs, ε⁻¹s, grids, s::B200Solver; nevs=fill(1, length(ωs)), max_eigsolves=60,
     maxiter=s.maxiter, k_tol=1e-8, eig_tol=1e-8, kguesses=nothing, Hguesses=nothing)
     n = length(ωs)
-    eps = [convert(Array{Float64,4}, e) for e in ε⁻¹s]
+    # one converted array per distinct input, so a sweep over ω shares its ε⁻¹ pointer
+    conv = IdDict{Any,Array{Float64,4}}()
+    eps = [get!(() -> convert(Array{Float64,4}, e), conv, e) for e in ε⁻¹s]
     kmags = [zeros(Float64, nevs[i]) for i in 1:n]
     evecs = [zeros(ComplexF64, 2 * grids[i].Nx * grids[i].Ny, nevs[i]) for i in 1:n]
     status = [zeros(Int32, nevs[i]) for i in 1:n]
@@ -116,7 +124,7 @@ function solve_k_batch(ωs, ε⁻¹s, grids, s::B200Solver; nevs=fill(1, length(
         insts = [OmbInstance(_omb_grid(grids[i]), ωs[i], pointer(eps[i]), nevs[i],
             kguesses === nothing ? 0.0 : Float64(first(kguesses[i])),
             guesses[i] === nothing ? Ptr{Float64}(C_NULL) : Ptr{Float64}(pointer(guesses[i])),
-            guesses[i] === nothing ? 0 : size(guesses[i], 2)) for i in 1:n]
+            guesses[i] === nothing ? 0 : size(guesses[i], 2), Ptr{Float64}(C_NULL)) for i in 1:n]
         res = [OmbResult(pointer(kmags[i]), Ptr{Float64}(pointer(evecs[i])), C_NULL, C_NULL,
             pointer(status[i]), C_NULL, C_NULL) for i in 1:n]
         opt = Ref(_omb_options(s; k_tol, eig_tol, max_eigsolves, maxiter))

@@ -131,13 +131,14 @@ class c_options(ctypes.Structure):
                 ("max_eigsolves", ctypes.c_int32), ("maxiter", ctypes.c_int32),
                 ("precision", ctypes.c_int32), ("preconditioner", ctypes.c_int32),
                 ("newton", ctypes.c_int32), ("canonicalize", ctypes.c_int32),
-                ("seed", ctypes.c_uint64), ("guard_bands", ctypes.c_int32)]
+                ("seed", ctypes.c_uint64), ("guard_bands", ctypes.c_int32),
+                ("warm_start", ctypes.c_int32)]
 
 
 class c_instance(ctypes.Structure):
     _fields_ = [("grid", c_grid), ("omega", ctypes.c_double), ("epsinv", _dp),
                 ("nev", ctypes.c_int32), ("kguess", ctypes.c_double), ("Hguess", _dp),
-                ("nguess", ctypes.c_int32)]
+                ("nguess", ctypes.c_int32), ("kguess_bands", _dp)]
 
 
 _ip = ctypes.POINTER(ctypes.c_int32)

@@ -124,3 +124,38 @@ def test_warm_start_guess(omb, case):
     _, info0 = omb.solve_k_batch([{"omega": OMEGA0, "eps_inv": ei, "grid": g, "nev": 2}],
                                  return_info=True)
     assert info[0]["iterations"].sum() < info0[0]["iterations"].sum()
+
+
+@pytest.mark.parametrize("newton", ["inner", "outer"])
+def test_sweep_warm_start(omb, case, newton):
+    """A frequency sweep in one batch (OMB_WARM_SWEEP): the same k as independent solves
+    (and the oracle), and the members started from the solved neighbour need fewer
+    iterations than their cold solves."""
+    grid, ei, _, _ = case
+    g = omb.Grid(6.0, 4.0, 24, 16)
+    omegas = [1 / 1.50, 1 / 1.53, 1 / 1.56, 1 / 1.59]
+    probs = [{"omega": w, "eps_inv": ei, "grid": g, "nev": 2} for w in omegas]
+    prec = "fp64" if newton == "outer" else "mixed"
+    cold, info_c = omb.solve_k_batch(probs, omb.B200Solver(precision=prec, newton=newton), return_info=True)
+    warm, info_w = omb.solve_k_batch(probs, omb.B200Solver(precision=prec, newton=newton, warm_start="sweep"),
+                                     return_info=True)
+    for w, (kc, _), (kw, vw), iw in zip(omegas, cold, warm, info_w):
+        assert np.all(iw["status"] == 0)
+        assert np.allclose(kw, kc, rtol=1e-9)
+        ref, _ = O.solve_k(w, ei, grid, nev=2, k_tol=1e-12, eig_tol=1e-11)
+        assert np.allclose(kw, ref, rtol=1e-9)
+        for b in range(2):
+            assert _resid(kw[b], ei, grid, vw[b], w * w) < 2e-8
+    # the anchor is the ω nearest the mean (index 1 or 2); the other three start warm
+    it_c = np.array([i["iterations"].sum() for i in info_c])
+    it_w = np.array([i["iterations"].sum() for i in info_w])
+    assert it_w.sum() < it_c.sum()
+
+
+def test_kguess_bands(omb, case):
+    """Per-band Newton starts reach the same k."""
+    grid, ei, km_ref, _ = case
+    g = omb.Grid(6.0, 4.0, 24, 16)
+    ret = omb.solve_k_batch([{"omega": OMEGA0, "eps_inv": ei, "grid": g, "nev": 2,
+                              "kguess_bands": km_ref * 1.01}])
+    assert np.allclose(ret[0][0], km_ref, rtol=1e-9)
