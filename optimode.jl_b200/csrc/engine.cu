@@ -333,6 +333,8 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
     if ((it & 3) == 3 || it < 4) {
       rc_out = download_states();
       if (rc_out) break;
+      int perr = 0;  // a streaming kernel gave up on a wait: stop replaying
+      if (cudaMemcpy(&perr, d_err_.p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess || perr != PIPE_OK) break;
       bool all = true;
       for (const TrackState& s : host_states_) all = all && s.done;
       if (all) break;

@@ -1,15 +1,23 @@
 // Bulk-copy pipeline primitives (sm_90+/sm_100a): mbarrier phases and 1D bulk copies
 // (cp.async.bulk, the TMA's untiled form) from global into this CTA's shared memory.
 //
-// Every wait is bounded: a wait that does not complete within WAIT_POLLS polls returns
-// false, and the caller records an error and leaves the pipeline instead of spinning on.
+// Every wait is bounded in time: a wait that has not completed after WAIT_NS nanoseconds
+// of the global timer returns false, and the caller records an error and leaves the
+// pipeline instead of spinning on (a poll of mbarrier.try_wait may itself suspend, so a
+// bound on the number of polls would not bound the time).
 #pragma once
 
 #include <stdint.h>
 
 namespace omb {
 
-constexpr int WAIT_POLLS = 1 << 22;
+constexpr uint64_t WAIT_NS = 1000000000ull;  // 1 s
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -41,11 +49,13 @@ __device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Wait for the phase with the given parity to complete; false after WAIT_POLLS polls.
+// Wait for the phase with the given parity to complete; false after WAIT_NS.
 __device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
-  for (int i = 0; i < WAIT_POLLS; ++i)
-    if (mbar_test(b, parity)) return true;
-  return false;
+  if (mbar_test(b, parity)) return true;
+  const uint64_t t0 = global_ns();
+  while (!mbar_test(b, parity))
+    if (global_ns() - t0 > WAIT_NS) return false;
+  return true;
 }
 // Bulk copy of `bytes` (multiple of 16; both addresses 16-byte aligned) completing on `b`.
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* b) {
