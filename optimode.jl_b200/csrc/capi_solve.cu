@@ -14,7 +14,8 @@ struct omb_batch {
   std::vector<const double*> src_eps;          // the caller's ε⁻¹ pointers (sweep groups)
   std::vector<std::vector<double>> guesses;    // copies of the warm starts
   std::vector<std::vector<double>> kbands;     // copies of the per-band k guesses
-  std::vector<omb::Problem> probs;
+  std::vector<omb::Problem> probs;             // distinct uploaded cells
+  std::vector<int> pidx;                        // instance → its cell in probs
   omb::SolveOptions so;
   bool canon = true;
   int warm = OMB_WARM_NONE;
@@ -71,7 +72,7 @@ static void add_tracks(omb_batch* b, int i, const std::vector<double>& k0, const
     // one Newton track per band: block = bands 0..b plus the guard columns
     for (int band = 0; band < I.nev; ++band) {
       TrackSpec ts;
-      ts.prob = i; ts.band = band; ts.nbands = 1; ts.M = band + 1 + b->so.guard; ts.need = band + 1;
+      ts.prob = b->pidx[i]; ts.band = band; ts.nbands = 1; ts.M = band + 1 + b->so.guard; ts.need = band + 1;
       ts.mode = MODE_NEWTON_INNER;
       ts.k0 = k0[band];
       fill(ts);
@@ -81,7 +82,7 @@ static void add_tracks(omb_batch* b, int i, const std::vector<double>& k0, const
   } else {
     // the reference loop: bands in turn on one block of nev columns
     TrackSpec ts;
-    ts.prob = i; ts.band = 0; ts.nbands = I.nev; ts.M = I.nev; ts.need = I.nev;
+    ts.prob = b->pidx[i]; ts.band = 0; ts.nbands = I.nev; ts.M = I.nev; ts.need = I.nev;
     ts.mode = MODE_NEWTON_OUTER;
     ts.k0 = k0[0];
     fill(ts);
@@ -93,7 +94,7 @@ static void add_tracks(omb_batch* b, int i, const std::vector<double>& k0, const
 // Newton starts of instance i from its own guesses (kguess_bands, kguess) or k_guess(ω, ε⁻¹).
 static std::vector<double> own_k0(const omb_batch* b, int i) {
   const omb_instance& I = b->inst[i];
-  const double base = I.kguess > 0 ? I.kguess : I.omega * std::sqrt(1.0 / b->probs[i].min_diag);
+  const double base = I.kguess > 0 ? I.kguess : I.omega * std::sqrt(1.0 / b->probs[b->pidx[i]].min_diag);
   std::vector<double> k0(I.nev, base);
   if (!b->kbands[i].empty())
     for (int j = 0; j < I.nev; ++j)
@@ -148,7 +149,8 @@ int omb_batch_create(omb_ctx* ctx, const omb_instance* inst, int n_inst, const o
   OMB_CU(cudaSetDevice(ctx->device));
   b->inst.assign(inst, inst + n_inst);
   b->warm = opt ? opt->warm_start : OMB_WARM_NONE;
-  b->probs.resize(n_inst);
+  b->probs.reserve(n_inst);
+  b->pidx.assign(n_inst, -1);
   b->guesses.resize(n_inst);
   b->kbands.resize(n_inst);
   b->src_eps.resize(n_inst);
@@ -158,13 +160,25 @@ int omb_batch_create(omb_ctx* ctx, const omb_instance* inst, int n_inst, const o
       return fail(OMB_ERR_INVALID_ARG, "nev + guard_bands must be in 2..12");
     if (!(I.omega > 0) || !std::isfinite(I.omega)) return fail(OMB_ERR_INVALID_ARG, "omega must be finite and positive");
     if (I.nguess < 0 || (I.nguess > 0 && !I.Hguess)) return fail(OMB_ERR_INVALID_ARG, "bad Hguess/nguess");
-    rc = upload_problem(ctx, &I.grid, I.epsinv, b->probs[i]);
-    if (rc) return rc;
-    b->h2d += problem_bytes(b->probs[i]);
-    if (2 * (long long)b->probs[i].N() < 3 * (I.nev + 2))
+    // instances that pass the same ε⁻¹ array for the same grid share one uploaded cell
+    for (int j = 0; j < i && b->pidx[i] < 0; ++j) {
+      const omb_instance& J = b->inst[j];
+      if (b->src_eps[j] == I.epsinv && J.grid.Nx == I.grid.Nx && J.grid.Ny == I.grid.Ny &&
+          J.grid.Dx == I.grid.Dx && J.grid.Dy == I.grid.Dy)
+        b->pidx[i] = b->pidx[j];
+    }
+    if (b->pidx[i] < 0) {
+      b->probs.emplace_back();
+      rc = upload_problem(ctx, &I.grid, I.epsinv, b->probs.back());
+      if (rc) return rc;
+      b->pidx[i] = (int)b->probs.size() - 1;
+      b->h2d += problem_bytes(b->probs.back());
+    }
+    const Problem& Pi = b->probs[b->pidx[i]];
+    if (2 * (long long)Pi.N() < 3 * (I.nev + 2))
       return fail(OMB_ERR_INVALID_ARG, "grid too small for the requested bands");
     if (I.nguess > 0) {
-      const size_t n = 4 * b->probs[i].N() * (size_t)I.nguess;
+      const size_t n = 4 * Pi.N() * (size_t)I.nguess;
       b->guesses[i].assign(I.Hguess, I.Hguess + n);
       I.Hguess = b->guesses[i].data();
       b->h2d += (int64_t)(n * sizeof(double));
@@ -287,7 +301,7 @@ int omb_batch_results(omb_batch* b, omb_result* out) {
     const omb_instance& I = b->inst[i];
     omb_result& r = out[i];
     if (!r.kmags) return fail(OMB_ERR_INVALID_ARG, "result kmags is NULL");
-    const size_t n2 = 2 * b->probs[i].N();
+    const size_t n2 = 2 * b->probs[b->pidx[i]].N();
     const int nb = b->so.newton_mode == MODE_NEWTON_INNER ? 1 : I.nev;
     for (int rb = 0; rb < nb; ++rb) {
       const int band = band0 + rb;
@@ -302,22 +316,21 @@ int omb_batch_results(omb_batch* b, omb_result* out) {
       all_ok = all_ok && s.status == TS_CONVERGED;
       if (r.evecs) {
         double* v = r.evecs + 2 * n2 * band;
-        int rc = E.fetch_result(t, rb, v);
-        if (rc) return rc;
-        b->d2h += (int64_t)(2 * n2 * sizeof(double));
+        int rc = OMB_OK;
         if (b->canon) {
+          // phase gauge on the device: the largest E component real and positive
           long long idx;
           double re, im;
           rc = E.result_efield_argmax(t, rb, &idx, &re, &im);
           if (rc) return rc;
           b->d2h += 24;
-          const std::complex<double> ph = std::polar(1.0, -std::atan2(im, re));
-          for (size_t q = 0; q < n2; ++q) {
-            const std::complex<double> w = std::complex<double>(v[2 * q], v[2 * q + 1]) * ph;
-            v[2 * q] = w.real();
-            v[2 * q + 1] = w.imag();
-          }
+          const double a = std::hypot(re, im);
+          if (a > 0) rc = E.rotate_result(t, rb, re / a, -im / a);
+          if (rc) return rc;
         }
+        rc = E.fetch_result(t, rb, v);
+        if (rc) return rc;
+        b->d2h += (int64_t)(2 * n2 * sizeof(double));
       }
     }
   }

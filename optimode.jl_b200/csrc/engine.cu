@@ -518,6 +518,13 @@ int Engine::fetch_block_column(int t, int col, double* out) {
   return OMB_OK;
 }
 
+int Engine::rotate_result(int t, int b, double c, double s) {
+  const size_t n2 = 2 * (*probs_)[tracks_[t].prob].N();
+  k_rotate_c64<<<blocks_for(n2), 256, 0, ctx_->stream>>>(store_.p + store_off_[t] + (size_t)b * n2, n2, c, s);
+  OMB_CU(cudaGetLastError());
+  return OMB_OK;
+}
+
 int Engine::result_efield_argmax(int t, int b, long long* idx, double* re, double* im) {
   const TrackSpec& ts = tracks_[t];
   const Problem& P = (*probs_)[ts.prob];

@@ -54,6 +54,8 @@ class Engine {
   }
   int fetch_block_column(int t, int col, double* out);
   int result_efield_argmax(int t, int b, long long* idx, double* re, double* im);
+  // multiply result b of track t by the unit phase c + i s on the device
+  int rotate_result(int t, int b, double c, double s);
   int64_t graph_launches() const { return launches_; }
   int64_t kernel_launches() const { return kernels_; }
   int max_iterations() const;

@@ -11,6 +11,12 @@ __global__ void k_c32_to_c64(const float2* __restrict__ a, double2* __restrict__
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     b[i] = make_double2((double)a[i].x, (double)a[i].y);
 }
+__global__ void k_rotate_c64(double2* __restrict__ v, size_t n, double c, double s) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double2 a = v[i];
+    v[i] = make_double2(a.x * c - a.y * s, a.x * s + a.y * c);
+  }
+}
 
 __global__ void k_reduce_partials(const double* __restrict__ partial, int nb, int ncol, double* __restrict__ out) {
   const int col = blockIdx.x;

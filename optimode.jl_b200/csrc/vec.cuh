@@ -8,6 +8,8 @@ namespace omb {
 // Precision conversion of complex arrays (n elements).
 __global__ void k_c64_to_c32(const double2* __restrict__ a, float2* __restrict__ b, size_t n);
 __global__ void k_c32_to_c64(const float2* __restrict__ a, double2* __restrict__ b, size_t n);
+// v ← v·(c + i s) (a unit phase), n elements
+__global__ void k_rotate_c64(double2* __restrict__ v, size_t n, double c, double s);
 
 // Diagonal preconditioner on a 2-component block: H ← H · eps_mean / |k+G|².
 template <typename T>
