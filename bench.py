@@ -43,13 +43,21 @@ WIDTHS = (1.0, 1.5, 2.0)
 FALLBACK_HBM_GBS = 6650.0
 
 
-def workload(n_inst: int, seed: int = 0):
+def rank_omegas(n_om: int, rank: int = 0, world: int = 1):
+    """The ω values of one rank: the whole job sweeps n_om·world frequencies uniform in
+    [1/1.60, 1/1.50] μm⁻¹ and rank r takes the r-th contiguous block of n_om (weak scaling:
+    every rank gets the same amount of work, no two ranks solve the same instance)."""
+    allw = np.linspace(1 / 1.60, 1 / 1.50, n_om * world)
+    return allw[rank * n_om:(rank + 1) * n_om]
+
+
+def workload(n_inst: int, rank: int = 0, world: int = 1):
     from omb200 import Grid
     from omb200 import geometry as G
     g = Grid(DX, DY, NX, NY)
     n_w = len(WIDTHS)
     n_om = max(1, (n_inst + n_w - 1) // n_w)
-    omegas = np.linspace(1 / 1.60, 1 / 1.50, n_om)
+    omegas = rank_omegas(n_om, rank, world)
     eps = {w: G.ln_ridge(g, top_width=w) for w in WIDTHS}
     probs = []
     for i in range(n_inst):
@@ -57,6 +65,20 @@ def workload(n_inst: int, seed: int = 0):
         om = omegas[(i // n_w) % n_om]
         probs.append({"omega": float(om), "eps_inv": eps[w], "grid": g, "nev": NEV})
     return g, probs
+
+
+def combine_ranks(dev_s: float, converged: int, e2e_s: float, dist=None, device="cpu"):
+    """Whole-job numbers from each rank's own: the slowest rank's device and end-to-end
+    times (max over ranks) and the converged modes of all ranks (sum).  Every rank calls
+    this once, at the same point, so the collectives line up."""
+    if dist is None:
+        return dev_s, converged, e2e_s
+    import torch
+    t = torch.tensor([dev_s, e2e_s], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor([converged], dtype=torch.int64, device=device)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return float(t[0].item()), int(c.item()), float(t[1].item())
 
 
 def sample_clocks(stop: threading.Event, out: list, index: int):
@@ -207,7 +229,7 @@ def main():
     # batched + warm-start: each ridge's ω values form a sweep (OMB_WARM_SWEEP)
     solver = omb200.B200Solver(precision="mixed", preconditioner="diag", newton="inner", device=local,
                                warm_start="sweep")
-    g, probs = workload(args.instances, seed=rank)
+    g, probs = workload(args.instances, rank, world)
     batch = omb200.Batch(probs, solver)
 
     def barrier():
@@ -234,17 +256,6 @@ def main():
     th.join(timeout=5)
     res, info = batch.results(return_info=True, raise_on_failure=False)
     converged = int(sum(int(np.sum(i["status"] == 0)) for i in info))
-    max_dev_s = dev_s
-    if dist is not None:
-        t = torch.tensor([dev_s], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        max_dev_s = float(t.item())
-        c = torch.tensor([converged], device=f"cuda:{local}")
-        dist.all_reduce(c, op=dist.ReduceOp.SUM)
-        converged_all = int(c.item())
-    else:
-        converged_all = converged
-    value = converged_all * args.steps / max_dev_s
     batch.close()
 
     # end to end through the public C ABI call with host buffers
@@ -262,11 +273,9 @@ def main():
     st4 = b4.stats()
     h2d, d2h = st4["h2d_bytes"], st4["d2h_bytes"]
     b4.close()
-    e2e_val = converged * args.e2e_steps / e2e_s
-    if dist is not None:
-        t = torch.tensor([e2e_s], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_val = converged_all * args.e2e_steps / float(t.item())
+    max_dev_s, converged_all, max_e2e_s = combine_ranks(dev_s, converged, e2e_s, dist, f"cuda:{local}")
+    value = converged_all * args.steps / max_dev_s
+    e2e_val = converged_all * args.e2e_steps / max_e2e_s
 
     out = None
     if rank == 0:
