@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(RR_NT) k_rr(TrackState* const* __restrict__ st
   double2* S = G + NMAX * NMAX;
   double2* V = S + NMAX * NMAX;
   double2* B = V + NMAX * NMAX;
-  __shared__ Rot rot[NMAX / 2 + 1];
+  __shared__ RotIdx ri[NMAX];
   __shared__ double red[64];
   __shared__ int order[NMAX];
   __shared__ double dsc[NMAX];
@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(RR_NT) k_rr(TrackState* const* __restrict__ st
       }
     }
     __syncthreads();
-    jacobi_eigh(B, V, r, ld, rot, red);
+    jacobi_eigh(B, V, r, ld, S, ri, red);  // S is free once B = L⁻¹ S L⁻ᴴ
     Ev = V;
     Av = B;
   } else {
@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(RR_NT) k_rr(TrackState* const* __restrict__ st
       G[a * ld + b] = B[a * ld + b];
     }
     __syncthreads();
-    jacobi_eigh(G, V, n, ld, rot, red);
+    jacobi_eigh(G, V, n, ld, B, ri, red);  // B's copy of G is back in G
     if (tid == 0) {
       double tmax = 0;
       for (int i = 0; i < n; ++i) { theta[i] = G[i * ld + i].x; tmax = fmax(tmax, theta[i]); }
@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(RR_NT) k_rr(TrackState* const* __restrict__ st
       G[i * ld + j] = acc;
     }
     __syncthreads();
-    jacobi_eigh(G, V, r, ld, rot, red);
+    jacobi_eigh(G, V, r, ld, S, ri, red);  // S is folded into G = Bᴴ S B
     Ev = V;
     Av = G;
   }

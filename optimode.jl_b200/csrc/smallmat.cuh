@@ -3,20 +3,25 @@
 // Matrices live in shared memory, row-major with leading dimension `ld`, complex double.
 // The eigensolver is the cyclic Jacobi method for complex Hermitian matrices with the
 // round-robin (tournament) ordering of Brent & Luk, so the n/2 rotations of a round act on
-// disjoint index pairs and are applied together: all row rotations (A ← JᴴA), then all
-// column rotations (A ← AJ, V ← VJ).  Each 2×2 rotation first removes the phase of A_pq
+// disjoint index pairs.  Each 2×2 rotation first removes the phase of A_pq
 // (D = diag(1, e^{-iφ})) and then applies the real symmetric Jacobi rotation with
 // t = sign(ζ)/(|ζ| + √(1+ζ²)), ζ = (A_qq − A_pp)/(2|A_pq|) (Golub & Van Loan, Matrix
-// Computations, §8.5).  Sweeps stop when the off-diagonal Frobenius norm falls below
-// 1e-13·‖A‖_F (eigenvalue perturbation ≲ 1e-26‖A‖²/gap; rounding keeps the off-diagonal
-// near n·1e-16‖A‖, so a tighter test would never pass) or after `max_sweeps`.
+// Computations, §8.5).  A round is two barriers: one thread per pair computes its rotation
+// (reciprocal square roots only, no divisions by |A_pq|), then every element of the new
+// matrix is formed from the four old elements it depends on, A' = JᴴAJ, into a second
+// buffer, while V ← VJ is updated in place by column pairs.  Sweeps stop when the
+// off-diagonal Frobenius norm falls below 1e-13·‖A‖_F (eigenvalue perturbation
+// ≲ 1e-26‖A‖²/gap; rounding keeps the off-diagonal near n·1e-16‖A‖, so a tighter test
+// would never pass) or after `max_sweeps`.
 #pragma once
 
 #include "omb_common.cuh"
 
 namespace omb {
 
-struct Rot { double c, s, er, ei; int p, q; };
+// Per index a of a round: partner pa and the coefficients of the two-sided update,
+// (JᴴA)_a· = α_a A_a· + β_a A_pa·  and  (AJ)_·a = γ_a A_·a + δ_a A_·pa.
+struct RotIdx { double2 al, be, ga, de; int pa; };
 
 // Round-robin pairing: players 0..ne-1 (ne even); player 0 fixed, the rest rotate.
 __device__ __forceinline__ void rr_pair(int round, int i, int ne, int& p, int& q) {
@@ -26,10 +31,14 @@ __device__ __forceinline__ void rr_pair(int round, int i, int ne, int& p, int& q
   q = a < b ? b : a;
 }
 
+__device__ __forceinline__ double2 zmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
 // Jacobi eigen-decomposition of the n×n Hermitian matrix A (overwritten with its
 // eigenvalues on the diagonal); V (n×n) receives the eigenvectors as columns.
-// `rot` needs ≥ n/2+1 entries of shared scratch, `red` ≥ 32 doubles.
-__device__ inline void jacobi_eigh(double2* A, double2* V, int n, int ld, Rot* rot, double* red,
+// `A2` is n×n scratch (leading dimension ld), `ri` ≥ n entries, `red` ≥ 2·(warps) doubles.
+__device__ inline void jacobi_eigh(double2* A, double2* V, int n, int ld, double2* A2, RotIdx* ri, double* red,
                                    int max_sweeps = 20) {
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int e = tid; e < n * n; e += nt) {
@@ -39,6 +48,8 @@ __device__ inline void jacobi_eigh(double2* A, double2* V, int n, int ld, Rot* r
   }
   __syncthreads();
   if (n <= 1) return;
+  double2* cur = A;
+  double2* nxt = A2;
   const int ne = n + (n & 1);
   const int npair = ne / 2;
   for (int sweep = 0; sweep < max_sweeps; ++sweep) {
@@ -46,7 +57,7 @@ __device__ inline void jacobi_eigh(double2* A, double2* V, int n, int ld, Rot* r
     double off = 0, tot = 0;
     for (int e = tid; e < n * n; e += nt) {
       const int r = e / n, c = e % n;
-      const double2 v = A[r * ld + c];
+      const double2 v = cur[r * ld + c];
       const double a2 = v.x * v.x + v.y * v.y;
       tot += a2;
       if (r != c) off += a2;
@@ -62,54 +73,64 @@ __device__ inline void jacobi_eigh(double2* A, double2* V, int n, int ld, Rot* r
     __syncthreads();
     if (so <= 1e-26 * st || so == 0.0) break;
     for (int round = 0; round < ne - 1; ++round) {
+      // 1. rotations of this round (identity for the odd player out and settled pairs)
       for (int i = tid; i < npair; i += nt) {
         int p, q;
         rr_pair(round, i, ne, p, q);
-        Rot R{1.0, 0.0, 1.0, 0.0, p, q};
+        const double2 one = make_double2(1.0, 0.0), zero = make_double2(0.0, 0.0);
+        RotIdx rp{one, zero, one, zero, q}, rq{one, zero, one, zero, p};
         if (q < n) {
-          const double2 apq = A[p * ld + q];
-          const double g = sqrt(apq.x * apq.x + apq.y * apq.y);
-          const double app = A[p * ld + p].x, aqq = A[q * ld + q].x;
-          if (g > 1e-300 && g > 1e-18 * sqrt(fabs(app * aqq))) {
-            const double zeta = (aqq - app) / (2.0 * g);
-            const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-            R.c = 1.0 / sqrt(1.0 + t * t);
-            R.s = t * R.c;
-            R.er = apq.x / g;  // e^{iφ}
-            R.ei = apq.y / g;
-          } else {
-            R.q = n;  // no-op
+          const double2 apq = cur[p * ld + q];
+          const double g2 = apq.x * apq.x + apq.y * apq.y;
+          const double app = cur[p * ld + p].x, aqq = cur[q * ld + q].x;
+          if (g2 > 1e-300 && g2 > 1e-36 * fabs(app * aqq)) {
+            const double rg = rsqrt(g2);                    // 1/|A_pq|
+            const double er = apq.x * rg, ei = apq.y * rg;  // e^{iφ}
+            const double zeta = 0.5 * (aqq - app) * rg;
+            const double h = 1.0 + zeta * zeta;
+            const double t = (zeta >= 0 ? 1.0 : -1.0) * __drcp_rn(fabs(zeta) + h * rsqrt(h));
+            const double c = rsqrt(1.0 + t * t), sn = t * c;
+            // rows:    A_p· ← c A_p· − s e A_q·,    A_q· ← s A_p· + c e A_q·
+            // columns: A_·p ← c A_·p − s ē A_·q,    A_·q ← s A_·p + c ē A_·q
+            rp.al = make_double2(c, 0.0);         rp.be = make_double2(-sn * er, -sn * ei);
+            rq.al = make_double2(c * er, c * ei); rq.be = make_double2(sn, 0.0);
+            rp.ga = make_double2(c, 0.0);         rp.de = make_double2(-sn * er, sn * ei);
+            rq.ga = make_double2(c * er, -c * ei); rq.de = make_double2(sn, 0.0);
           }
+          ri[q] = rq;
         }
-        rot[i] = R;
+        ri[p] = rp;
       }
       __syncthreads();
-      // rows: A_p· ← c A_p· − s e^{iφ} A_q· ;  A_q· ← s A_p· + c e^{iφ} A_q·
-      for (int e = tid; e < npair * n; e += nt) {
-        const Rot R = rot[e / n];
-        if (R.q >= n) continue;
-        const int col = e % n;
-        const double2 ap = A[R.p * ld + col], aq = A[R.q * ld + col];
-        const double2 eaq = make_double2(R.er * aq.x - R.ei * aq.y, R.er * aq.y + R.ei * aq.x);
-        A[R.p * ld + col] = make_double2(R.c * ap.x - R.s * eaq.x, R.c * ap.y - R.s * eaq.y);
-        A[R.q * ld + col] = make_double2(R.s * ap.x + R.c * eaq.x, R.s * ap.y + R.c * eaq.y);
+      // 2. A' = JᴴAJ element by element into the other buffer; V ← VJ by column pairs
+      for (int e = tid; e < n * n; e += nt) {
+        const int i = e / n, j = e % n;
+        const RotIdx a = ri[i], b = ri[j];
+        double2 v = zmul(zmul(a.al, cur[i * ld + j]), b.ga);
+        if (b.pa < n) v = v + zmul(zmul(a.al, cur[i * ld + b.pa]), b.de);
+        if (a.pa < n) {
+          v = v + zmul(zmul(a.be, cur[a.pa * ld + j]), b.ga);
+          if (b.pa < n) v = v + zmul(zmul(a.be, cur[a.pa * ld + b.pa]), b.de);
+        }
+        nxt[i * ld + j] = v;
+      }
+      for (int e = tid; e < n * npair; e += nt) {
+        const int i = e / npair, k = e % npair;
+        int p, q;
+        rr_pair(round, k, ne, p, q);
+        if (q >= n) continue;
+        const RotIdx rp = ri[p], rq = ri[q];
+        const double2 vp = V[i * ld + p], vq = V[i * ld + q];
+        V[i * ld + p] = zmul(rp.ga, vp) + zmul(rp.de, vq);
+        V[i * ld + q] = zmul(rq.ga, vq) + zmul(rq.de, vp);
       }
       __syncthreads();
-      // columns: A_·p ← c A_·p − s e^{-iφ} A_·q ;  A_·q ← s A_·p + c e^{-iφ} A_·q   (and V)
-      for (int e = tid; e < 2 * npair * n; e += nt) {
-        const int which = e / (npair * n);
-        const int ee = e % (npair * n);
-        const Rot R = rot[ee / n];
-        if (R.q >= n) continue;
-        const int row = ee % n;
-        double2* M = which ? V : A;
-        const double2 ap = M[row * ld + R.p], aq = M[row * ld + R.q];
-        const double2 eaq = make_double2(R.er * aq.x + R.ei * aq.y, R.er * aq.y - R.ei * aq.x);
-        M[row * ld + R.p] = make_double2(R.c * ap.x - R.s * eaq.x, R.c * ap.y - R.s * eaq.y);
-        M[row * ld + R.q] = make_double2(R.s * ap.x + R.c * eaq.x, R.s * ap.y + R.c * eaq.y);
-      }
-      __syncthreads();
+      double2* tmp = cur; cur = nxt; nxt = tmp;
     }
+  }
+  if (cur != A) {
+    for (int e = tid; e < n * n; e += nt) A[(e / n) * ld + e % n] = cur[(e / n) * ld + e % n];
+    __syncthreads();
   }
   for (int e = tid; e < n; e += nt) A[e * ld + e].y = 0.0;
   __syncthreads();
