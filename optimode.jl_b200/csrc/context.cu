@@ -45,6 +45,79 @@ cudaError_t ensure_smem(const void* func, size_t bytes) {
   return e;
 }
 
+namespace {
+struct BigBlock {
+  void* p = nullptr;
+  size_t bytes = 0;
+  bool busy = false;
+  cudaStream_t last = nullptr;
+  cudaEvent_t done = nullptr;  // recorded on `last` when the block was returned
+};
+std::mutex g_big_mu;
+std::map<int, std::vector<BigBlock>> g_big;  // per device
+}  // namespace
+
+cudaError_t big_alloc(void** p, size_t bytes, cudaStream_t st) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  bytes = (bytes + ((size_t)2 << 20) - 1) & ~(((size_t)2 << 20) - 1);  // 2 MiB granules
+  std::lock_guard<std::mutex> lk(g_big_mu);
+  std::vector<BigBlock>& v = g_big[dev];
+  BigBlock* best = nullptr;
+  for (BigBlock& b : v)
+    if (!b.busy && b.bytes >= bytes && (!best || b.bytes < best->bytes)) best = &b;
+  if (best) {
+    if (best->last != st && best->done) {
+      e = cudaStreamWaitEvent(st, best->done, 0);
+      if (e != cudaSuccess) return e;
+    }
+    best->busy = true;
+    best->last = st;
+    *p = best->p;
+    return cudaSuccess;
+  }
+  BigBlock b;
+  e = cudaMalloc(&b.p, bytes);
+  if (e != cudaSuccess) {
+    // release the idle cached blocks and try once more
+    cudaDeviceSynchronize();
+    for (auto it = v.begin(); it != v.end();) {
+      if (!it->busy) {
+        cudaFree(it->p);
+        if (it->done) cudaEventDestroy(it->done);
+        it = v.erase(it);
+      } else {
+        ++it;
+      }
+    }
+    cudaGetLastError();
+    e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) return e;
+  }
+  e = cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming);
+  if (e != cudaSuccess) { cudaFree(b.p); return e; }
+  b.bytes = bytes;
+  b.busy = true;
+  b.last = st;
+  v.push_back(b);
+  *p = b.p;
+  return cudaSuccess;
+}
+
+void big_free(void* p, cudaStream_t st) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  std::lock_guard<std::mutex> lk(g_big_mu);
+  for (BigBlock& b : g_big[dev])
+    if (b.p == p) {
+      b.busy = false;
+      b.last = st;
+      cudaEventRecord(b.done, st);
+      return;
+    }
+}
+
 int row_blocks(int Nx, int Ny) {
   const int rows = plan2_a(Nx) ? l2_rows(Nx) : rows_for(Nx);
   return (Ny + rows - 1) / rows;

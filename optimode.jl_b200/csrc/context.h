@@ -29,7 +29,18 @@ int cuda_fail(cudaError_t e, const char* what);
     if (e__ != cudaSuccess) return ::omb::cuda_fail(e__, #x); \
   } while (0)
 
-// Stream-ordered device buffer (cudaMallocAsync from the device's pool).
+// Large device blocks (≥ BIG_BLOCK bytes) come from a per-device cache of cudaMalloc'd
+// blocks that are kept for the life of the process and handed out best-fit, so the
+// multi-GB block buffers of consecutive phases, stages and batches reuse memory instead of
+// growing the stream-ordered pool (which maps new pages, hundreds of ms per GB, whenever
+// no free fragment fits).  A returned block records an event on the stream that last used
+// it; a later user on another stream waits on that event first.
+constexpr size_t BIG_BLOCK = (size_t)4 << 20;
+cudaError_t big_alloc(void** p, size_t bytes, cudaStream_t st);
+void big_free(void* p, cudaStream_t st);
+
+// Stream-ordered device buffer: cudaMallocAsync from the device's pool for small buffers,
+// the block cache above for large ones.
 template <typename T> struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
@@ -48,11 +59,15 @@ template <typename T> struct DevBuf {
     st = stream;
     n = count;
     if (count == 0) return cudaSuccess;
+    if (count * sizeof(T) >= BIG_BLOCK) return big_alloc(reinterpret_cast<void**>(&p), count * sizeof(T), stream);
     return cudaMallocAsync(reinterpret_cast<void**>(&p), count * sizeof(T), stream);
   }
   cudaError_t zero() { return n ? cudaMemsetAsync(p, 0, n * sizeof(T), st) : cudaSuccess; }
   void release() {
-    if (p) cudaFreeAsync(p, st);
+    if (p) {
+      if (n * sizeof(T) >= BIG_BLOCK) big_free(p, st);
+      else cudaFreeAsync(p, st);
+    }
     p = nullptr;
     n = 0;
   }

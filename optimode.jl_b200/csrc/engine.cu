@@ -224,8 +224,12 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
   }
   DevBuf<TrackDesc<T>> d_descs;
   DevBuf<OpUnit<T>> d_uA[2], d_uP[2], d_uH[2];
+  // device-side per-track arrays are in grid-sorted position order (order_), so every lane
+  // below and every grid group is a contiguous range of positions
+  std::vector<TrackDesc<T>> sdescs(nt_);
+  for (int gi = 0; gi < nt_; ++gi) sdescs[gi] = descs[order_[gi]];
   OMB_CU(d_descs.alloc(nt_, st));
-  OMB_CU(cudaMemcpyAsync(d_descs.p, descs.data(), nt_ * sizeof(TrackDesc<T>), cudaMemcpyHostToDevice, st));
+  OMB_CU(cudaMemcpyAsync(d_descs.p, sdescs.data(), nt_ * sizeof(TrackDesc<T>), cudaMemcpyHostToDevice, st));
   for (int par = 0; par < 2; ++par) {
     OMB_CU(d_uA[par].alloc(nt_, st));
     OMB_CU(d_uP[par].alloc(nt_, st));
@@ -273,47 +277,104 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
   const int grid_u = std::max(1, occ_u) * ctx_->num_sms;
   OMB_CU(gram_acc_.zero());
   OMB_CU(res_acc_.zero());
-  const int cb = (nt_ + 127) / 128;
+  // Two lanes of tracks (split by Σ M², the Gram cost) run their iterations on two streams,
+  // so one lane's latency-bound kernels (k_rr, k_control, k_newton, the prefix) overlap the
+  // other lane's streaming kernels.
+  int nl = nt_ >= 2 ? 2 : 1;
+  int lane_lo[2] = {0, nt_}, lane_hi[2] = {nt_, nt_};
+  if (nl == 2) {
+    double tot = 0, acc = 0;
+    for (int gi = 0; gi < nt_; ++gi) tot += (double)tracks_[order_[gi]].M * tracks_[order_[gi]].M;
+    int h = 1;
+    for (int gi = 0; gi < nt_ - 1; ++gi) {
+      acc += (double)tracks_[order_[gi]].M * tracks_[order_[gi]].M;
+      h = gi + 1;
+      if (acc >= 0.5 * tot) break;
+    }
+    lane_hi[0] = h; lane_lo[1] = h; lane_hi[1] = nt_;
+  }
+  OMB_CU(d_pre_.alloc(4 * ((size_t)nt_ + 1), st));
 
   const char* step = "";
-  auto iteration = [&](int par) -> cudaError_t {
+  auto iteration = [&](int par, int L, cudaStream_t s) -> cudaError_t {
     cudaError_t e = cudaSuccess;
     auto ok = [&](const char* name, cudaError_t r) { step = name; e = r; return r == cudaSuccess; };
-    if (!opt_.prec_diag)
-      for (const Group& g : groups_)
-        if (!ok("preconditioner pass", launch_op<T>(OP_P, d_uP[par].p + g.off, g.n, g.Nx, g.Ny, g.Mmax, ctx_->tw, st))) return e;
-    for (const Group& g : groups_)
-      if (!ok("HMkH pass", launch_op<T>(OP_HMKH, d_uH[par].p + g.off, g.n, g.Nx, g.Ny, 1, ctx_->tw, st))) return e;
-    k_newton<<<cb, 128, 0, st>>>(d_state_ptrs_.p, d_hmkh_ptrs_.p, d_hmkh_nb_.p, nt_, prm);
+    const int a = lane_lo[L], n = lane_hi[L] - lane_lo[L];
+    if (n <= 0) return e;
+    int* preg = d_pre_.p + (size_t)L * 2 * (nt_ + 1);
+    int* preu = preg + nt_ + 1;
+    // the lane's part of every grid group
+    auto for_groups = [&](auto&& f) -> bool {
+      for (const Group& g : groups_) {
+        const int lo = std::max(g.off, a), hi = std::min(g.off + g.n, a + n);
+        if (hi > lo && !f(g, lo, hi - lo)) return false;
+      }
+      return true;
+    };
+    if (!opt_.prec_diag &&
+        !for_groups([&](const Group& g, int off, int cnt) {
+          return ok("preconditioner pass", launch_op<T>(OP_P, d_uP[par].p + off, cnt, g.Nx, g.Ny, g.Mmax, ctx_->tw, s));
+        }))
+      return e;
+    if (!for_groups([&](const Group& g, int off, int cnt) {
+          return ok("HMkH pass", launch_op<T>(OP_HMKH, d_uH[par].p + off, cnt, g.Nx, g.Ny, 1, ctx_->tw, s));
+        }))
+      return e;
+    k_newton<<<(n + 127) / 128, 128, 0, s>>>(d_state_ptrs_.p + a, d_hmkh_ptrs_.p + a, d_hmkh_nb_.p + a, n, prm);
     if (!ok("k_newton", cudaGetLastError())) return e;
-    for (const Group& g : groups_)
-      if (!ok("operator pass", launch_op<T>(OP_M, d_uA[par].p + g.off, g.n, g.Nx, g.Ny, 3 * g.Mmax, ctx_->tw, st))) return e;
-    k_live_prefix<<<1, 1024, 0, st>>>(d_state_ptrs_.p, d_n2_.p, nt_, rg, UpdCfg<T>::R, d_pre_.p,
-                                      d_pre_.p + nt_ + 1);
+    if (!for_groups([&](const Group& g, int off, int cnt) {
+          return ok("operator pass", launch_op<T>(OP_M, d_uA[par].p + off, cnt, g.Nx, g.Ny, 3 * g.Mmax, ctx_->tw, s));
+        }))
+      return e;
+    k_live_prefix<<<1, 1024, 0, s>>>(d_state_ptrs_.p + a, d_n2_.p + a, n, rg, UpdCfg<T>::R, preg, preu);
     if (!ok("k_live_prefix", cudaGetLastError())) return e;
-    k_gram<T><<<grid_g, GramCfg<T>::NT, sm_gram, st>>>(d_descs.p, d_pre_.p, nt_, par, nmax, rg, gstages, d_err_.p);
+    k_gram<T><<<grid_g, GramCfg<T>::NT, sm_gram, s>>>(d_descs.p + a, preg, n, par, nmax, rg, gstages, d_err_.p);
     if (!ok("k_gram", cudaGetLastError())) return e;
-    k_rr<<<nt_, RR_NT, sm_rr, st>>>(d_state_ptrs_.p, d_gram_ptrs_.p, d_coef_ptrs_.p, d_coef32_ptrs_.p, nt_, prm);
+    k_rr<<<n, RR_NT, sm_rr, s>>>(d_state_ptrs_.p + a, d_gram_ptrs_.p + a, d_coef_ptrs_.p + a, d_coef32_ptrs_.p + a, n,
+                                 prm);
     if (!ok("k_rr", cudaGetLastError())) return e;
-    update_kernel<<<grid_u, UpdCfg<T>::NT, sm_upd, st>>>(d_descs.p, d_pre_.p + nt_ + 1, nt_, par, prm.prec_diag,
-                                                          d_err_.p);
+    update_kernel<<<grid_u, UpdCfg<T>::NT, sm_upd, s>>>(d_descs.p + a, preu, n, par, prm.prec_diag, d_err_.p);
     if (!ok("k_update", cudaGetLastError())) return e;
-    k_control<<<(nt_ + 3) / 4, 128, 0, st>>>(d_state_ptrs_.p, d_res_ptrs_.p, nt_, prm);
+    k_control<<<(n + 3) / 4, 128, 0, s>>>(d_state_ptrs_.p + a, d_res_ptrs_.p + a, n, prm);
     ok("k_control", cudaGetLastError());
     return e;
   };
 
   // two eager iterations (they also size the kernels' shared memory), then the graph
-  for (int par = 0; par < 2; ++par) {
-    const cudaError_t e = iteration(par);
-    if (e != cudaSuccess) return cuda_fail(e, step);
-  }
+  for (int par = 0; par < 2; ++par)
+    for (int L = 0; L < nl; ++L) {
+      const cudaError_t e = iteration(par, L, st);
+      if (e != cudaSuccess) return cuda_fail(e, step);
+    }
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  cudaStream_t st2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  OMB_CU(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
+  OMB_CU(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+  OMB_CU(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+  auto release = [&]() {
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (st2) cudaStreamDestroy(st2);
+  };
   OMB_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-  cudaError_t ce = iteration(0);
-  if (ce == cudaSuccess) ce = iteration(1);
+  cudaError_t ce = cudaSuccess;
+  if (nl == 2) {
+    ce = cudaEventRecord(ev_fork, st);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(st2, ev_fork, 0);
+  }
+  for (int par = 0; par < 2 && ce == cudaSuccess; ++par) {
+    ce = iteration(par, 0, st);
+    if (ce == cudaSuccess && nl == 2) ce = iteration(par, 1, st2);
+  }
+  if (nl == 2) {
+    const cudaError_t j1 = cudaEventRecord(ev_join, st2);
+    const cudaError_t j2 = cudaStreamWaitEvent(st, ev_join, 0);
+    if (ce == cudaSuccess) ce = j1 != cudaSuccess ? j1 : j2;
+  }
   cudaError_t ee = cudaStreamEndCapture(st, &graph);
+  release();
   if (ce != cudaSuccess) { if (graph) cudaGraphDestroy(graph); return cuda_fail(ce, step); }
   OMB_CU(ee);
   OMB_CU(cudaGraphInstantiate(&exec, graph, 0));
@@ -378,7 +439,6 @@ int Engine::run() {
   OMB_CU(hmkh_part_.alloc((size_t)nt_ * 2 * 512, st));
   OMB_CU(coef_.zero());
   OMB_CU(coef32_.zero());
-  OMB_CU(d_pre_.alloc(2 * ((size_t)nt_ + 1), st));
   OMB_CU(d_err_.alloc(1, st));
   OMB_CU(d_err_.zero());
   std::vector<TrackState*> sp(nt_);
@@ -387,16 +447,17 @@ int Engine::run() {
   std::vector<double*> rp(nt_), hp(nt_);
   std::vector<int> hnb(nt_);
   std::vector<long long> n2s(nt_);
-  for (int t = 0; t < nt_; ++t) {
+  for (int gi = 0; gi < nt_; ++gi) {  // position gi holds track order_[gi]
+    const int t = order_[gi];
     const Problem& P = (*probs_)[tracks_[t].prob];
-    sp[t] = d_states_.p + t;
-    gp[t] = gram_acc_.p + (size_t)t * 2 * NMAX * NMAX;
-    cp[t] = coef_.p + (size_t)t * 2 * NMAX * MMAX;
-    cp32[t] = coef32_.p + (size_t)t * 2 * NMAX * MMAX;
-    rp[t] = res_acc_.p + (size_t)t * MMAX;
-    hp[t] = hmkh_part_.p + (size_t)t * 2 * 512;
-    hnb[t] = row_blocks(P.Nx, P.Ny);
-    n2s[t] = 2 * (long long)P.N();
+    sp[gi] = d_states_.p + t;
+    gp[gi] = gram_acc_.p + (size_t)t * 2 * NMAX * NMAX;
+    cp[gi] = coef_.p + (size_t)t * 2 * NMAX * MMAX;
+    cp32[gi] = coef32_.p + (size_t)t * 2 * NMAX * MMAX;
+    rp[gi] = res_acc_.p + (size_t)t * MMAX;
+    hp[gi] = hmkh_part_.p + (size_t)t * 2 * 512;
+    hnb[gi] = row_blocks(P.Nx, P.Ny);
+    n2s[gi] = 2 * (long long)P.N();
   }
   OMB_CU(d_state_ptrs_.alloc(nt_, st));
   OMB_CU(d_gram_ptrs_.alloc(nt_, st));

@@ -325,8 +325,14 @@ __global__ void k_control(TrackState* const* __restrict__ states, double* const*
       if (s.newton_steps > 0 && maxres < prm.tau_phase && fabs(s.dk_last) < prm.dk_phase) {
         finish(s, TS_PHASE_DONE); return;
       }
+      // stalled at the FP32 floor: the FP64 phase takes over, with or without a Newton step
+      // here (a warm start can give a k so close that λ_b − ω² never dominates the
+      // residual); plateaus far above the floor keep iterating in FP32
+      const bool at_floor = maxres < 4.0 * prm.tau_phase;
+      if (at_floor && s.stall >= 8) { finish(s, TS_PHASE_DONE); return; }
       if (s.newton_steps > 0 && s.stall >= 8) { finish(s, TS_PHASE_DONE); return; }
-      if (s.since_newton >= 2 && maxres < fmax(0.1 * fabs(dw2), prm.tau_phase)) s.hmkh_ncol = 1;
+      if (s.since_newton >= 2 && (maxres < fmax(0.1 * fabs(dw2), prm.tau_phase) || (at_floor && s.stall >= 4)))
+        s.hmkh_ncol = 1;
     }
   } else {  // MODE_NEWTON_OUTER: the reference loop, a step after each converged eigensolve
     if (maxres < prm.tol) s.hmkh_ncol = 1;
