@@ -294,6 +294,11 @@ int omb_batch_results(omb_batch* b, omb_result* out) {
   OMB_CU(cudaSetDevice(b->ctx->device));
   bool all_ok = true;
   b->d2h = 0;
+  if (b->canon)
+    for (auto& e : b->engines) {
+      const int rc = e->canonicalize_results();
+      if (rc) return rc;
+    }
   for (size_t w = 0; w < b->who.size(); ++w) {
     const int i = b->who[w].inst, band0 = b->who[w].band0;
     Engine& E = *b->engines[b->who[w].eng];
@@ -315,24 +320,16 @@ int omb_batch_results(omb_batch* b, omb_result* out) {
       b->d2h += 8 * 4 + 4 * 3;
       all_ok = all_ok && s.status == TS_CONVERGED;
       if (r.evecs) {
-        double* v = r.evecs + 2 * n2 * band;
-        int rc = OMB_OK;
-        if (b->canon) {
-          // phase gauge on the device: the largest E component real and positive
-          long long idx;
-          double re, im;
-          rc = E.result_efield_argmax(t, rb, &idx, &re, &im);
-          if (rc) return rc;
-          b->d2h += 24;
-          const double a = std::hypot(re, im);
-          if (a > 0) rc = E.rotate_result(t, rb, re / a, -im / a);
-          if (rc) return rc;
-        }
-        rc = E.fetch_result(t, rb, v);
+        // (phase gauge already applied on the device above)
+        const int rc = E.fetch_result_async(t, rb, r.evecs + 2 * n2 * band);
         if (rc) return rc;
-        b->d2h += (int64_t)(2 * n2 * sizeof(double));
+        b->d2h += (int64_t)(2 * n2 * sizeof(double)) + (b->canon ? 24 : 0);
       }
     }
+  }
+  for (auto& e : b->engines) {
+    const int rc = e->sync();
+    if (rc) return rc;
   }
   if (!all_ok) return fail(OMB_ERR_NOT_CONVERGED, "one or more bands did not converge (see the per-band status)");
   return OMB_OK;

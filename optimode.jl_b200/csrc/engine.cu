@@ -3,6 +3,8 @@
 #include <cmath>
 #include <cstring>
 
+#include <map>
+
 #include "engine.h"
 #include "vec.cuh"
 
@@ -576,6 +578,72 @@ int Engine::fetch_block_column(int t, int col, double* out) {
     OMB_CU(cudaStreamSynchronize(st));
   }
   OMB_CU(cudaStreamSynchronize(st));
+  return OMB_OK;
+}
+
+int Engine::fetch_result_async(int t, int b, double* out) {
+  const size_t n2 = 2 * (*probs_)[tracks_[t].prob].N();
+  OMB_CU(cudaMemcpyAsync(out, store_.p + store_off_[t] + (size_t)b * n2, n2 * sizeof(double2),
+                         cudaMemcpyDeviceToHost, ctx_->stream));
+  return OMB_OK;
+}
+
+int Engine::sync() {
+  OMB_CU(cudaStreamSynchronize(ctx_->stream));
+  return OMB_OK;
+}
+
+int Engine::canonicalize_results() {
+  cudaStream_t st = ctx_->stream;
+  // finished results (track, band), grouped by grid
+  std::map<std::pair<int, int>, std::vector<std::pair<int, int>>> groups;
+  for (int t = 0; t < nt_; ++t) {
+    const Problem& P = (*probs_)[tracks_[t].prob];
+    for (int b = 0; b < (int)snaps_[t].size(); ++b) groups[{P.Nx, P.Ny}].push_back({t, b});
+  }
+  constexpr int CHUNK = 64;
+  for (const auto& kv : groups) {
+    const int Nx = kv.first.first, Ny = kv.first.second;
+    const size_t N = (size_t)Nx * Ny, n2 = 2 * N;
+    const auto& all = kv.second;
+    for (size_t c0 = 0; c0 < all.size(); c0 += CHUNK) {
+      const int cnt = (int)std::min<size_t>(CHUNK, all.size() - c0);
+      DevBuf<double> kd, red;
+      DevBuf<double2> scr;
+      DevBuf<OpUnit<double>> du;
+      OMB_CU(kd.alloc(cnt, st));
+      OMB_CU(red.alloc(3 * (size_t)cnt, st));
+      OMB_CU(scr.alloc(3 * N * (size_t)cnt, st));
+      OMB_CU(du.alloc(cnt, st));
+      std::vector<double> kh(cnt);
+      std::vector<OpUnit<double>> uh(cnt);
+      for (int j = 0; j < cnt; ++j) {
+        const int t = all[c0 + j].first, b = all[c0 + j].second;
+        kh[j] = snaps_[t][b].k;
+        OpUnit<double> u = make_unit<double>((*probs_)[tracks_[t].prob]);
+        u.in = store_.p + store_off_[t] + (size_t)b * n2;
+        u.scr = scr.p + (size_t)j * 3 * N;
+        u.k_dev = kd.p + j;
+        u.in_cs = (long long)n2; u.scr_cs = 3 * (long long)N; u.ncol = 1;
+        uh[j] = u;
+      }
+      OMB_CU(cudaMemcpyAsync(kd.p, kh.data(), cnt * sizeof(double), cudaMemcpyHostToDevice, st));
+      OMB_CU(cudaMemcpyAsync(du.p, uh.data(), cnt * sizeof(OpUnit<double>), cudaMemcpyHostToDevice, st));
+      OMB_CU(launch_op<double>(OP_EFIELD, du.p, cnt, Nx, Ny, 1, ctx_->tw, st));
+      k_argmax_abs2<double><<<cnt, 1024, 0, st>>>(scr.p, (long long)N, 3 * (long long)N, cnt, red.p);
+      OMB_CU(cudaGetLastError());
+      std::vector<double> h(3 * (size_t)cnt);
+      OMB_CU(cudaMemcpyAsync(h.data(), red.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+      OMB_CU(cudaStreamSynchronize(st));  // also keeps kh/uh alive until the uploads are done
+      for (int j = 0; j < cnt; ++j) {
+        const double re = h[3 * j + 1], im = h[3 * j + 2], a = std::hypot(re, im);
+        if (a > 0) {
+          const int rc = rotate_result(all[c0 + j].first, all[c0 + j].second, re / a, -im / a);
+          if (rc) return rc;
+        }
+      }
+    }
+  }
   return OMB_OK;
 }
 

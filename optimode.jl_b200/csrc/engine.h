@@ -56,6 +56,12 @@ class Engine {
   int result_efield_argmax(int t, int b, long long* idx, double* re, double* im);
   // multiply result b of track t by the unit phase c + i s on the device
   int rotate_result(int t, int b, double c, double s);
+  // phase gauge of every finished result on the device: the largest E component of each
+  // becomes real and positive (batched per grid: one E-field pass, one argmax, one sync)
+  int canonicalize_results();
+  // queue the copy of result b of track t into host memory (no synchronisation)
+  int fetch_result_async(int t, int b, double* out);
+  int sync();
   int64_t graph_launches() const { return launches_; }
   int64_t kernel_launches() const { return kernels_; }
   int max_iterations() const;

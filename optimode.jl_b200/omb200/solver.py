@@ -120,8 +120,11 @@ class Batch:
             pass
 
 
-def _unmarshal(outs, return_info):
-    ret = [(o["kmags"].copy(), [o["evecs"][:, j].copy() for j in range(o["kmags"].size)]) for o in outs]
+def _unmarshal(outs, return_info, copy=True):
+    # copy=False: the output arrays are fresh and owned by these results (one-shot calls),
+    # so the eigenvectors are returned as column views instead of copies
+    c = (lambda a: a.copy()) if copy else (lambda a: a)
+    ret = [(c(o["kmags"]), [c(o["evecs"][:, j]) for j in range(o["kmags"].size)]) for o in outs]
     if return_info:
         info = [{k: o[k].copy() for k in ("residuals", "dw2dk", "status", "iterations", "newton_steps")}
                 for o in outs]
@@ -146,7 +149,8 @@ def _marshal(problems):
         n2 = 2 * g.N
         G, ng = _guess_block(pr.get("Hguess"), n2)
         o = {
-            "kmags": np.zeros(nev), "evecs": np.zeros((n2, nev), dtype=np.complex128, order="F"),
+            # every entry of evecs is written by the library (no need to clear 16·n2·nev bytes)
+            "kmags": np.zeros(nev), "evecs": np.empty((n2, nev), dtype=np.complex128, order="F"),
             "residuals": np.zeros(nev), "dw2dk": np.zeros(nev),
             "status": np.zeros(nev, dtype=np.int32), "iterations": np.zeros(nev, dtype=np.int32),
             "newton_steps": np.zeros(nev, dtype=np.int32),
@@ -191,7 +195,7 @@ def solve_k_batch(problems, solver: B200Solver | None = None, k_tol=1e-8, eig_to
     rc = lib.omb_solve_k(ctx.handle, insts, len(problems), ctypes.byref(opt), results)
     if rc != 0 and (raise_on_failure or rc != 3):
         _lib.check(rc)
-    return _unmarshal(outs, return_info)
+    return _unmarshal(outs, return_info, copy=False)
 
 
 def solve_k(omega: float, eps_inv, grid: Grid, solver: B200Solver | None = None, nev: int = 1,
