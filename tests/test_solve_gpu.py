@@ -159,3 +159,26 @@ def test_kguess_bands(omb, case):
     ret = omb.solve_k_batch([{"omega": OMEGA0, "eps_inv": ei, "grid": g, "nev": 2,
                               "kguess_bands": km_ref * 1.01}])
     assert np.allclose(ret[0][0], km_ref, rtol=1e-9)
+
+
+def test_uneven_batch(omb):
+    """One batch mixing grids, cells, frequencies and band counts (the shape of the
+    uneven-grid sweep): every instance matches its own oracle solve."""
+    specs = [  # (Nx, Ny, Dx, Dy, ω, nev, bump)
+        (24, 16, 6.0, 4.0, 1 / 1.55, 2, P_WG),
+        (32, 24, 6.0, 4.5, 1 / 1.45, 3, (4.6, 2.1, 1.1, 0.7)),
+        (20, 20, 5.0, 5.0, 1 / 1.60, 1, (3.98, 2.09, 0.9, 0.9)),
+        (24, 16, 6.0, 4.0, 1 / 1.50, 3, P_WG),
+        (48, 32, 6.0, 4.0, 1 / 1.55, 2, P_WG),
+    ]
+    probs, refs = [], []
+    for Nx, Ny, Dx, Dy, w, nev, p in specs:
+        ei = gaussian_epsinv(p, Dx, Dy, Nx, Ny)
+        probs.append({"omega": w, "eps_inv": ei, "grid": omb.Grid(Dx, Dy, Nx, Ny), "nev": nev})
+        refs.append(O.solve_k(w, ei, O.Grid(Dx, Dy, Nx, Ny), nev=nev, k_tol=1e-12, eig_tol=1e-11)[0])
+    for warm in ("none", "sweep"):
+        out, info = omb.solve_k_batch(probs, omb.B200Solver(warm_start=warm), return_info=True)
+        for (km, kv), i, ref, pr in zip(out, info, refs, probs):
+            assert np.all(i["status"] == 0)
+            assert np.allclose(km, ref, rtol=1e-9)
+            assert len(kv) == pr["nev"] and all(v.shape == (2 * pr["grid"].N,) for v in kv)
