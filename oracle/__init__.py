@@ -46,6 +46,7 @@ from .maxwell import (  # noqa: F401
 )
 from .lobpcg import lobpcg  # noqa: F401
 from .solve import solve_omega2, solve_k  # noqa: F401
+from .analysis import group_index, tensor_product  # noqa: F401
 from .adjoint import (  # noqa: F401
     eig_adjt, epsinv_bar, grad_k_mag_m_n, solve_k_pullback, sliceinv_3x3,
     sliceinv_3x3_pullback,

@@ -150,3 +150,44 @@ def test_sliceinv_pullback_vs_fd():
     dA = rng.standard_normal(A.shape)
     f = lambda t: np.sum(Ybar * O.sliceinv_3x3(A + t * dA))
     assert np.isclose(np.sum(Abar * dA), _fd5(f, 0.0, 1e-4), rtol=1e-8)
+
+
+def _dispersive_case():
+    from conftest import P_WG, gaussian_epsinv
+    g = O.Grid(6.0, 4.0, 24, 16)
+    ei0 = gaussian_epsinv(P_WG)
+    eps0 = np.zeros_like(ei0)
+    for a in range(3):
+        eps0[a, a] = 1.0 / ei0[a, a]
+    x = -3 + np.arange(24) * 0.25
+    y = -2 + np.arange(16) * 0.25
+    X, Y = np.meshgrid(x, y, indexing="ij")
+    bump = np.exp(-(X ** 2 / 1.0 + Y ** 2 / 0.36))
+    deps = np.zeros_like(eps0)
+    for a in range(3):
+        deps[a, a] = 0.8 * bump + 0.1
+    deps[0, 1] = deps[1, 0] = 0.05 * bump
+    return g, eps0, deps
+
+
+def _epsinv_at(eps0, deps, w, w0):
+    e = eps0 + deps * (w - w0)
+    return np.moveaxis(np.linalg.inv(np.moveaxis(e, (0, 1), (-2, -1))), (-2, -1), (0, 1))
+
+
+def test_group_index_matches_finite_difference():
+    """n_g = dk/dω (lib/ModeAnalysis/src/group_index.jl:21-29) against central differences
+    of solve_k with ε(ω) = ε₀ + (∂ε/∂ω)(ω − ω₀) (the reference's dk/dω check,
+    ME/test/runtests.jl:94, rtol 1e-4; here it holds to ~1e-9)."""
+    g, eps0, deps = _dispersive_case()
+    w0, h = 1 / 1.55, 1e-4
+    km, kv = O.solve_k(w0, _epsinv_at(eps0, deps, w0, w0), g, nev=2, k_tol=1e-13, eig_tol=1e-12)
+    kp = O.solve_k(w0 + h, _epsinv_at(eps0, deps, w0 + h, w0), g, nev=2, k_tol=1e-13, eig_tol=1e-12)[0]
+    kmn = O.solve_k(w0 - h, _epsinv_at(eps0, deps, w0 - h, w0), g, nev=2, k_tol=1e-13, eig_tol=1e-12)[0]
+    for b in range(2):
+        ng = O.group_index(km[b], kv[b], w0, _epsinv_at(eps0, deps, w0, w0), deps, g)
+        fd = (kp[b] - kmn[b]) / (2 * h)
+        assert abs(ng - fd) / fd < 1e-7
+        # without dispersion the formula reduces to 2ω/(∂ω²/∂k)
+        ng0 = O.group_index(km[b], kv[b], w0, _epsinv_at(eps0, deps, w0, w0), None, g)
+        assert ng0 < ng
