@@ -51,14 +51,26 @@ def rank_omegas(n_om: int, rank: int = 0, world: int = 1):
     return allw[rank * n_om:(rank + 1) * n_om]
 
 
-def workload(n_inst: int, rank: int = 0, world: int = 1):
-    from omb200 import Grid
+def ridge_epsinv(g, width: float, smoothing: str = "gpu"):
+    """Smoothed ε⁻¹ of the LiNbO₃ ridge of top width `width`: the library's device smoothing,
+    or (for the CPU arms, which must not run this library) the oracle's CPU restatement,
+    which the GPU tests hold bit-identical to it."""
     from omb200 import geometry as G
+    shapes, bg = G.ln_ridge_shapes(g, top_width=width)
+    if smoothing == "gpu":
+        return G.smooth_epsinv(shapes, bg, g)
+    sys.path.insert(0, ROOT)
+    import oracle.smoothing as OS
+    return OS.smooth_epsinv_constant(shapes, bg, g)
+
+
+def workload(n_inst: int, rank: int = 0, world: int = 1, smoothing: str = "gpu"):
+    from omb200 import Grid
     g = Grid(DX, DY, NX, NY)
     n_w = len(WIDTHS)
     n_om = max(1, (n_inst + n_w - 1) // n_w)
     omegas = rank_omegas(n_om, rank, world)
-    eps = {w: G.ln_ridge(g, top_width=w) for w in WIDTHS}
+    eps = {w: ridge_epsinv(g, w, smoothing) for w in WIDTHS}
     probs = []
     for i in range(n_inst):
         w = WIDTHS[i % n_w]
@@ -135,10 +147,9 @@ def cpu_baseline(seconds_budget: float):
     workload: band 0 of the 1.5 μm ridge at ω = 1/1.55, all host threads for the FFTs."""
     sys.path.insert(0, ROOT)
     import oracle as O
-    from omb200 import geometry as G
     from omb200 import Grid
     g = Grid(DX, DY, NX, NY)
-    ei = G.ln_ridge(g, top_width=1.5)
+    ei = ridge_epsinv(g, 1.5, "oracle")
     cores = os.cpu_count() or 1
     O.maxwell.FFT_WORKERS = cores
     t0 = time.perf_counter()
@@ -154,7 +165,7 @@ def run_reference(args, rank):
     sys.path.insert(0, ROOT)
     import oracle as O
     from omb200 import Grid
-    g, probs = workload(max(args.instances, 1))
+    g, probs = workload(max(args.instances, 1), smoothing="oracle")
     cores = os.cpu_count() or 1
     O.maxwell.FFT_WORKERS = cores
     og = O.Grid(DX, DY, NX, NY)

@@ -237,6 +237,63 @@ int omb_batch_destroy(omb_batch* b);
 int omb_profile_apply(omb_ctx* ctx, int op, int precision, const omb_grid* grid, double k,
                       const double* epsinv, int ncol, int nbatch, int reps, double* seconds);
 
+/* ---------------------------------------------------------------------------------
+ * Kottke sub-pixel smoothing (the solver's input generator, lib/DielectricSmoothing)
+ * --------------------------------------------------------------------------------- */
+
+typedef struct omb_smoothing_plan omb_smoothing_plan;
+
+/* fill fraction of an interface pixel */
+#define OMB_FILL_PLANE 0 /* the reference's volfrac: the voxel's area on the inner side of the
+                            tangent line through the nearest surface point              */
+#define OMB_FILL_EXACT 1 /* the exact area of polygon ∩ voxel                            */
+
+/* pixel kinds (SmoothingPlan's _PLAN_UNIFORM/_INTERFACE/_MULTI) */
+#define OMB_PIXEL_UNIFORM 1
+#define OMB_PIXEL_INTERFACE 2
+#define OMB_PIXEL_MULTI 3
+
+/* Frequency-independent geometry pass on the device.  Replaces
+ * smoothing_plan(shapes, minds, grid) (lib/DielectricSmoothing/src/smoothing_plan.jl:70-100):
+ * corners (src/grid.jl:271-312), corner_sinds/proc_sinds (src/smooth.jl:24-72) and the
+ * interface geometry of smooth_ε_single! (src/smooth.jl:80-121).
+ *   shapes : `nshapes` convex polygons in priority order (the first containing a point
+ *            wins); polygon s has nverts[s] ∈ [3, 64] vertices, stored one polygon after
+ *            another in `verts` as (x, y) pairs (either orientation)
+ *   minds  : nshapes + 1 material columns in [0, 255] (0-based), the background last
+ * Blocks until the plan is built. */
+int omb_smoothing_plan_create(omb_ctx* ctx, const omb_grid* grid, int32_t nshapes, const int32_t* nverts,
+                              const double* verts, const int32_t* minds, int32_t fill_rule,
+                              omb_smoothing_plan** out);
+
+/* Contents of a plan, pixels in corners(grid) order (x fastest); any pointer may be NULL.
+ *   counts[3]      : uniform, interface and multi-material pixels
+ *   kind[N]        : OMB_PIXEL_*
+ *   mats[4N]       : material columns (uniform: [a]; interface: [a, b]; multi: the four
+ *                    corners' columns; unused entries −1)
+ *   rvol[N]        : fill fraction of material a (interface pixels; else 0)
+ *   normal[2N]     : outward interface normal (nx, ny) of the higher-priority shape */
+int omb_smoothing_plan_query(const omb_smoothing_plan* plan, int64_t* counts, uint8_t* kind, int32_t* mats,
+                             double* rvol, double* normal);
+
+/* Material pass for `nsets` material tables at once (e.g. one per frequency).  Replaces
+ * smooth_ε(plan, mat_vals) (smoothing_plan.jl:120-140; per pixel the three branches of
+ * smooth_ε_single!, with the dispersive Kottke kernel εₑ_∂ωεₑ_∂²ωεₑ of src/kottke.jl:218-268)
+ * and, fused, sliceinv_3x3 of its ε slice (lib/MaxwellEigenmodes/src/linalg.jl:126-147).
+ *   mat_vals : Float64 (27, nmat, nsets); column = vcat(vec(ε), vec(∂ωε), vec(∂²ωε))
+ *   eps      : Float64 (3, 3, 3, Nx, Ny, nsets) or NULL
+ *   epsinv   : Float64 (3, 3, Nx, Ny, nsets) or NULL — the solver's ε⁻¹ input */
+int omb_smooth_eps(omb_smoothing_plan* plan, const double* mat_vals, int32_t nmat, int32_t nsets,
+                   double* eps, double* epsinv);
+
+/* As omb_smooth_eps with device outputs, stream-ordered on `stream` (a cudaStream_t, or
+ * NULL for the context's stream); returns once the work is queued. */
+int omb_smooth_eps_device(omb_smoothing_plan* plan, const double* mat_vals, int32_t nmat, int32_t nsets,
+                          double* d_eps, double* d_epsinv, void* stream);
+
+/* Waits for the device, then frees the plan. */
+int omb_smoothing_plan_destroy(omb_smoothing_plan* plan);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,633 @@
+// Kottke sub-pixel smoothing on the device: the geometry pass (`smoothing_plan`) and the
+// per-frequency material pass (`smooth_ε(plan, mat_vals)`) of lib/DielectricSmoothing, with
+// `sliceinv_3x3` of the ε slice fused into the material pass so the solver's ε⁻¹ input is
+// produced in the same sweep over the pixels.
+//
+// Reference semantics (paths relative to the OptiMode.jl project root):
+//   corners          lib/DielectricSmoothing/src/grid.jl:271-312 (myrange, grid.jl:107-110)
+//   classification   corner_sinds / proc_sinds, src/smooth.jl:24-72
+//   interface pixel  smooth_ε_single! / _interface_geometry, src/smooth.jl:80-121
+//   Kottke kernel    normcart, τ_trans, τ⁻¹_trans, avg_param_rot, J2 jet and the lab-frame
+//                    εₑ_∂ωεₑ_∂²ωεₑ, src/kottke.jl:13-20, 44-99, 114-137, 218-268
+//   plan / apply     SmoothingPlan, smoothing_plan, smooth_ε(plan, mat_vals),
+//                    src/smoothing_plan.jl:26-140
+//   ε⁻¹              sliceinv_3x3, lib/MaxwellEigenmodes/src/linalg.jl:126-147
+// GeometryPrimitives' polygon queries (un-vendored in the reference) are restated for convex
+// polygons: inclusive point-in-polygon, the clamped projection onto the nearest edge (first
+// edge on ties) with that edge's outward normal, and the voxel fraction on the inner side of
+// the tangent line through that point ("plane" fill) or the exact polygon ∩ voxel area
+// ("exact" fill).
+//
+// This file is compiled without floating-point contraction (-fmad=false): every value is a
+// chain of individually rounded IEEE operations in a fixed order, so corner classification is
+// exact and the results reproduce a CPU restatement that performs the same operations.
+//
+// Layout in HBM.  Plan: per pixel (x fastest) a uint2 code {kind | m0<<8 | m1<<16 | m2<<24,
+// m3} of the pixel kind and four 8-bit material columns, the fill fraction (double) and the
+// interface normal (double2) — 32 B per pixel.  Apply: outputs are the reference's column-major
+// (3, 3, 3, Nx, Ny) — 27 contiguous doubles per pixel — and (3, 3, Nx, Ny) ε⁻¹, one block of
+// each per material set; a CTA stages its 128 pixels' results in shared memory and writes them
+// back as one contiguous, coalesced range.
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "context.h"
+
+namespace omb {
+
+namespace sm {
+
+constexpr int KIND_UNIFORM = 1;
+constexpr int KIND_INTERFACE = 2;
+constexpr int KIND_MULTI = 3;
+constexpr int MAX_VERTS = 64;          // vertices per polygon
+constexpr int MAX_SHAPES = 255;        // shapes per geometry (slot 255 = background at most)
+constexpr int MAX_MATS = 256;          // material columns (8-bit indices)
+constexpr int CLIP_CAP = MAX_VERTS + 8;
+constexpr int PLAN_NT = 128;
+constexpr int APPLY_NT = 128;
+
+struct Shapes {
+  const double2* verts;  // counter-clockwise vertices of every shape, shape after shape
+  const int* voff;       // shape s owns verts[voff[s], voff[s+1])
+  const int* minds;      // material column of slot s (nshapes + 1 slots, background last)
+  int nshapes;
+};
+
+struct Axis {
+  double a, step;  // corner i at a + step·i
+};
+
+__device__ __forceinline__ double corner(const Axis& ax, int i) { return ax.a + ax.step * (double)i; }
+
+__device__ __forceinline__ double edge_cross(double2 a, double2 b, double px, double py) {
+  return (b.x - a.x) * (py - a.y) - (b.y - a.y) * (px - a.x);
+}
+
+__device__ int slot_at(const Shapes& sh, double px, double py) {
+  for (int s = 0; s < sh.nshapes; ++s) {
+    const int v0 = sh.voff[s], v1 = sh.voff[s + 1];
+    bool in = true;
+    for (int i = v0; i < v1 && in; ++i) {
+      const int j = (i + 1 < v1) ? i + 1 : v0;
+      in = edge_cross(sh.verts[i], sh.verts[j], px, py) >= 0.0;
+    }
+    if (in) return s;
+  }
+  return sh.nshapes;
+}
+
+struct Surf {
+  double r0x, r0y, nx, ny;
+};
+
+__device__ Surf surfpt_nearby(const Shapes& sh, int s, double cx, double cy) {
+  const int v0 = sh.voff[s], v1 = sh.voff[s + 1];
+  double best = INFINITY;
+  Surf out{0.0, 0.0, 1.0, 0.0};
+  for (int i = v0; i < v1; ++i) {
+    const int j = (i + 1 < v1) ? i + 1 : v0;
+    const double2 a = sh.verts[i], b = sh.verts[j];
+    const double dx = b.x - a.x, dy = b.y - a.y;
+    const double dd = dx * dx + dy * dy;
+    double t = ((cx - a.x) * dx + (cy - a.y) * dy) / dd;
+    t = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+    const double px = a.x + t * dx, py = a.y + t * dy;
+    const double ex = cx - px, ey = cy - py;
+    const double d2 = ex * ex + ey * ey;
+    if (d2 < best) {
+      best = d2;
+      const double L = sqrt(dd);
+      out = Surf{px, py, dy / L, -dx / L};
+    }
+  }
+  return out;
+}
+
+// One Sutherland–Hodgman step over `n` vertices (keep f ≥ 0); returns the new count.
+template <typename F>
+__device__ int clip_step(const double2* in, int n, double2* out, F f) {
+  int m = 0;
+  for (int j = 0; j < n; ++j) {
+    const double2 p = in[j], q = in[(j + 1 < n) ? j + 1 : 0];
+    const double sp = f(p), sq = f(q);
+    if (sp >= 0.0 && m < CLIP_CAP) out[m++] = p;
+    if ((sp >= 0.0) != (sq >= 0.0) && m < CLIP_CAP) {
+      const double t = sp / (sp - sq);
+      out[m++] = make_double2(p.x + t * (q.x - p.x), p.y + t * (q.y - p.y));
+    }
+  }
+  return m;
+}
+
+__device__ double poly_area(const double2* p, int n) {
+  if (n < 3) return 0.0;
+  double s = 0.0;
+  for (int j = 0; j < n; ++j) {
+    const double2 a = p[j], b = p[(j + 1 < n) ? j + 1 : 0];
+    s += a.x * b.y - b.x * a.y;
+  }
+  return 0.5 * fabs(s);
+}
+
+__device__ double volfrac_plane(double x0, double x1, double y0, double y1, const Surf& sf) {
+  double2 box[4] = {make_double2(x0, y0), make_double2(x1, y0), make_double2(x1, y1), make_double2(x0, y1)};
+  double2 out[8];
+  int m = 0;
+  for (int j = 0; j < 4; ++j) {
+    const double2 p = box[j], q = box[(j + 1) & 3];
+    const double sp = -((p.x - sf.r0x) * sf.nx + (p.y - sf.r0y) * sf.ny);
+    const double sq = -((q.x - sf.r0x) * sf.nx + (q.y - sf.r0y) * sf.ny);
+    if (sp >= 0.0) out[m++] = p;
+    if ((sp >= 0.0) != (sq >= 0.0)) {
+      const double t = sp / (sp - sq);
+      out[m++] = make_double2(p.x + t * (q.x - p.x), p.y + t * (q.y - p.y));
+    }
+  }
+  return poly_area(out, m) / ((x1 - x0) * (y1 - y0));
+}
+
+__device__ double volfrac_exact(const Shapes& sh, int s, double x0, double x1, double y0, double y1) {
+  double2 A[CLIP_CAP], B[CLIP_CAP];
+  A[0] = make_double2(x0, y0); A[1] = make_double2(x1, y0); A[2] = make_double2(x1, y1); A[3] = make_double2(x0, y1);
+  int n = 4;
+  double2* cur = A;
+  double2* nxt = B;
+  const int v0 = sh.voff[s], v1 = sh.voff[s + 1];
+  for (int i = v0; i < v1; ++i) {
+    const int j = (i + 1 < v1) ? i + 1 : v0;
+    const double2 a = sh.verts[i], b = sh.verts[j];
+    n = clip_step(cur, n, nxt, [&](double2 p) { return edge_cross(a, b, p.x, p.y); });
+    double2* t = cur; cur = nxt; nxt = t;
+    if (n == 0) return 0.0;
+  }
+  return poly_area(cur, n) / ((x1 - x0) * (y1 - y0));
+}
+
+// Geometry pass: one thread per pixel.
+__global__ void __launch_bounds__(PLAN_NT) k_smooth_plan(Shapes sh, Axis ax, Axis ay, int Nx, int Ny, int fill,
+                                                         uint2* __restrict__ code, double* __restrict__ rvol,
+                                                         double2* __restrict__ nrm,
+                                                         unsigned long long* __restrict__ counts) {
+  __shared__ unsigned int cnt[3];
+  if (threadIdx.x < 3) cnt[threadIdx.x] = 0;
+  __syncthreads();
+  const long long N = (long long)Nx * Ny;
+  const long long v = (long long)blockIdx.x * PLAN_NT + threadIdx.x;
+  if (v < N) {
+    const int ix = (int)(v % Nx), iy = (int)(v / Nx);
+    const double x0 = corner(ax, ix), x1 = corner(ax, ix + 1);
+    const double y0 = corner(ay, iy), y1 = corner(ay, iy + 1);
+    // corners (x0,y0), (x0,y1), (x1,y1), (x1,y0)
+    const int c0 = slot_at(sh, x0, y0), c1 = slot_at(sh, x0, y1);
+    const int c2 = slot_at(sh, x1, y1), c3 = slot_at(sh, x1, y0);
+    const int lo = min(min(c0, c1), min(c2, c3)), hi = max(max(c0, c1), max(c2, c3));
+    int nd = 1;
+    bool mid = false;  // a third distinct slot strictly between lo and hi
+    for (int c : {c0, c1, c2, c3}) mid |= (c != lo && c != hi);
+    if (hi != lo) nd = mid ? 3 : 2;
+    uint2 cd;
+    double r = 0.0;
+    double2 n = make_double2(0.0, 0.0);
+    if (nd == 1) {
+      cd = make_uint2(KIND_UNIFORM | ((unsigned)sh.minds[lo] << 8), 0u);
+    } else if (nd == 2) {
+      const double cx = (((x0 + x0) + x1) + x1) / 4.0;
+      const double cy = (((y0 + y1) + y1) + y0) / 4.0;
+      const Surf sf = surfpt_nearby(sh, lo, cx, cy);
+      r = fill == 0 ? volfrac_plane(x0, x1, y0, y1, sf) : volfrac_exact(sh, lo, x0, x1, y0, y1);
+      r = r < 0.0 ? 0.0 : (r > 1.0 ? 1.0 : r);
+      n = make_double2(sf.nx, sf.ny);
+      cd = make_uint2(KIND_INTERFACE | ((unsigned)sh.minds[lo] << 8) | ((unsigned)sh.minds[hi] << 16), 0u);
+    } else {
+      cd = make_uint2(KIND_MULTI | ((unsigned)sh.minds[c0] << 8) | ((unsigned)sh.minds[c1] << 16) |
+                          ((unsigned)sh.minds[c2] << 24),
+                      (unsigned)sh.minds[c3]);
+    }
+    code[v] = cd;
+    rvol[v] = r;
+    nrm[v] = n;
+    atomicAdd(&cnt[nd - 1], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x < 3 && cnt[threadIdx.x]) atomicAdd(&counts[threadIdx.x], (unsigned long long)cnt[threadIdx.x]);
+}
+
+// ---- the dispersive Kottke kernel: a second-order Taylor jet (f, f′, f″) ----------------
+
+struct J2 {
+  double v, d, dd;
+};
+
+__device__ __forceinline__ J2 jadd(J2 a, J2 b) { return J2{a.v + b.v, a.d + b.d, a.dd + b.dd}; }
+__device__ __forceinline__ J2 jsub(J2 a, J2 b) { return J2{a.v - b.v, a.d - b.d, a.dd - b.dd}; }
+__device__ __forceinline__ J2 jneg(J2 a) { return J2{-a.v, -a.d, -a.dd}; }
+__device__ __forceinline__ J2 jmul(J2 a, J2 b) {
+  return J2{a.v * b.v, a.d * b.v + a.v * b.d, (a.dd * b.v + 2.0 * a.d * b.d) + a.v * b.dd};
+}
+__device__ __forceinline__ J2 jinv(J2 a) {
+  const double i = 1.0 / a.v;
+  return J2{i, -a.d * i * i, -a.dd * i * i + 2.0 * a.d * a.d * i * i * i};
+}
+
+// τ_trans in place on a row-major jet matrix e[r*3+c]
+__device__ __forceinline__ void tau(J2* e) {
+  const J2 i = jinv(e[0]);
+  const J2 e01 = e[1], e02 = e[2], e10 = e[3], e20 = e[6];
+  e[0] = jneg(i);
+  e[1] = jmul(e01, i);
+  e[2] = jmul(e02, i);
+  e[3] = jmul(e10, i);
+  e[4] = jsub(e[4], jmul(jmul(e10, e01), i));
+  e[5] = jsub(e[5], jmul(jmul(e10, e02), i));
+  e[6] = jmul(e20, i);
+  e[7] = jsub(e[7], jmul(jmul(e20, e01), i));
+  e[8] = jsub(e[8], jmul(jmul(e20, e02), i));
+}
+
+__device__ __forceinline__ void tau_inv(J2* t) {
+  const J2 i = jinv(t[0]);
+  const J2 t01 = t[1], t02 = t[2], t10 = t[3], t20 = t[6];
+  t[0] = jneg(i);
+  t[1] = jmul(jneg(t01), i);
+  t[2] = jmul(jneg(t02), i);
+  t[3] = jmul(jneg(t10), i);
+  t[4] = jsub(t[4], jmul(jmul(t10, t01), i));
+  t[5] = jsub(t[5], jmul(jmul(t10, t02), i));
+  t[6] = jmul(jneg(t20), i);
+  t[7] = jsub(t[7], jmul(jmul(t20, t01), i));
+  t[8] = jsub(t[8], jmul(jmul(t20, t02), i));
+}
+
+// C = A·B for row-major 3×3 (sum in index order)
+__device__ __forceinline__ void mm3(const double* A, const double* B, double* C) {
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) C[r * 3 + c] = (A[r * 3] * B[c] + A[r * 3 + 1] * B[3 + c]) + A[r * 3 + 2] * B[6 + c];
+}
+
+// slice s of a 27-entry column (column-major 3×3) → row-major X = Sᵀ (E S)
+__device__ __forceinline__ void rotate_in(const double* col, int s, const double* S, const double* St, double* X) {
+  double E[9], T[9];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) E[r * 3 + c] = col[9 * s + r + 3 * c];
+  mm3(E, S, T);
+  mm3(St, T, X);
+}
+
+__device__ void kottke_jet(double r1, double nx, double ny, const double* c1, const double* c2, double* out) {
+  // S = normcart((nx, ny, 0)), columns n, h, v (row-major S[r*3+c])
+  const double hx0 = -ny, hy0 = nx;
+  const double L = sqrt(hx0 * hx0 + hy0 * hy0);
+  const double h0 = hx0 / L, h1 = hy0 / L, h2 = 0.0 / L;
+  const double n0 = nx, n1 = ny, n2 = 0.0;
+  const double w0 = n1 * h2 - n2 * h1, w1 = n2 * h0 - n0 * h2, w2 = n0 * h1 - n1 * h0;
+  const double S[9] = {n0, h0, w0, n1, h1, w1, n2, h2, w2};
+  const double St[9] = {n0, n1, n2, h0, h1, h2, w0, w1, w2};
+  J2 a[9], b[9];
+  {
+    double X0[9], X1[9], X2[9];
+    rotate_in(c1, 0, S, St, X0);
+    rotate_in(c1, 1, S, St, X1);
+    rotate_in(c1, 2, S, St, X2);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) a[k] = J2{X0[k], X1[k], X2[k]};
+    rotate_in(c2, 0, S, St, X0);
+    rotate_in(c2, 1, S, St, X1);
+    rotate_in(c2, 2, S, St, X2);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) b[k] = J2{X0[k], X1[k], X2[k]};
+  }
+  tau(a);
+  tau(b);
+  const J2 ra{r1, 0.0, 0.0}, rb{1.0 - r1, 0.0, 0.0};
+#pragma unroll
+  for (int k = 0; k < 9; ++k) a[k] = jadd(jmul(ra, a[k]), jmul(rb, b[k]));
+  tau_inv(a);
+  // back to the lab frame: S (X Sᵀ), written column-major per slice
+#pragma unroll
+  for (int s = 0; s < 3; ++s) {
+    double X[9], T[9], Y[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) X[k] = s == 0 ? a[k].v : (s == 1 ? a[k].d : a[k].dd);
+    mm3(X, St, T);
+    mm3(S, T, Y);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) out[9 * s + r + 3 * c] = Y[r * 3 + c];
+  }
+}
+
+// column-major 3×3 inverse by the adjugate
+__device__ __forceinline__ void inv3(const double* m, double* o) {
+  const double a = m[0], b = m[3], c = m[6];
+  const double d = m[1], e = m[4], f = m[7];
+  const double g = m[2], h = m[5], i = m[8];
+  const double A = e * i - f * h, B = f * g - d * i, C = d * h - e * g;
+  const double det = (a * A + b * B) + c * C;
+  const double r = 1.0 / det;
+  o[0] = A * r; o[1] = B * r; o[2] = C * r;
+  o[3] = (c * h - b * i) * r; o[4] = (a * i - c * g) * r; o[5] = (b * g - a * h) * r;
+  o[6] = (b * f - c * e) * r; o[7] = (c * d - a * f) * r; o[8] = (a * e - b * d) * r;
+}
+
+// Material pass: grid (⌈N/128⌉, nsets), 128 threads.  Shared memory: the set's material
+// table (27·nmat doubles), then the 128-pixel staging of the 27-value and 9-value outputs.
+__global__ void __launch_bounds__(APPLY_NT) k_smooth_apply(const uint2* __restrict__ code,
+                                                           const double* __restrict__ rvol,
+                                                           const double2* __restrict__ nrm, long long N,
+                                                           const double* __restrict__ mats, int nmat,
+                                                           double* __restrict__ eps, double* __restrict__ epsinv) {
+  extern __shared__ double smem[];
+  double* M = smem;                          // 27·nmat
+  double* st27 = M + 27 * nmat;              // 27·128
+  double* st9 = st27 + 27 * APPLY_NT;        // 9·128
+  const int set = blockIdx.y;
+  const double* src = mats + (size_t)set * 27 * nmat;
+  for (int k = threadIdx.x; k < 27 * nmat; k += APPLY_NT) M[k] = src[k];
+  __syncthreads();
+  const long long base = (long long)blockIdx.x * APPLY_NT;
+  const long long v = base + threadIdx.x;
+  const int t = threadIdx.x;
+  if (v < N) {
+    const uint2 cd = code[v];
+    const int kind = cd.x & 0xff;
+    double o[27];
+    if (kind == KIND_INTERFACE) {
+      const double2 n = nrm[v];
+      kottke_jet(rvol[v], n.x, n.y, M + 27 * ((cd.x >> 8) & 0xff), M + 27 * ((cd.x >> 16) & 0xff), o);
+    } else if (kind == KIND_MULTI) {
+      const double* p0 = M + 27 * ((cd.x >> 8) & 0xff);
+      const double* p1 = M + 27 * ((cd.x >> 16) & 0xff);
+      const double* p2 = M + 27 * ((cd.x >> 24) & 0xff);
+      const double* p3 = M + 27 * (cd.y & 0xff);
+#pragma unroll
+      for (int k = 0; k < 27; ++k) o[k] = ((((0.0 + p0[k]) + p1[k]) + p2[k]) + p3[k]) / 4.0;
+    } else {
+      const double* p0 = M + 27 * ((cd.x >> 8) & 0xff);
+#pragma unroll
+      for (int k = 0; k < 27; ++k) o[k] = p0[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 27; ++k) st27[t * 27 + k] = o[k];
+    if (epsinv) {
+      double q[9];
+      inv3(o, q);
+#pragma unroll
+      for (int k = 0; k < 9; ++k) st9[t * 9 + k] = q[k];
+    }
+  }
+  __syncthreads();
+  const long long rem = N - base;
+  const int np = rem < APPLY_NT ? (int)rem : APPLY_NT;
+  if (eps) {
+    double* dst = eps + (size_t)set * 27 * N + (size_t)base * 27;
+    for (int k = threadIdx.x; k < 27 * np; k += APPLY_NT) dst[k] = st27[k];
+  }
+  if (epsinv) {
+    double* dst = epsinv + (size_t)set * 9 * N + (size_t)base * 9;
+    for (int k = threadIdx.x; k < 9 * np; k += APPLY_NT) dst[k] = st9[k];
+  }
+}
+
+}  // namespace sm
+
+}  // namespace omb
+
+struct omb_smoothing_plan {
+  omb_ctx* ctx = nullptr;
+  int Nx = 0, Ny = 0;
+  double Dx = 0, Dy = 0;
+  int fill = 0;
+  int max_mat = 0;  // largest material column the plan references
+  long long counts[3] = {0, 0, 0};
+  omb::DevBuf<uint2> code;
+  omb::DevBuf<double> rvol;
+  omb::DevBuf<double2> nrm;
+};
+
+
+using namespace omb;
+
+namespace {
+
+bool is_finite(double x) { return std::isfinite(x); }
+
+int check_plan(const omb_smoothing_plan* p) {
+  if (!p || !p->ctx) return fail(OMB_ERR_INVALID_ARG, "smoothing plan is NULL");
+  return OMB_OK;
+}
+
+sm::Axis axis(double D, int N) {
+  const double d = D / N;
+  const double a = -(D + d) / 2;
+  const double b = (D - d) / 2;
+  return sm::Axis{a, (b - a) / N};
+}
+
+int apply_launch(omb_smoothing_plan* p, const double* d_mats, int nmat, int nsets, double* d_eps, double* d_inv,
+                 cudaStream_t st) {
+  static bool attr_set[64] = {};
+  const size_t smem = sizeof(double) * (27 * (size_t)nmat + 36 * (size_t)sm::APPLY_NT);
+  const int dev = p->ctx->device;
+  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+    OMB_CU(cudaFuncSetAttribute(sm::k_smooth_apply, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(sizeof(double) * (27 * sm::MAX_MATS + 36 * sm::APPLY_NT))));
+    attr_set[dev] = true;
+  }
+  const long long N = (long long)p->Nx * p->Ny;
+  const dim3 grid((unsigned)((N + sm::APPLY_NT - 1) / sm::APPLY_NT), (unsigned)nsets);
+  sm::k_smooth_apply<<<grid, sm::APPLY_NT, smem, st>>>(p->code.p, p->rvol.p, p->nrm.p, N, d_mats, nmat, d_eps, d_inv);
+  OMB_CU(cudaGetLastError());
+  return OMB_OK;
+}
+
+int check_apply_args(const omb_smoothing_plan* p, const double* mat_vals, int nmat, int nsets) {
+  int rc = check_plan(p);
+  if (rc) return rc;
+  if (!mat_vals) return fail(OMB_ERR_INVALID_ARG, "mat_vals is NULL");
+  if (nmat < 1 || nmat > sm::MAX_MATS)
+    return fail(OMB_ERR_INVALID_ARG, "nmat must be in [1, 256], got " + std::to_string(nmat));
+  if (nmat <= p->max_mat)
+    return fail(OMB_ERR_INVALID_ARG, "the plan references material column " + std::to_string(p->max_mat) +
+                                         " but mat_vals has " + std::to_string(nmat) + " columns");
+  if (nsets < 1 || nsets > 65535) return fail(OMB_ERR_INVALID_ARG, "nsets must be in [1, 65535]");
+  return OMB_OK;
+}
+
+}  // namespace
+
+extern "C" int omb_smoothing_plan_create(omb_ctx* ctx, const omb_grid* grid, int32_t nshapes, const int32_t* nverts,
+                                         const double* verts, const int32_t* minds, int32_t fill_rule,
+                                         omb_smoothing_plan** out) {
+  if (!ctx || !grid || !out) return fail(OMB_ERR_INVALID_ARG, "NULL context, grid or output handle");
+  *out = nullptr;
+  if (grid->Nx < 1 || grid->Ny < 1 || !(grid->Dx > 0) || !(grid->Dy > 0) || !is_finite(grid->Dx) || !is_finite(grid->Dy))
+    return fail(OMB_ERR_INVALID_ARG, "grid needs Nx, Ny ≥ 1 and finite Dx, Dy > 0");
+  if ((long long)grid->Nx * grid->Ny > (1LL << 31))
+    return fail(OMB_ERR_INVALID_ARG, "grid has more than 2^31 pixels");
+  if (nshapes < 0 || nshapes > sm::MAX_SHAPES)
+    return fail(OMB_ERR_INVALID_ARG, "nshapes must be in [0, 255], got " + std::to_string(nshapes));
+  if (fill_rule != OMB_FILL_PLANE && fill_rule != OMB_FILL_EXACT)
+    return fail(OMB_ERR_INVALID_ARG, "fill_rule must be OMB_FILL_PLANE or OMB_FILL_EXACT");
+  if (!minds || (nshapes > 0 && (!nverts || !verts))) return fail(OMB_ERR_INVALID_ARG, "NULL shape arrays");
+  // counter-clockwise convex polygons
+  std::vector<int> voff(nshapes + 1, 0);
+  std::vector<double2> hv;
+  size_t pos = 0;
+  for (int s = 0; s < nshapes; ++s) {
+    const int nv = nverts[s];
+    if (nv < 3 || nv > sm::MAX_VERTS)
+      return fail(OMB_ERR_INVALID_ARG, "shape " + std::to_string(s) + " needs 3 to 64 vertices");
+    std::vector<double2> v(nv);
+    for (int i = 0; i < nv; ++i) {
+      v[i] = make_double2(verts[2 * (pos + i)], verts[2 * (pos + i) + 1]);
+      if (!is_finite(v[i].x) || !is_finite(v[i].y))
+        return fail(OMB_ERR_INVALID_ARG, "shape " + std::to_string(s) + " has a non-finite vertex");
+    }
+    pos += nv;
+    double area2 = 0.0;
+    for (int i = 0; i < nv; ++i) {
+      const int j = (i + 1) % nv;
+      area2 += v[i].x * v[j].y - v[j].x * v[i].y;
+    }
+    if (area2 < 0) std::reverse(v.begin(), v.end());
+    if (area2 == 0) return fail(OMB_ERR_INVALID_ARG, "shape " + std::to_string(s) + " has zero area");
+    for (int i = 0; i < nv; ++i) {
+      const double2 a = v[i], b = v[(i + 1) % nv], c = v[(i + 2) % nv];
+      const double turn = (b.x - a.x) * (c.y - b.y) - (b.y - a.y) * (c.x - b.x);
+      if (turn < 0) return fail(OMB_ERR_INVALID_ARG, "shape " + std::to_string(s) + " is not convex");
+    }
+    voff[s + 1] = voff[s] + nv;
+    hv.insert(hv.end(), v.begin(), v.end());
+  }
+  int max_mat = 0;
+  for (int s = 0; s <= nshapes; ++s) {
+    if (minds[s] < 0 || minds[s] >= sm::MAX_MATS)
+      return fail(OMB_ERR_INVALID_ARG, "minds entries must be material columns in [0, 255]");
+    max_mat = std::max(max_mat, (int)minds[s]);
+  }
+  auto* p = new omb_smoothing_plan();
+  p->ctx = ctx;
+  p->Nx = grid->Nx; p->Ny = grid->Ny; p->Dx = grid->Dx; p->Dy = grid->Dy;
+  p->fill = fill_rule;
+  p->max_mat = max_mat;
+  cudaStream_t st = ctx->stream;
+  const size_t N = (size_t)p->Nx * p->Ny;
+  auto bail = [&](int rc) { delete p; return rc; };
+  DevBuf<double2> dv;
+  DevBuf<int> doff, dm;
+  DevBuf<unsigned long long> dcnt;
+  if (cudaError_t e = cudaSetDevice(ctx->device); e != cudaSuccess) return bail(cuda_fail(e, "cudaSetDevice"));
+#define PLAN_CU(x)                                          \
+  do {                                                      \
+    cudaError_t e__ = (x);                                  \
+    if (e__ != cudaSuccess) return bail(cuda_fail(e__, #x)); \
+  } while (0)
+  PLAN_CU(p->code.alloc(N, st));
+  PLAN_CU(p->rvol.alloc(N, st));
+  PLAN_CU(p->nrm.alloc(N, st));
+  PLAN_CU(dv.alloc(std::max<size_t>(hv.size(), 1), st));
+  PLAN_CU(doff.alloc(nshapes + 1, st));
+  PLAN_CU(dm.alloc(nshapes + 1, st));
+  PLAN_CU(dcnt.alloc(3, st));
+  if (!hv.empty()) PLAN_CU(cudaMemcpyAsync(dv.p, hv.data(), hv.size() * sizeof(double2), cudaMemcpyHostToDevice, st));
+  PLAN_CU(cudaMemcpyAsync(doff.p, voff.data(), voff.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+  std::vector<int> hm(minds, minds + nshapes + 1);
+  PLAN_CU(cudaMemcpyAsync(dm.p, hm.data(), hm.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+  PLAN_CU(dcnt.zero());
+  sm::Shapes sh{dv.p, doff.p, dm.p, nshapes};
+  const unsigned blocks = (unsigned)((N + sm::PLAN_NT - 1) / sm::PLAN_NT);
+  sm::k_smooth_plan<<<blocks, sm::PLAN_NT, 0, st>>>(sh, axis(p->Dx, p->Nx), axis(p->Dy, p->Ny), p->Nx, p->Ny,
+                                                    fill_rule, p->code.p, p->rvol.p, p->nrm.p, dcnt.p);
+  PLAN_CU(cudaGetLastError());
+  unsigned long long hc[3];
+  PLAN_CU(cudaMemcpyAsync(hc, dcnt.p, sizeof(hc), cudaMemcpyDeviceToHost, st));
+  PLAN_CU(cudaStreamSynchronize(st));
+#undef PLAN_CU
+  for (int k = 0; k < 3; ++k) p->counts[k] = (long long)hc[k];
+  *out = p;
+  return OMB_OK;
+}
+
+extern "C" int omb_smoothing_plan_query(const omb_smoothing_plan* p, int64_t* counts, uint8_t* kind, int32_t* mats,
+                                        double* rvol, double* normal) {
+  int rc = check_plan(p);
+  if (rc) return rc;
+  if (counts)
+    for (int k = 0; k < 3; ++k) counts[k] = p->counts[k];
+  const size_t N = (size_t)p->Nx * p->Ny;
+  cudaStream_t st = p->ctx->stream;
+  OMB_CU(cudaSetDevice(p->ctx->device));
+  if (kind || mats) {
+    std::vector<uint2> c(N);
+    OMB_CU(cudaMemcpyAsync(c.data(), p->code.p, N * sizeof(uint2), cudaMemcpyDeviceToHost, st));
+    OMB_CU(cudaStreamSynchronize(st));
+    for (size_t v = 0; v < N; ++v) {
+      const int kd = c[v].x & 0xff;
+      if (kind) kind[v] = (uint8_t)kd;
+      if (mats) {
+        int32_t* m = mats + 4 * v;
+        m[0] = (int32_t)((c[v].x >> 8) & 0xff);
+        m[1] = kd >= sm::KIND_INTERFACE ? (int32_t)((c[v].x >> 16) & 0xff) : -1;
+        m[2] = kd == sm::KIND_MULTI ? (int32_t)((c[v].x >> 24) & 0xff) : -1;
+        m[3] = kd == sm::KIND_MULTI ? (int32_t)(c[v].y & 0xff) : -1;
+      }
+    }
+  }
+  if (rvol) OMB_CU(cudaMemcpyAsync(rvol, p->rvol.p, N * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (normal) OMB_CU(cudaMemcpyAsync(normal, p->nrm.p, N * sizeof(double2), cudaMemcpyDeviceToHost, st));
+  OMB_CU(cudaStreamSynchronize(st));
+  return OMB_OK;
+}
+
+extern "C" int omb_smooth_eps(omb_smoothing_plan* p, const double* mat_vals, int32_t nmat, int32_t nsets,
+                              double* eps, double* epsinv) {
+  int rc = check_apply_args(p, mat_vals, nmat, nsets);
+  if (rc) return rc;
+  if (!eps && !epsinv) return fail(OMB_ERR_INVALID_ARG, "both outputs are NULL");
+  cudaStream_t st = p->ctx->stream;
+  OMB_CU(cudaSetDevice(p->ctx->device));
+  const size_t N = (size_t)p->Nx * p->Ny, nm = 27 * (size_t)nmat * nsets;
+  DevBuf<double> dmat, de, di;
+  OMB_CU(dmat.alloc(nm, st));
+  OMB_CU(cudaMemcpyAsync(dmat.p, mat_vals, nm * sizeof(double), cudaMemcpyHostToDevice, st));
+  if (eps) OMB_CU(de.alloc(27 * N * nsets, st));
+  if (epsinv) OMB_CU(di.alloc(9 * N * nsets, st));
+  rc = apply_launch(p, dmat.p, nmat, nsets, de.p, di.p, st);
+  if (rc) return rc;
+  if (eps) OMB_CU(cudaMemcpyAsync(eps, de.p, 27 * N * nsets * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (epsinv) OMB_CU(cudaMemcpyAsync(epsinv, di.p, 9 * N * nsets * sizeof(double), cudaMemcpyDeviceToHost, st));
+  OMB_CU(cudaStreamSynchronize(st));
+  return OMB_OK;
+}
+
+extern "C" int omb_smooth_eps_device(omb_smoothing_plan* p, const double* mat_vals, int32_t nmat, int32_t nsets,
+                                     double* d_eps, double* d_epsinv, void* stream) {
+  int rc = check_apply_args(p, mat_vals, nmat, nsets);
+  if (rc) return rc;
+  if (!d_eps && !d_epsinv) return fail(OMB_ERR_INVALID_ARG, "both outputs are NULL");
+  cudaStream_t st = stream ? (cudaStream_t)stream : p->ctx->stream;
+  OMB_CU(cudaSetDevice(p->ctx->device));
+  const size_t nm = 27 * (size_t)nmat * nsets;
+  DevBuf<double> dmat;
+  OMB_CU(dmat.alloc(nm, st));
+  OMB_CU(cudaMemcpyAsync(dmat.p, mat_vals, nm * sizeof(double), cudaMemcpyHostToDevice, st));
+  return apply_launch(p, dmat.p, nmat, nsets, d_eps, d_epsinv, st);
+}
+
+extern "C" int omb_smoothing_plan_destroy(omb_smoothing_plan* p) {
+  if (!p) return OMB_OK;
+  if (p->ctx) {
+    cudaSetDevice(p->ctx->device);
+    cudaDeviceSynchronize();  // applies on caller streams may still read the plan
+  }
+  delete p;
+  return OMB_OK;
+}

@@ -220,3 +220,26 @@ def _declare_pullback(lib):
 
 EXPORTS = EXPORTS + ("omb_pullback",)
 _DECLARERS.append(_declare_pullback)
+
+
+def _declare_smoothing(lib):
+    vp = ctypes.c_void_p
+    i32p = ctypes.POINTER(ctypes.c_int32)
+    sig = {
+        "omb_smoothing_plan_create": (ctypes.c_int, [vp, ctypes.POINTER(c_grid), ctypes.c_int32, i32p, _dp, i32p,
+                                                     ctypes.c_int32, ctypes.POINTER(vp)]),
+        "omb_smoothing_plan_query": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int64),
+                                                    ctypes.POINTER(ctypes.c_uint8), i32p, _dp, _dp]),
+        "omb_smooth_eps": (ctypes.c_int, [vp, _dp, ctypes.c_int32, ctypes.c_int32, _dp, _dp]),
+        "omb_smooth_eps_device": (ctypes.c_int, [vp, _dp, ctypes.c_int32, ctypes.c_int32, vp, vp, vp]),
+        "omb_smoothing_plan_destroy": (ctypes.c_int, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+
+
+EXPORTS = EXPORTS + ("omb_smoothing_plan_create", "omb_smoothing_plan_query", "omb_smooth_eps",
+                     "omb_smooth_eps_device", "omb_smoothing_plan_destroy")
+_DECLARERS.append(_declare_smoothing)

@@ -1,30 +1,31 @@
-"""Waveguide cross-sections → sub-pixel-smoothed inverse permittivity (host, FP64).
+"""Waveguide cross-sections → Kottke sub-pixel-smoothed permittivity on the GPU.
 
-The input generator of the benchmark and the tests: convex polygons (rectangles, ridge
-trapezoids) with constant dielectric tensors are rendered onto a ``Grid`` with the
-anisotropic sub-pixel average of Kottke, Farjadpour & Johnson, Phys. Rev. E 77, 036611
-(2008), following the reference's per-pixel rule (``lib/DielectricSmoothing/src/smooth.jl:90-121``,
-``src/kottke.jl:44-101``):
+Convex polygons (rectangles, ridge trapezoids, any convex outline) in priority order are
+rendered onto a ``Grid`` by the library's smoothing kernels, which follow the reference's
+``lib/DielectricSmoothing`` (``smoothing_plan`` / ``smooth_ε`` / ``smooth_ε(plan, mat_vals)``,
+``src/smoothing_plan.jl``, ``src/smooth.jl:24-121``, ``src/kottke.jl``) and fuse
+``sliceinv_3x3`` so the solver's ε⁻¹ input comes out of the same pass:
 
-* a pixel whose four corners lie in one material takes that material's ε;
-* a pixel whose corners see exactly two materials takes the τ-average of the two,
-  weighted by the exact area fraction of the higher-priority shape inside the pixel, in the
-  frame of that shape's nearest edge normal;
-* a pixel whose corners see three or more materials takes the mean of the corner ε.
+* a pixel whose four corners lie in one material takes that material's data;
+* a pixel whose corners see exactly two materials takes the dispersive τ-average of the two
+  (ε, ∂ωε and ∂²ωε by a second-order Taylor jet), weighted by the fill fraction of the
+  higher-priority shape, in the frame of that shape's nearest edge normal;
+* a pixel whose corners see three or more materials takes the mean of its corners' data.
 
-Shapes are listed in priority order (the first shape containing a point wins); the
-reference queries GeometryPrimitives (an un-vendored dependency) for the same fill
-fraction and normal, so ε maps agree with the reference only up to that library's
-geometry routines.
+Material data are the reference's 27-entry columns vcat(vec(ε), vec(∂ωε), vec(∂²ωε)).
+GeometryPrimitives (the reference's un-vendored geometry library) is restated for convex
+polygons, so ε maps agree with the reference up to that library's polygon routines.
 """
 
 from __future__ import annotations
 
+import ctypes
 import dataclasses
 from typing import Sequence
 
 import numpy as np
 
+from . import _lib
 from .grid import Grid
 
 
@@ -36,63 +37,22 @@ def diag_eps(a, b=None, c=None) -> np.ndarray:
 
 @dataclasses.dataclass
 class Polygon:
-    """Convex polygon with counter-clockwise vertices ``(n, 2)`` and a 3×3 ε tensor."""
+    """Convex polygon: ``(n, 2)`` vertices (stored counter-clockwise) and, for
+    :func:`smooth_epsinv`, a constant 3×3 ε tensor."""
 
     vertices: np.ndarray
-    eps: np.ndarray
+    eps: np.ndarray | None = None
 
     def __post_init__(self):
         v = np.asarray(self.vertices, dtype=np.float64)
+        if v.ndim != 2 or v.shape[1] != 2 or v.shape[0] < 3:
+            raise ValueError("a polygon needs an (n ≥ 3, 2) vertex array")
         area2 = np.sum(v[:, 0] * np.roll(v[:, 1], -1) - np.roll(v[:, 0], -1) * v[:, 1])
         if area2 < 0:
             v = v[::-1]
-        self.vertices = v
-        self.eps = np.asarray(self.eps, dtype=np.float64)
-
-    def contains(self, x: np.ndarray, y: np.ndarray) -> np.ndarray:
-        v = self.vertices
-        inside = np.ones(np.broadcast(x, y).shape, dtype=bool)
-        for i in range(len(v)):
-            a, b = v[i], v[(i + 1) % len(v)]
-            inside &= (b[0] - a[0]) * (y - a[1]) - (b[1] - a[1]) * (x - a[0]) >= 0
-        return inside
-
-    def clip_area(self, x0, x1, y0, y1) -> float:
-        """Area of the intersection with the box [x0,x1]×[y0,y1] (Sutherland–Hodgman)."""
-        poly = [(x0, y0), (x1, y0), (x1, y1), (x0, y1)]
-        v = self.vertices
-        for i in range(len(v)):
-            a, b = v[i], v[(i + 1) % len(v)]
-            side = lambda p: (b[0] - a[0]) * (p[1] - a[1]) - (b[1] - a[1]) * (p[0] - a[0])
-            out = []
-            for j in range(len(poly)):
-                p, q = poly[j], poly[(j + 1) % len(poly)]
-                sp, sq = side(p), side(q)
-                if sp >= 0:
-                    out.append(p)
-                if (sp >= 0) != (sq >= 0):
-                    t = sp / (sp - sq)
-                    out.append((p[0] + t * (q[0] - p[0]), p[1] + t * (q[1] - p[1])))
-            poly = out
-            if not poly:
-                return 0.0
-        P = np.array(poly)
-        return 0.5 * abs(np.sum(P[:, 0] * np.roll(P[:, 1], -1) - np.roll(P[:, 0], -1) * P[:, 1]))
-
-    def nearest_normal(self, x: float, y: float) -> np.ndarray:
-        """Outward unit normal of the edge nearest to (x, y)."""
-        v = self.vertices
-        best, nrm = np.inf, None
-        for i in range(len(v)):
-            a, b = v[i], v[(i + 1) % len(v)]
-            d = b - a
-            t = np.clip(np.dot([x - a[0], y - a[1]], d) / np.dot(d, d), 0.0, 1.0)
-            p = a + t * d
-            dist = np.hypot(x - p[0], y - p[1])
-            if dist < best:
-                best = dist
-                nrm = np.array([d[1], -d[0]]) / np.hypot(d[0], d[1])
-        return nrm
+        self.vertices = np.ascontiguousarray(v)
+        if self.eps is not None:
+            self.eps = np.asarray(self.eps, dtype=np.float64)
 
 
 def rectangle(cx, cy, wx, wy, eps) -> Polygon:
@@ -108,63 +68,157 @@ def ridge(cx, y0, top_width, height, sidewall_deg, eps) -> Polygon:
                              [cx - top_width / 2, y0 + height]]), eps)
 
 
-def _tau(e):
-    i = 1.0 / e[0, 0]
-    return np.array([[-i, e[0, 1] * i, e[0, 2] * i],
-                     [e[1, 0] * i, e[1, 1] - e[1, 0] * e[0, 1] * i, e[1, 2] - e[1, 0] * e[0, 2] * i],
-                     [e[2, 0] * i, e[2, 1] - e[2, 0] * e[0, 1] * i, e[2, 2] - e[2, 0] * e[0, 2] * i]])
+def material_column(eps, deps=None, ddeps=None) -> np.ndarray:
+    """The reference's 27-entry material column vcat(vec(ε), vec(∂ωε), vec(∂²ωε)) from 3×3
+    arrays (None → zeros), the layout of ``MaterialDispersion._f_ε_mats`` columns."""
+    parts = []
+    for m in (eps, deps, ddeps):
+        m = np.zeros((3, 3)) if m is None else np.asarray(m, dtype=np.float64)
+        if m.shape != (3, 3):
+            raise ValueError("material tensors must be 3×3")
+        parts.append(m.reshape(9, order="F"))
+    return np.concatenate(parts)
 
 
-def _tau_inv(t):
-    i = 1.0 / t[0, 0]
-    return np.array([[-i, -t[0, 1] * i, -t[0, 2] * i],
-                     [-t[1, 0] * i, t[1, 1] - t[1, 0] * t[0, 1] * i, t[1, 2] - t[1, 0] * t[0, 2] * i],
-                     [-t[2, 0] * i, t[2, 1] - t[2, 0] * t[0, 1] * i, t[2, 2] - t[2, 0] * t[0, 2] * i]])
+_FILL = {"plane": 0, "exact": 1}
+UNIFORM, INTERFACE, MULTI = 1, 2, 3
 
 
-def kottke_average(e1, e2, normal2d, r1) -> np.ndarray:
-    """S τ⁻¹(r τ(Sᵀε₁S) + (1−r) τ(Sᵀε₂S)) Sᵀ with S's first column the interface normal."""
-    n = np.array([normal2d[0], normal2d[1], 0.0])
-    t = np.array([-normal2d[1], normal2d[0], 0.0])
-    S = np.stack([n, t, np.array([0.0, 0.0, 1.0])], axis=1)
-    tau = r1 * _tau(S.T @ e1 @ S) + (1 - r1) * _tau(S.T @ e2 @ S)
-    return S @ _tau_inv(tau) @ S.T
+class SmoothingPlan:
+    """Frequency-independent geometry scaffold on the device (the reference's
+    ``SmoothingPlan``, ``lib/DielectricSmoothing/src/smoothing_plan.jl:26-100``).
+
+    ``shapes`` are convex polygons in priority order (the first containing a point wins),
+    ``minds`` the 0-based material column of every shape and then of the background, and
+    ``fill`` the interface fill-fraction rule: ``"plane"`` (the reference's ``volfrac`` of the
+    voxel cut by the tangent line at the nearest surface point) or ``"exact"`` (the exact
+    polygon ∩ voxel area).  Apply it per frequency with :meth:`smooth_eps`."""
+
+    def __init__(self, shapes: Sequence, minds: Sequence[int], grid: Grid, fill: str = "plane", device: int = 0):
+        if fill not in _FILL:
+            raise ValueError(f"fill must be 'plane' or 'exact', got {fill!r}")
+        if len(minds) != len(shapes) + 1:
+            raise ValueError("minds needs one material column per shape plus the background")
+        self.grid = grid
+        self.fill = fill
+        self.nmat_min = int(max(minds)) + 1
+        self._ctx = _lib.context(device)
+        lib = _lib.load()
+        nv = np.array([np.asarray(getattr(s, "vertices", s)).shape[0] for s in shapes] or [0], dtype=np.int32)
+        verts = (np.concatenate([np.asarray(getattr(s, "vertices", s), dtype=np.float64).reshape(-1)
+                                 for s in shapes]) if shapes else np.zeros(2))
+        verts = np.ascontiguousarray(verts)
+        md = np.ascontiguousarray(np.asarray(minds, dtype=np.int32))
+        h = ctypes.c_void_p()
+        _lib.check(lib.omb_smoothing_plan_create(
+            self._ctx.handle, ctypes.byref(grid.c()), len(shapes), nv.ctypes.data_as(_lib._ip),
+            _lib.dptr(verts), md.ctypes.data_as(_lib._ip), _FILL[fill], ctypes.byref(h)))
+        self._h = h
+        counts = (ctypes.c_int64 * 3)()
+        _lib.check(lib.omb_smoothing_plan_query(self._h, counts, None, None, None, None))
+        self.counts = tuple(int(c) for c in counts)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().omb_smoothing_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def query(self):
+        """(kind (N,), mats (N, 4), rvol (N,), normal (N, 2)), pixels in corners(grid) order."""
+        N = self.grid.N
+        kind = np.empty(N, dtype=np.uint8)
+        mats = np.empty((N, 4), dtype=np.int32)
+        rvol = np.empty(N)
+        normal = np.empty((N, 2))
+        _lib.check(_lib.load().omb_smoothing_plan_query(
+            self._h, None, kind.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), mats.ctypes.data_as(_lib._ip),
+            _lib.dptr(rvol), _lib.dptr(normal)))
+        return kind, mats, rvol, normal
+
+    def _mats(self, mat_vals):
+        M = np.asarray(mat_vals, dtype=np.float64)
+        single = M.ndim == 2
+        if single:
+            M = M[:, :, None]
+        if M.ndim != 3 or M.shape[0] != 27:
+            raise ValueError("mat_vals must be (27, n_materials) or (27, n_materials, n_sets)")
+        return np.asfortranarray(M), single
+
+    def smooth_eps(self, mat_vals, eps: bool = True, epsinv: bool = False):
+        """``smooth_ε(plan, mat_vals)`` on the device.  ``mat_vals`` is the reference's
+        (27, n_materials) matrix, or (27, n_materials, n_sets) for several frequencies at
+        once.  Returns the reference-indexed (3, 3, 3, Nx, Ny[, n_sets]) (ε, ∂ωε, ∂²ωε) and/or
+        the (3, 3, Nx, Ny[, n_sets]) ``sliceinv_3x3`` of its ε slice."""
+        M, single = self._mats(mat_vals)
+        nmat, nsets = M.shape[1], M.shape[2]
+        g = self.grid
+        e = np.empty((3, 3, 3, g.Nx, g.Ny, nsets), order="F") if eps else None
+        ei = np.empty((3, 3, g.Nx, g.Ny, nsets), order="F") if epsinv else None
+        if e is None and ei is None:
+            raise ValueError("ask for eps, epsinv or both")
+        _lib.check(_lib.load().omb_smooth_eps(self._h, _lib.dptr(M), nmat, nsets,
+                                             _lib.dptr(e) if e is not None else None,
+                                             _lib.dptr(ei) if ei is not None else None))
+        if single:
+            e = e[..., 0] if e is not None else None
+            ei = ei[..., 0] if ei is not None else None
+        if eps and epsinv:
+            return e, ei
+        return e if eps else ei
+
+    def smooth_eps_device(self, mat_vals, eps_out=None, epsinv_out=None, stream=None):
+        """As :meth:`smooth_eps` into caller-owned device buffers (torch float64 CUDA tensors
+        holding 27·N·n_sets and 9·N·n_sets values), queued on ``stream`` (a torch stream, or
+        the library's own stream when None)."""
+        M, _ = self._mats(mat_vals)
+        nmat, nsets = M.shape[1], M.shape[2]
+        N = self.grid.N
+        for t, per in ((eps_out, 27), (epsinv_out, 9)):
+            if t is not None and (t.dtype.__str__() != "torch.float64" or not t.is_cuda or not t.is_contiguous()
+                                  or t.numel() != per * N * nsets):
+                raise ValueError(f"device outputs must be contiguous float64 CUDA tensors of {per}·N·n_sets values")
+        st = None if stream is None else ctypes.c_void_p(stream.cuda_stream)
+        _lib.check(_lib.load().omb_smooth_eps_device(
+            self._h, _lib.dptr(M), nmat, nsets,
+            ctypes.c_void_p(eps_out.data_ptr()) if eps_out is not None else None,
+            ctypes.c_void_p(epsinv_out.data_ptr()) if epsinv_out is not None else None, st))
 
 
-def smooth_epsinv(shapes: Sequence[Polygon], background_eps, grid: Grid) -> np.ndarray:
-    """Smoothed ε⁻¹ with the reference's index semantics ``(3, 3, Nx, Ny)``."""
-    bg = np.asarray(background_eps, dtype=np.float64)
-    mats = [s.eps for s in shapes] + [bg]
-    dx, dy = grid.Dx / grid.Nx, grid.Dy / grid.Ny
-    xc, yc = grid.x(), grid.y()
-    # shape index at every pixel corner: corners (i ± 1/2, j ± 1/2)
-    xk = np.concatenate([xc - dx / 2, [xc[-1] + dx / 2]])
-    yk = np.concatenate([yc - dy / 2, [yc[-1] + dy / 2]])
-    XK, YK = np.meshgrid(xk, yk, indexing="ij")
-    sid = np.full(XK.shape, len(shapes), dtype=np.int32)
-    for i in range(len(shapes) - 1, -1, -1):
-        sid[shapes[i].contains(XK, YK)] = i
-    c4 = np.stack([sid[:-1, :-1], sid[1:, :-1], sid[:-1, 1:], sid[1:, 1:]], axis=-1)  # (Nx, Ny, 4)
-    eps = np.empty((grid.Nx, grid.Ny, 3, 3))
-    first = c4[..., 0]
-    uniform = np.all(c4 == first[..., None], axis=-1)
-    M = np.stack(mats)  # (nmat, 3, 3)
-    eps[uniform] = M[first[uniform]]
-    for ix, iy in zip(*np.nonzero(~uniform)):
-        ids = sorted(set(int(v) for v in c4[ix, iy]))
-        if len(ids) == 2:
-            s1, s2 = ids
-            x0, x1 = xc[ix] - dx / 2, xc[ix] + dx / 2
-            y0, y1 = yc[iy] - dy / 2, yc[iy] + dy / 2
-            r1 = shapes[s1].clip_area(x0, x1, y0, y1) / (dx * dy)
-            # remove the parts of higher-priority shapes (none here: s1 has top priority)
-            nrm = shapes[s1].nearest_normal(xc[ix], yc[iy])
-            eps[ix, iy] = kottke_average(mats[s1], mats[s2], nrm, min(max(r1, 0.0), 1.0))
-        else:
-            eps[ix, iy] = np.mean([mats[int(v)] for v in c4[ix, iy]], axis=0)
-    ei = np.linalg.inv(eps)
-    ei = 0.5 * (ei + np.swapaxes(ei, -1, -2))
-    return np.ascontiguousarray(np.transpose(ei, (2, 3, 0, 1)))
+def smoothing_plan(shapes: Sequence, minds: Sequence[int], grid: Grid, fill: str = "plane",
+                   device: int = 0) -> SmoothingPlan:
+    """``smoothing_plan(shapes, minds, grid)`` (0-based ``minds``)."""
+    return SmoothingPlan(shapes, minds, grid, fill, device)
+
+
+def smooth_eps(shapes, mat_vals, minds=None, grid: Grid | None = None, fill: str = "plane", device: int = 0):
+    """``smooth_ε(shapes, mat_vals, minds, grid)`` or ``smooth_ε(plan, mat_vals)``:
+    reference-indexed (3, 3, 3, Nx, Ny) smoothed (ε, ∂ωε, ∂²ωε), computed on the GPU."""
+    if isinstance(shapes, SmoothingPlan):
+        return shapes.smooth_eps(mat_vals)
+    plan = SmoothingPlan(shapes, minds, grid, fill, device)
+    try:
+        return plan.smooth_eps(mat_vals)
+    finally:
+        plan.close()
+
+
+def smooth_epsinv(shapes: Sequence[Polygon], background_eps, grid: Grid, fill: str = "plane",
+                  device: int = 0) -> np.ndarray:
+    """Smoothed ε⁻¹ (reference index semantics (3, 3, Nx, Ny)) of shapes with constant ε
+    (``shape.eps``) in a constant background, computed on the GPU."""
+    cols = [material_column(s.eps) for s in shapes] + [material_column(background_eps)]
+    M = np.stack(cols, axis=1)
+    plan = SmoothingPlan(shapes, list(range(len(cols))), grid, fill, device)
+    try:
+        return np.ascontiguousarray(plan.smooth_eps(M, eps=False, epsinv=True))
+    finally:
+        plan.close()
 
 
 # ---- the benchmark cross-sections -------------------------------------------------------
@@ -175,15 +229,16 @@ EPS_SI = 12.1
 EPS_LN_XCUT = (4.97, 4.61, 4.97)
 
 
-def si3n4_rect(grid: Grid, w=1.7, h=0.7, eps_core=EPS_SI3N4, eps_clad=EPS_SIO2) -> np.ndarray:
-    """Centred rectangular core in uniform cladding (isotropic)."""
-    return smooth_epsinv([rectangle(0.0, 0.0, w, h, diag_eps(eps_core))], diag_eps(eps_clad), grid)
+def si3n4_rect_shapes(w=1.7, h=0.7, eps_core=EPS_SI3N4, eps_clad=EPS_SIO2):
+    """(shapes, background ε) of a centred rectangular core in uniform cladding."""
+    return [rectangle(0.0, 0.0, w, h, diag_eps(eps_core))], diag_eps(eps_clad)
 
 
-def ln_ridge(grid: Grid, top_width=1.5, film=0.6, etch=0.3, sidewall_deg=70.0,
-             eps_core=EPS_LN_XCUT, eps_sub=EPS_SIO2, eps_top=1.0) -> np.ndarray:
-    """x-cut LiNbO₃ ridge: a slab of thickness film−etch on SiO₂ with a trapezoidal ridge
-    of height `etch` on top, air above; the film is centred in the cell."""
+def ln_ridge_shapes(grid: Grid, top_width=1.5, film=0.6, etch=0.3, sidewall_deg=70.0,
+                    eps_core=EPS_LN_XCUT, eps_sub=EPS_SIO2, eps_top=1.0):
+    """(shapes, background ε) of an x-cut LiNbO₃ ridge: a slab of thickness film−etch on SiO₂
+    with a trapezoidal ridge of height `etch` on top, air above; the film is centred in the
+    cell."""
     slab = film - etch
     y_sub = -film / 2
     big = 4 * max(grid.Dx, grid.Dy)
@@ -192,4 +247,16 @@ def ln_ridge(grid: Grid, top_width=1.5, film=0.6, etch=0.3, sidewall_deg=70.0,
         rectangle(0.0, y_sub + slab / 2, big, slab, diag_eps(*eps_core)),
         rectangle(0.0, y_sub - big / 2, big, big, diag_eps(eps_sub)),
     ]
-    return smooth_epsinv(shapes, diag_eps(eps_top), grid)
+    return shapes, diag_eps(eps_top)
+
+
+def si3n4_rect(grid: Grid, device: int = 0, **kw) -> np.ndarray:
+    """Smoothed ε⁻¹ of :func:`si3n4_rect_shapes` (GPU)."""
+    shapes, bg = si3n4_rect_shapes(**kw)
+    return smooth_epsinv(shapes, bg, grid, device=device)
+
+
+def ln_ridge(grid: Grid, device: int = 0, **kw) -> np.ndarray:
+    """Smoothed ε⁻¹ of :func:`ln_ridge_shapes` (GPU)."""
+    shapes, bg = ln_ridge_shapes(grid, **kw)
+    return smooth_epsinv(shapes, bg, grid, device=device)
