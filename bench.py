@@ -142,6 +142,80 @@ def profiled_traffic():
         return None
 
 
+def smoothing_materials(n_shapes: int, nsets: int) -> np.ndarray:
+    """(27, n_shapes + 1, nsets) material columns for the ridge's shapes and air: the
+    cross-section's ε with a seeded synthetic dispersion, one set per frequency."""
+    from omb200 import geometry as G
+    rng = np.random.default_rng(7)
+    base = [np.diag(G.EPS_LN_XCUT), np.diag(G.EPS_LN_XCUT), G.EPS_SIO2 * np.eye(3), np.eye(3)][:n_shapes + 1]
+    d1 = [np.diag(rng.uniform(0.05, 0.2, 3)) for _ in base]
+    d2 = [np.diag(rng.uniform(-0.1, 0.1, 3)) for _ in base]
+    sets = []
+    for s in range(nsets):
+        dw = (s - nsets / 2) * 1e-3
+        sets.append(np.stack([G.material_column(e + d * dw + dd * dw * dw / 2, d + dd * dw, dd)
+                              for e, d, dd in zip(base, d1, d2)], axis=1))
+    return np.stack(sets, axis=2)
+
+
+def smoothing_measure(device: int, nsets: int = 64, reps: int = 10):
+    """Device Kottke smoothing of the bench cross-section (the 1.5 um LiNbO3 ridge, 256x256):
+    the geometry plan once, then the material pass for `nsets` frequencies (27 values
+    (eps, d eps/d omega, d2 eps/d omega2) and the fused inverse per pixel, 1.2 GB written per
+    launch, above L2) timed with CUDA events on its stream; beside it the same pass through
+    the host-buffer C ABI call and the oracle's CPU restatement on one frequency."""
+    import torch
+    import omb200
+    from omb200 import geometry as G
+    g = omb200.Grid(DX, DY, NX, NY)
+    shapes, _ = G.ln_ridge_shapes(g, top_width=1.5)
+    minds = list(range(len(shapes) + 1))
+    M = smoothing_materials(len(shapes), nsets)
+    G.SmoothingPlan(shapes, minds, g, device=device).close()  # library and context set-up
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    plan = G.SmoothingPlan(shapes, minds, g, device=device)
+    plan_s = time.perf_counter() - t0
+    N = g.N
+    de = torch.empty(27 * N * nsets, dtype=torch.float64, device=f"cuda:{device}")
+    di = torch.empty(9 * N * nsets, dtype=torch.float64, device=f"cuda:{device}")
+    st = torch.cuda.Stream(device)
+    for _ in range(3):
+        plan.smooth_eps_device(M, de, di, stream=st)
+    st.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(reps):
+        plan.smooth_eps_device(M, de, di, stream=st)
+    e1.record(st)
+    e1.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / reps
+    nu, ni, nm = plan.counts
+    alg = nsets * (296 * N + 24 * ni)  # writes 27+9 doubles, reads the 8 B code (+24 B geometry)
+    peak, peak_kind = measured_peak_hbm()
+    t0 = time.perf_counter()
+    plan.smooth_eps(M, eps=True, epsinv=True)
+    e2e = time.perf_counter() - t0
+    plan.close()
+    del de, di
+    sys.path.insert(0, ROOT)
+    import oracle.smoothing as OS
+    t0 = time.perf_counter()
+    oplan = OS.smoothing_plan(shapes, minds, g)
+    t1 = time.perf_counter()
+    OS.epsinv_of(OS.apply_plan(oplan, M[:, :, 0]), g)
+    t2 = time.perf_counter()
+    return {"what": f"Kottke smoothing of the 1.5 um ridge, {NX}x{NY}, {nsets} frequency sets per launch",
+            "pixels": {"uniform": nu, "interface": ni, "multi": nm},
+            "plan_seconds": plan_s, "apply_seconds_per_launch": t, "pixel_sets_per_s": N * nsets / t,
+            "roofline": {"bound": "hbm", "achieved": alg / t / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / t / 1e9 / peak, "algorithmic_bytes_per_launch": alg,
+                         "peak_source": peak_kind},
+            "e2e_seconds_host_buffers": e2e,
+            "cpu_oracle": {"plan_seconds": t1 - t0, "apply_seconds_per_set": t2 - t1, "cores": 1,
+                           "kind": "port"}}
+
+
 def cpu_baseline(seconds_budget: float):
     """FP64 oracle (the reference algorithm restated in NumPy/SciPy) on one mode of the
     workload: band 0 of the 1.5 μm ridge at ω = 1/1.55, all host threads for the FFTs."""
@@ -204,17 +278,24 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
-    ap.add_argument("--case", default="full", choices=["full", "apply", "solve1", "batch"],
-                    help="apply / solve1 / batch: one operator-apply timing, one single-instance "
-                         "solve, or one batched solve of --instances cells (small, self-contained "
-                         "runs for profiling)")
+    ap.add_argument("--no-smoothing", action="store_true")
+    ap.add_argument("--case", default="full", choices=["full", "apply", "solve1", "batch", "smoothing"],
+                    help="apply / solve1 / batch / smoothing: one operator-apply timing, one "
+                         "single-instance solve, one batched solve of --instances cells, or the "
+                         "smoothing measurement with --smoothing-sets frequency sets (small, "
+                         "self-contained runs for profiling)")
     ap.add_argument("--apply-cells", type=int, default=64)
+    ap.add_argument("--smoothing-sets", type=int, default=64)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank)
+    if args.case == "smoothing":
+        print(json.dumps({"case": "smoothing", **smoothing_measure(local, nsets=args.smoothing_sets,
+                                                                    reps=args.steps)}))
+        return
     if args.case != "full":
         import omb200
         g, probs = workload(args.instances if args.case == "batch" else 1)
@@ -320,6 +401,7 @@ def main():
                      "seconds": pst["run_seconds"], "converged": pconv}
             pb.close()
         cpu = None if args.no_cpu_baseline or world > 1 else cpu_baseline(30.0)
+        smoothing = None if args.no_smoothing else smoothing_measure(local, nsets=args.smoothing_sets)
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * max_dev_s / args.steps, "higher_is_better": True,
@@ -338,6 +420,7 @@ def main():
             "gpu_launches": int(kernels),
             "roofline": roofline,
             "plain_fp64_single": plain,
+            "smoothing": smoothing,
             "cpu_baseline": cpu,
             "clocks": clock_summary(samples),
         }

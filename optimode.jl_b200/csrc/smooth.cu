@@ -47,7 +47,8 @@ constexpr int MAX_SHAPES = 255;        // shapes per geometry (slot 255 = backgr
 constexpr int MAX_MATS = 256;          // material columns (8-bit indices)
 constexpr int CLIP_CAP = MAX_VERTS + 8;
 constexpr int PLAN_NT = 128;
-constexpr int APPLY_NT = 128;
+constexpr int BULK_NT = 256;
+constexpr int SPECIAL_NT = 128;
 
 struct Shapes {
   const double2* verts;  // counter-clockwise vertices of every shape, shape after shape
@@ -337,63 +338,92 @@ __device__ __forceinline__ void inv3(const double* m, double* o) {
   o[6] = (b * f - c * e) * r; o[7] = (c * d - a * f) * r; o[8] = (a * e - b * d) * r;
 }
 
-// Material pass: grid (⌈N/128⌉, nsets), 128 threads.  Shared memory: the set's material
-// table (27·nmat doubles), then the 128-pixel staging of the 27-value and 9-value outputs.
-__global__ void __launch_bounds__(APPLY_NT) k_smooth_apply(const uint2* __restrict__ code,
-                                                           const double* __restrict__ rvol,
-                                                           const double2* __restrict__ nrm, long long N,
-                                                           const double* __restrict__ mats, int nmat,
-                                                           double* __restrict__ eps, double* __restrict__ epsinv) {
+// Material pass, part 1 (uniform pixels, all but a thin layer of the cell): grid
+// (⌈N/256⌉, nsets), 256 threads, one tile of 256 pixels per CTA.  Shared memory holds the
+// set's material columns, their ε⁻¹ and the tile's codes; the CTA then writes the tile's
+// 27·256 and 9·256 output doubles as contiguous ranges, consecutive threads on consecutive
+// addresses.  Interface and multi-material pixels are left to part 2.
+__global__ void __launch_bounds__(BULK_NT) k_smooth_bulk(const uint2* __restrict__ code, long long N,
+                                                         const double* __restrict__ mats, int nmat,
+                                                         double* __restrict__ eps, double* __restrict__ epsinv) {
   extern __shared__ double smem[];
-  double* M = smem;                          // 27·nmat
-  double* st27 = M + 27 * nmat;              // 27·128
-  double* st9 = st27 + 27 * APPLY_NT;        // 9·128
+  double* M = smem;              // 27·nmat
+  double* Mi = M + 27 * nmat;    // 9·nmat
+  uint2* cds = reinterpret_cast<uint2*>(Mi + 9 * nmat);  // BULK_NT
   const int set = blockIdx.y;
   const double* src = mats + (size_t)set * 27 * nmat;
-  for (int k = threadIdx.x; k < 27 * nmat; k += APPLY_NT) M[k] = src[k];
-  __syncthreads();
-  const long long base = (long long)blockIdx.x * APPLY_NT;
-  const long long v = base + threadIdx.x;
-  const int t = threadIdx.x;
-  if (v < N) {
-    const uint2 cd = code[v];
-    const int kind = cd.x & 0xff;
-    double o[27];
-    if (kind == KIND_INTERFACE) {
-      const double2 n = nrm[v];
-      kottke_jet(rvol[v], n.x, n.y, M + 27 * ((cd.x >> 8) & 0xff), M + 27 * ((cd.x >> 16) & 0xff), o);
-    } else if (kind == KIND_MULTI) {
-      const double* p0 = M + 27 * ((cd.x >> 8) & 0xff);
-      const double* p1 = M + 27 * ((cd.x >> 16) & 0xff);
-      const double* p2 = M + 27 * ((cd.x >> 24) & 0xff);
-      const double* p3 = M + 27 * (cd.y & 0xff);
-#pragma unroll
-      for (int k = 0; k < 27; ++k) o[k] = ((((0.0 + p0[k]) + p1[k]) + p2[k]) + p3[k]) / 4.0;
-    } else {
-      const double* p0 = M + 27 * ((cd.x >> 8) & 0xff);
-#pragma unroll
-      for (int k = 0; k < 27; ++k) o[k] = p0[k];
-    }
-#pragma unroll
-    for (int k = 0; k < 27; ++k) st27[t * 27 + k] = o[k];
-    if (epsinv) {
-      double q[9];
-      inv3(o, q);
-#pragma unroll
-      for (int k = 0; k < 9; ++k) st9[t * 9 + k] = q[k];
-    }
-  }
-  __syncthreads();
+  for (int k = threadIdx.x; k < 27 * nmat; k += BULK_NT) M[k] = src[k];
+  const long long base = (long long)blockIdx.x * BULK_NT;
   const long long rem = N - base;
-  const int np = rem < APPLY_NT ? (int)rem : APPLY_NT;
+  const int np = rem < BULK_NT ? (int)rem : BULK_NT;
+  if (threadIdx.x < np) cds[threadIdx.x] = code[base + threadIdx.x];
+  __syncthreads();
+  if (epsinv) {
+    for (int m = threadIdx.x; m < nmat; m += BULK_NT) inv3(M + 27 * m, Mi + 9 * m);
+    __syncthreads();
+  }
   if (eps) {
     double* dst = eps + (size_t)set * 27 * N + (size_t)base * 27;
-    for (int k = threadIdx.x; k < 27 * np; k += APPLY_NT) dst[k] = st27[k];
+    for (int e = threadIdx.x; e < 27 * np; e += BULK_NT) {
+      const int p = e / 27, k = e - 27 * p;
+      const unsigned x = cds[p].x;
+      if ((x & 0xff) == KIND_UNIFORM) dst[e] = M[27 * ((x >> 8) & 0xff) + k];
+    }
   }
   if (epsinv) {
     double* dst = epsinv + (size_t)set * 9 * N + (size_t)base * 9;
-    for (int k = threadIdx.x; k < 9 * np; k += APPLY_NT) dst[k] = st9[k];
+    for (int e = threadIdx.x; e < 9 * np; e += BULK_NT) {
+      const int p = e / 9, k = e - 9 * p;
+      const unsigned x = cds[p].x;
+      if ((x & 0xff) == KIND_UNIFORM) dst[e] = Mi[9 * ((x >> 8) & 0xff) + k];
+    }
   }
+}
+
+// Material pass, part 2: one thread per (listed interface or multi-material pixel, set).
+__global__ void __launch_bounds__(SPECIAL_NT) k_smooth_special(const int* __restrict__ list, int nspecial, int nsets,
+                                                               const uint2* __restrict__ code,
+                                                               const double* __restrict__ rvol,
+                                                               const double2* __restrict__ nrm, long long N,
+                                                               const double* __restrict__ mats, int nmat,
+                                                               double* __restrict__ eps, double* __restrict__ epsinv) {
+  const long long i = (long long)blockIdx.x * SPECIAL_NT + threadIdx.x;
+  if (i >= (long long)nspecial * nsets) return;
+  const int set = (int)(i / nspecial);
+  const long long v = list[i - (long long)set * nspecial];
+  const double* M = mats + (size_t)set * 27 * nmat;
+  const uint2 cd = code[v];
+  double o[27];
+  if ((cd.x & 0xff) == KIND_INTERFACE) {
+    const double2 n = nrm[v];
+    kottke_jet(rvol[v], n.x, n.y, M + 27 * ((cd.x >> 8) & 0xff), M + 27 * ((cd.x >> 16) & 0xff), o);
+  } else {
+    const double* p0 = M + 27 * ((cd.x >> 8) & 0xff);
+    const double* p1 = M + 27 * ((cd.x >> 16) & 0xff);
+    const double* p2 = M + 27 * ((cd.x >> 24) & 0xff);
+    const double* p3 = M + 27 * (cd.y & 0xff);
+#pragma unroll
+    for (int k = 0; k < 27; ++k) o[k] = ((((0.0 + p0[k]) + p1[k]) + p2[k]) + p3[k]) / 4.0;
+  }
+  if (eps) {
+    double* dst = eps + (size_t)set * 27 * N + (size_t)v * 27;
+#pragma unroll
+    for (int k = 0; k < 27; ++k) dst[k] = o[k];
+  }
+  if (epsinv) {
+    double q[9];
+    inv3(o, q);
+    double* dst = epsinv + (size_t)set * 9 * N + (size_t)v * 9;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) dst[k] = q[k];
+  }
+}
+
+// Geometry pass, part 2: the list of interface and multi-material pixels (any order).
+__global__ void k_smooth_list(const uint2* __restrict__ code, long long N, int* __restrict__ list,
+                              unsigned int* __restrict__ count) {
+  const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < N && (code[v].x & 0xff) != KIND_UNIFORM) list[atomicAdd(count, 1u)] = (int)v;
 }
 
 }  // namespace sm
@@ -410,6 +440,16 @@ struct omb_smoothing_plan {
   omb::DevBuf<uint2> code;
   omb::DevBuf<double> rvol;
   omb::DevBuf<double2> nrm;
+  omb::DevBuf<int> special;  // interface and multi-material pixels
+  int nspecial = 0;
+  // part 2 of the material pass runs on `aux`, beside part 1 (they write disjoint pixels)
+  cudaStream_t aux = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  ~omb_smoothing_plan() {
+    if (join) cudaEventDestroy(join);
+    if (fork) cudaEventDestroy(fork);
+    if (aux) cudaStreamDestroy(aux);
+  }
 };
 
 
@@ -434,17 +474,27 @@ sm::Axis axis(double D, int N) {
 int apply_launch(omb_smoothing_plan* p, const double* d_mats, int nmat, int nsets, double* d_eps, double* d_inv,
                  cudaStream_t st) {
   static bool attr_set[64] = {};
-  const size_t smem = sizeof(double) * (27 * (size_t)nmat + 36 * (size_t)sm::APPLY_NT);
+  const size_t smem = sizeof(double) * 36 * (size_t)nmat + sizeof(uint2) * sm::BULK_NT;
   const int dev = p->ctx->device;
   if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-    OMB_CU(cudaFuncSetAttribute(sm::k_smooth_apply, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(sizeof(double) * (27 * sm::MAX_MATS + 36 * sm::APPLY_NT))));
+    OMB_CU(cudaFuncSetAttribute(sm::k_smooth_bulk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(sizeof(double) * 36 * sm::MAX_MATS + sizeof(uint2) * sm::BULK_NT)));
     attr_set[dev] = true;
   }
   const long long N = (long long)p->Nx * p->Ny;
-  const dim3 grid((unsigned)((N + sm::APPLY_NT - 1) / sm::APPLY_NT), (unsigned)nsets);
-  sm::k_smooth_apply<<<grid, sm::APPLY_NT, smem, st>>>(p->code.p, p->rvol.p, p->nrm.p, N, d_mats, nmat, d_eps, d_inv);
+  if (p->nspecial > 0) {
+    OMB_CU(cudaEventRecord(p->fork, st));
+    OMB_CU(cudaStreamWaitEvent(p->aux, p->fork, 0));
+    const long long work = (long long)p->nspecial * nsets;
+    sm::k_smooth_special<<<(unsigned)((work + sm::SPECIAL_NT - 1) / sm::SPECIAL_NT), sm::SPECIAL_NT, 0, p->aux>>>(
+        p->special.p, p->nspecial, nsets, p->code.p, p->rvol.p, p->nrm.p, N, d_mats, nmat, d_eps, d_inv);
+    OMB_CU(cudaGetLastError());
+    OMB_CU(cudaEventRecord(p->join, p->aux));
+  }
+  const dim3 grid((unsigned)((N + sm::BULK_NT - 1) / sm::BULK_NT), (unsigned)nsets);
+  sm::k_smooth_bulk<<<grid, sm::BULK_NT, smem, st>>>(p->code.p, N, d_mats, nmat, d_eps, d_inv);
   OMB_CU(cudaGetLastError());
+  if (p->nspecial > 0) OMB_CU(cudaStreamWaitEvent(st, p->join, 0));
   return OMB_OK;
 }
 
@@ -530,6 +580,9 @@ extern "C" int omb_smoothing_plan_create(omb_ctx* ctx, const omb_grid* grid, int
     cudaError_t e__ = (x);                                  \
     if (e__ != cudaSuccess) return bail(cuda_fail(e__, #x)); \
   } while (0)
+  PLAN_CU(cudaStreamCreateWithFlags(&p->aux, cudaStreamNonBlocking));
+  PLAN_CU(cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming));
+  PLAN_CU(cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming));
   PLAN_CU(p->code.alloc(N, st));
   PLAN_CU(p->rvol.alloc(N, st));
   PLAN_CU(p->nrm.alloc(N, st));
@@ -550,8 +603,21 @@ extern "C" int omb_smoothing_plan_create(omb_ctx* ctx, const omb_grid* grid, int
   unsigned long long hc[3];
   PLAN_CU(cudaMemcpyAsync(hc, dcnt.p, sizeof(hc), cudaMemcpyDeviceToHost, st));
   PLAN_CU(cudaStreamSynchronize(st));
-#undef PLAN_CU
   for (int k = 0; k < 3; ++k) p->counts[k] = (long long)hc[k];
+  p->nspecial = (int)(hc[1] + hc[2]);
+  if (p->nspecial > 0) {
+    DevBuf<unsigned int> dn;
+    PLAN_CU(p->special.alloc(p->nspecial, st));
+    PLAN_CU(dn.alloc(1, st));
+    PLAN_CU(dn.zero());
+    sm::k_smooth_list<<<blocks, sm::PLAN_NT, 0, st>>>(p->code.p, (long long)N, p->special.p, dn.p);
+    PLAN_CU(cudaGetLastError());
+    unsigned int hn = 0;
+    PLAN_CU(cudaMemcpyAsync(&hn, dn.p, sizeof(hn), cudaMemcpyDeviceToHost, st));
+    PLAN_CU(cudaStreamSynchronize(st));
+    if ((int)hn != p->nspecial) return bail(fail(OMB_ERR_CUDA, "smoothing plan: inconsistent pixel list"));
+  }
+#undef PLAN_CU
   *out = p;
   return OMB_OK;
 }

@@ -203,3 +203,56 @@ function ChainRulesCore.rrule(::typeof(solve_k), ω::T0, ε⁻¹::AbstractArray{
     end
     return ((kmags, evecs), b200_solve_k_pullback)
 end
+
+# ---- Kottke smoothing on the device -------------------------------------------------------
+# `SmoothingPlan` / `smooth_ε(plan, mat_vals)` of lib/DielectricSmoothing/src/smoothing_plan.jl
+# computed by libomb200.  Shapes are passed as convex polygons: one (n, 2) vertex matrix per
+# shape in priority order (a GeometryPrimitives Polygon's vertices, or a Cuboid's four
+# corners); `minds` are the reference's 1-based material columns, the background last.
+
+mutable struct B200SmoothingPlan
+    h::Ptr{Cvoid}
+    grid::Grid{2,Float64}
+end
+
+function b200_smoothing_plan(polys::AbstractVector{<:AbstractMatrix}, minds, grid::Grid{2};
+                             fill::Symbol=:plane, device::Int=0)
+    nv = Int32[size(p, 1) for p in polys]
+    verts = Float64[]
+    for p in polys, i in axes(p, 1)
+        push!(verts, p[i, 1], p[i, 2])
+    end
+    md = Int32[m - 1 for m in minds]
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    _omb_check(ccall((:omb_smoothing_plan_create, OMB200_LIB), Cint,
+        (Ptr{Cvoid}, Ref{OmbGrid}, Int32, Ptr{Int32}, Ptr{Float64}, Ptr{Int32}, Int32, Ref{Ptr{Cvoid}}),
+        _omb_ctx(B200Solver(; device=device)), _omb_grid(grid), length(polys), nv, verts, md,
+        fill === :exact ? Int32(1) : Int32(0), h))
+    plan = B200SmoothingPlan(h[], grid)
+    finalizer(p -> ccall((:omb_smoothing_plan_destroy, OMB200_LIB), Cint, (Ptr{Cvoid},), p.h), plan)
+    return plan
+end
+
+"""
+    smooth_ε(plan::B200SmoothingPlan, mat_vals) -> Array{Float64,5}
+
+The `(3, 3, 3, Nx, Ny)` smoothed (ε, ∂ωε, ∂²ωε) of `smooth_ε(plan, mat_vals)`, computed on
+the device; `sliceinv_3x3` of its ε slice comes from `b200_smooth_epsinv`.
+"""
+function smooth_ε(plan::B200SmoothingPlan, mat_vals::AbstractMatrix{<:Real})
+    M = Matrix{Float64}(mat_vals)
+    out = Array{Float64}(undef, 3, 3, 3, plan.grid.Nx, plan.grid.Ny)
+    _omb_check(ccall((:omb_smooth_eps, OMB200_LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Float64}, Int32, Int32, Ptr{Float64}, Ptr{Float64}),
+        plan.h, M, size(M, 2), 1, out, C_NULL))
+    return out
+end
+
+function b200_smooth_epsinv(plan::B200SmoothingPlan, mat_vals::AbstractMatrix{<:Real})
+    M = Matrix{Float64}(mat_vals)
+    out = Array{Float64}(undef, 3, 3, plan.grid.Nx, plan.grid.Ny)
+    _omb_check(ccall((:omb_smooth_eps, OMB200_LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Float64}, Int32, Int32, Ptr{Float64}, Ptr{Float64}),
+        plan.h, M, size(M, 2), 1, C_NULL, out))
+    return out
+end

@@ -21,6 +21,9 @@ What it restates (reference paths are relative to the OptiMode.jl project root,
   residuals, warm start from the incoming block).
 * ``solve.py``    -- ``solve_ω²`` and the per-band Newton ``solve_k``
   (``ME/src/solve.jl:38-115, 182-210``; Newton loop as ``ME/src/solvers/gpu.jl:222-237``).
+* ``smoothing.py`` -- Kottke sub-pixel smoothing (``lib/DielectricSmoothing``: corners,
+  ``corner_sinds``/``proc_sinds``, the dispersive Taylor-jet τ average, ``smoothing_plan`` and
+  its apply, ``sliceinv_3x3``), the solver's input generator; its header lists the lines.
 * ``adjoint.py``  -- ``eig_adjt`` (``ME/src/grads/solve.jl:96-113``), ``ε⁻¹_bar``
   (``ME/src/grads/solve.jl:490-515``), ``∇ₖmag_m_n`` (``ME/src/maxwell.jl:560-566``),
   the ``solve_k`` pull-back (``ME/src/solve.jl:213-289``) and the ``sliceinv_3x3``
