@@ -291,6 +291,15 @@ int omb_smooth_eps(omb_smoothing_plan* plan, const double* mat_vals, int32_t nma
 int omb_smooth_eps_device(omb_smoothing_plan* plan, const double* mat_vals, int32_t nmat, int32_t nsets,
                           double* d_eps, double* d_epsinv, void* stream);
 
+/* Material-data VJP of omb_smooth_eps's 27-value output: mat_vals_bar (27, nmat, nsets) =
+ * ∂⟨eps_bar, smooth_ε(plan, mat_vals)⟩/∂mat_vals for eps_bar (3, 3, 3, Nx, Ny, nsets).
+ * Replaces _plan_vjp / rrule(smooth_ε, plan, mat_vals) (smoothing_plan.jl:160-218): uniform
+ * pixels pass their cotangent to their column, multi-material pixels a quarter to each corner
+ * column, interface pixels Jᵀȳ of the Taylor-jet Kottke kernel (forward derivatives along
+ * each of the two columns' 54 entries, one device thread each). */
+int omb_smooth_eps_vjp(omb_smoothing_plan* plan, const double* mat_vals, int32_t nmat, int32_t nsets,
+                       const double* eps_bar, double* mat_vals_bar);
+
 /* Waits for the device, then frees the plan. */
 int omb_smoothing_plan_destroy(omb_smoothing_plan* plan);
 

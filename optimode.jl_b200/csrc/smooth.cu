@@ -217,26 +217,49 @@ __global__ void __launch_bounds__(PLAN_NT) k_smooth_plan(Shapes sh, Axis ax, Axi
 }
 
 // ---- the dispersive Kottke kernel: a second-order Taylor jet (f, f′, f″) ----------------
+// Written over a scalar type R: double for the material pass, Dual (value and one forward
+// derivative with respect to a material entry) for the material-data VJP.
 
-struct J2 {
-  double v, d, dd;
+struct Dual {
+  double v, d;
+  __device__ Dual() = default;
+  __device__ constexpr Dual(double x) : v(x), d(0.0) {}
+  __device__ constexpr Dual(double x, double y) : v(x), d(y) {}
+};
+__device__ __forceinline__ Dual operator+(Dual a, Dual b) { return Dual(a.v + b.v, a.d + b.d); }
+__device__ __forceinline__ Dual operator-(Dual a, Dual b) { return Dual(a.v - b.v, a.d - b.d); }
+__device__ __forceinline__ Dual operator-(Dual a) { return Dual(-a.v, -a.d); }
+__device__ __forceinline__ Dual operator*(Dual a, Dual b) { return Dual(a.v * b.v, a.d * b.v + a.v * b.d); }
+__device__ __forceinline__ Dual operator*(double a, Dual b) { return Dual(a * b.v, a * b.d); }
+__device__ __forceinline__ Dual operator*(Dual a, double b) { return Dual(a.v * b, a.d * b); }
+__device__ __forceinline__ Dual operator/(double a, Dual b) {
+  const double i = a / b.v;
+  return Dual(i, -(i * b.d) / b.v);
+}
+
+template <typename R> struct J2 {
+  R v, d, dd;
 };
 
-__device__ __forceinline__ J2 jadd(J2 a, J2 b) { return J2{a.v + b.v, a.d + b.d, a.dd + b.dd}; }
-__device__ __forceinline__ J2 jsub(J2 a, J2 b) { return J2{a.v - b.v, a.d - b.d, a.dd - b.dd}; }
-__device__ __forceinline__ J2 jneg(J2 a) { return J2{-a.v, -a.d, -a.dd}; }
-__device__ __forceinline__ J2 jmul(J2 a, J2 b) {
-  return J2{a.v * b.v, a.d * b.v + a.v * b.d, (a.dd * b.v + 2.0 * a.d * b.d) + a.v * b.dd};
+template <typename R> __device__ __forceinline__ J2<R> jadd(J2<R> a, J2<R> b) {
+  return J2<R>{a.v + b.v, a.d + b.d, a.dd + b.dd};
 }
-__device__ __forceinline__ J2 jinv(J2 a) {
-  const double i = 1.0 / a.v;
-  return J2{i, -a.d * i * i, -a.dd * i * i + 2.0 * a.d * a.d * i * i * i};
+template <typename R> __device__ __forceinline__ J2<R> jsub(J2<R> a, J2<R> b) {
+  return J2<R>{a.v - b.v, a.d - b.d, a.dd - b.dd};
+}
+template <typename R> __device__ __forceinline__ J2<R> jneg(J2<R> a) { return J2<R>{-a.v, -a.d, -a.dd}; }
+template <typename R> __device__ __forceinline__ J2<R> jmul(J2<R> a, J2<R> b) {
+  return J2<R>{a.v * b.v, a.d * b.v + a.v * b.d, (a.dd * b.v + 2.0 * a.d * b.d) + a.v * b.dd};
+}
+template <typename R> __device__ __forceinline__ J2<R> jinv(J2<R> a) {
+  const R i = 1.0 / a.v;
+  return J2<R>{i, -a.d * i * i, -a.dd * i * i + 2.0 * a.d * a.d * i * i * i};
 }
 
 // τ_trans in place on a row-major jet matrix e[r*3+c]
-__device__ __forceinline__ void tau(J2* e) {
-  const J2 i = jinv(e[0]);
-  const J2 e01 = e[1], e02 = e[2], e10 = e[3], e20 = e[6];
+template <typename R> __device__ __forceinline__ void tau(J2<R>* e) {
+  const J2<R> i = jinv(e[0]);
+  const J2<R> e01 = e[1], e02 = e[2], e10 = e[3], e20 = e[6];
   e[0] = jneg(i);
   e[1] = jmul(e01, i);
   e[2] = jmul(e02, i);
@@ -248,9 +271,9 @@ __device__ __forceinline__ void tau(J2* e) {
   e[8] = jsub(e[8], jmul(jmul(e20, e02), i));
 }
 
-__device__ __forceinline__ void tau_inv(J2* t) {
-  const J2 i = jinv(t[0]);
-  const J2 t01 = t[1], t02 = t[2], t10 = t[3], t20 = t[6];
+template <typename R> __device__ __forceinline__ void tau_inv(J2<R>* t) {
+  const J2<R> i = jinv(t[0]);
+  const J2<R> t01 = t[1], t02 = t[2], t10 = t[3], t20 = t[6];
   t[0] = jneg(i);
   t[1] = jmul(jneg(t01), i);
   t[2] = jmul(jneg(t02), i);
@@ -263,7 +286,8 @@ __device__ __forceinline__ void tau_inv(J2* t) {
 }
 
 // C = A·B for row-major 3×3 (sum in index order)
-__device__ __forceinline__ void mm3(const double* A, const double* B, double* C) {
+template <typename RA, typename RB, typename RC>
+__device__ __forceinline__ void mm3(const RA* A, const RB* B, RC* C) {
 #pragma unroll
   for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -271,8 +295,9 @@ __device__ __forceinline__ void mm3(const double* A, const double* B, double* C)
 }
 
 // slice s of a 27-entry column (column-major 3×3) → row-major X = Sᵀ (E S)
-__device__ __forceinline__ void rotate_in(const double* col, int s, const double* S, const double* St, double* X) {
-  double E[9], T[9];
+template <typename R>
+__device__ __forceinline__ void rotate_in(const R* col, int s, const double* S, const double* St, R* X) {
+  R E[9], T[9];
 #pragma unroll
   for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -281,7 +306,8 @@ __device__ __forceinline__ void rotate_in(const double* col, int s, const double
   mm3(St, T, X);
 }
 
-__device__ void kottke_jet(double r1, double nx, double ny, const double* c1, const double* c2, double* out) {
+template <typename R>
+__device__ void kottke_jet(double r1, double nx, double ny, const R* c1, const R* c2, R* out) {
   // S = normcart((nx, ny, 0)), columns n, h, v (row-major S[r*3+c])
   const double hx0 = -ny, hy0 = nx;
   const double L = sqrt(hx0 * hx0 + hy0 * hy0);
@@ -290,30 +316,30 @@ __device__ void kottke_jet(double r1, double nx, double ny, const double* c1, co
   const double w0 = n1 * h2 - n2 * h1, w1 = n2 * h0 - n0 * h2, w2 = n0 * h1 - n1 * h0;
   const double S[9] = {n0, h0, w0, n1, h1, w1, n2, h2, w2};
   const double St[9] = {n0, n1, n2, h0, h1, h2, w0, w1, w2};
-  J2 a[9], b[9];
+  J2<R> a[9], b[9];
   {
-    double X0[9], X1[9], X2[9];
+    R X0[9], X1[9], X2[9];
     rotate_in(c1, 0, S, St, X0);
     rotate_in(c1, 1, S, St, X1);
     rotate_in(c1, 2, S, St, X2);
 #pragma unroll
-    for (int k = 0; k < 9; ++k) a[k] = J2{X0[k], X1[k], X2[k]};
+    for (int k = 0; k < 9; ++k) a[k] = J2<R>{X0[k], X1[k], X2[k]};
     rotate_in(c2, 0, S, St, X0);
     rotate_in(c2, 1, S, St, X1);
     rotate_in(c2, 2, S, St, X2);
 #pragma unroll
-    for (int k = 0; k < 9; ++k) b[k] = J2{X0[k], X1[k], X2[k]};
+    for (int k = 0; k < 9; ++k) b[k] = J2<R>{X0[k], X1[k], X2[k]};
   }
   tau(a);
   tau(b);
-  const J2 ra{r1, 0.0, 0.0}, rb{1.0 - r1, 0.0, 0.0};
+  const J2<R> ra{R(r1), R(0.0), R(0.0)}, rb{R(1.0 - r1), R(0.0), R(0.0)};
 #pragma unroll
   for (int k = 0; k < 9; ++k) a[k] = jadd(jmul(ra, a[k]), jmul(rb, b[k]));
   tau_inv(a);
   // back to the lab frame: S (X Sᵀ), written column-major per slice
 #pragma unroll
   for (int s = 0; s < 3; ++s) {
-    double X[9], T[9], Y[9];
+    R X[9], T[9], Y[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) X[k] = s == 0 ? a[k].v : (s == 1 ? a[k].d : a[k].dd);
     mm3(X, St, T);
@@ -419,7 +445,104 @@ __global__ void __launch_bounds__(SPECIAL_NT) k_smooth_special(const int* __rest
   }
 }
 
-// Geometry pass, part 2: the list of interface and multi-material pixels (any order).
+// ---- material-data VJP of the material pass (`_plan_vjp`) ------------------------------
+
+// Part 1: per tile of 256 pixels and set, the uniform and multi-material pixels' cotangents
+// summed per material entry (one thread per entry, pixels in order), written as the tile's
+// partial sums.
+__global__ void __launch_bounds__(BULK_NT) k_vjp_tiles(const uint2* __restrict__ code, long long N, int nmat,
+                                                       const double* __restrict__ ybar, double* __restrict__ part) {
+  __shared__ uint2 cds[BULK_NT];
+  const int set = blockIdx.y, tile = blockIdx.x;
+  const long long base = (long long)tile * BULK_NT;
+  const long long rem = N - base;
+  const int np = rem < BULK_NT ? (int)rem : BULK_NT;
+  if (threadIdx.x < np) cds[threadIdx.x] = code[base + threadIdx.x];
+  __syncthreads();
+  const double* y = ybar + (size_t)set * 27 * N + (size_t)base * 27;
+  double* out = part + ((size_t)set * gridDim.x + tile) * 27 * nmat;
+  for (int e = threadIdx.x; e < 27 * nmat; e += BULK_NT) {
+    const unsigned m = (unsigned)(e / 27);
+    const int k = e - 27 * (int)m;
+    double acc = 0.0;
+    for (int p = 0; p < np; ++p) {
+      const uint2 x = cds[p];
+      const int kind = x.x & 0xff;
+      if (kind == KIND_UNIFORM) {
+        if (((x.x >> 8) & 0xff) == m) acc = acc + y[27 * p + k];
+      } else if (kind == KIND_MULTI) {
+        const double q = y[27 * p + k] / 4.0;
+        if (((x.x >> 8) & 0xff) == m) acc = acc + q;
+        if (((x.x >> 16) & 0xff) == m) acc = acc + q;
+        if (((x.x >> 24) & 0xff) == m) acc = acc + q;
+        if ((x.y & 0xff) == m) acc = acc + q;
+      }
+    }
+    out[e] = acc;
+  }
+}
+
+// Part 2: one thread per (listed pixel, set, material entry j ∈ [0, 54)): for an interface
+// pixel, ȳ · ∂(Kottke kernel)/∂(entry j of column a, or j − 27 of column b), by a forward
+// derivative through the Taylor-jet kernel; 0 for a multi-material pixel.
+__global__ void __launch_bounds__(SPECIAL_NT) k_vjp_interface(const int* __restrict__ list, int nspecial, int nsets,
+                                                              const uint2* __restrict__ code,
+                                                              const double* __restrict__ rvol,
+                                                              const double2* __restrict__ nrm, long long N,
+                                                              const double* __restrict__ mats, int nmat,
+                                                              const double* __restrict__ ybar,
+                                                              double* __restrict__ ib) {
+  const long long i = (long long)blockIdx.x * SPECIAL_NT + threadIdx.x;
+  if (i >= (long long)nspecial * nsets * 54) return;
+  const int j = (int)(i % 54);
+  const long long rest = i / 54;
+  const int sp = (int)(rest % nspecial), set = (int)(rest / nspecial);
+  const long long v = list[sp];
+  const uint2 cd = code[v];
+  if ((cd.x & 0xff) != KIND_INTERFACE) { ib[i] = 0.0; return; }
+  const double* M = mats + (size_t)set * 27 * nmat;
+  const double* ca = M + 27 * ((cd.x >> 8) & 0xff);
+  const double* cb = M + 27 * ((cd.x >> 16) & 0xff);
+  Dual c1[27], c2[27], o[27];
+#pragma unroll
+  for (int q = 0; q < 27; ++q) {
+    c1[q] = Dual(ca[q], q == j ? 1.0 : 0.0);
+    c2[q] = Dual(cb[q], q + 27 == j ? 1.0 : 0.0);
+  }
+  const double2 n = nrm[v];
+  kottke_jet(rvol[v], n.x, n.y, c1, c2, o);
+  const double* y = ybar + (size_t)set * 27 * N + (size_t)v * 27;
+  double acc = 0.0;
+#pragma unroll
+  for (int q = 0; q < 27; ++q) acc = acc + y[q] * o[q].d;
+  ib[i] = acc;
+}
+
+// Part 3: one thread per (set, material entry): the tiles' partial sums in tile order, then
+// the interface contributions in pixel order.
+__global__ void k_vjp_reduce(const double* __restrict__ part, int ntiles, const double* __restrict__ ib,
+                             const int* __restrict__ list, int nspecial, const uint2* __restrict__ code, int nmat,
+                             int nsets, double* __restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)nsets * 27 * nmat) return;
+  const int set = (int)(i / (27 * nmat));
+  const int e = (int)(i - (long long)set * 27 * nmat);
+  const unsigned m = (unsigned)(e / 27);
+  const int k = e - 27 * (int)m;
+  double acc = 0.0;
+  for (int t = 0; t < ntiles; ++t) acc = acc + part[((size_t)set * ntiles + t) * 27 * nmat + e];
+  for (int sp = 0; sp < nspecial; ++sp) {
+    const uint2 cd = code[list[sp]];
+    if ((cd.x & 0xff) != KIND_INTERFACE) continue;
+    const double* g = ib + ((size_t)set * nspecial + sp) * 54;
+    if (((cd.x >> 8) & 0xff) == m) acc = acc + g[k];
+    if (((cd.x >> 16) & 0xff) == m) acc = acc + g[27 + k];
+  }
+  out[i] = acc;
+}
+
+// Geometry pass, part 2: the list of interface and multi-material pixels (in any order; the
+// host sorts it).
 __global__ void k_smooth_list(const uint2* __restrict__ code, long long N, int* __restrict__ list,
                               unsigned int* __restrict__ count) {
   const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -616,6 +739,11 @@ extern "C" int omb_smoothing_plan_create(omb_ctx* ctx, const omb_grid* grid, int
     PLAN_CU(cudaMemcpyAsync(&hn, dn.p, sizeof(hn), cudaMemcpyDeviceToHost, st));
     PLAN_CU(cudaStreamSynchronize(st));
     if ((int)hn != p->nspecial) return bail(fail(OMB_ERR_CUDA, "smoothing plan: inconsistent pixel list"));
+    std::vector<int> hl(p->nspecial);
+    PLAN_CU(cudaMemcpy(hl.data(), p->special.p, hl.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    std::sort(hl.begin(), hl.end());  // pixel order: deterministic sums in the VJP
+    PLAN_CU(cudaMemcpyAsync(p->special.p, hl.data(), hl.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    PLAN_CU(cudaStreamSynchronize(st));
   }
 #undef PLAN_CU
   *out = p;
@@ -686,6 +814,40 @@ extern "C" int omb_smooth_eps_device(omb_smoothing_plan* p, const double* mat_va
   OMB_CU(dmat.alloc(nm, st));
   OMB_CU(cudaMemcpyAsync(dmat.p, mat_vals, nm * sizeof(double), cudaMemcpyHostToDevice, st));
   return apply_launch(p, dmat.p, nmat, nsets, d_eps, d_epsinv, st);
+}
+
+extern "C" int omb_smooth_eps_vjp(omb_smoothing_plan* p, const double* mat_vals, int32_t nmat, int32_t nsets,
+                                  const double* eps_bar, double* mat_vals_bar) {
+  int rc = check_apply_args(p, mat_vals, nmat, nsets);
+  if (rc) return rc;
+  if (!eps_bar || !mat_vals_bar) return fail(OMB_ERR_INVALID_ARG, "eps_bar and mat_vals_bar must be non-NULL");
+  cudaStream_t st = p->ctx->stream;
+  OMB_CU(cudaSetDevice(p->ctx->device));
+  const long long N = (long long)p->Nx * p->Ny;
+  const size_t nm = 27 * (size_t)nmat * nsets, ny = 27 * (size_t)N * nsets;
+  const int ntiles = (int)((N + sm::BULK_NT - 1) / sm::BULK_NT);
+  DevBuf<double> dmat, dy, dpart, dib, dout;
+  OMB_CU(dmat.alloc(nm, st));
+  OMB_CU(dy.alloc(ny, st));
+  OMB_CU(dpart.alloc((size_t)ntiles * 27 * nmat * nsets, st));
+  OMB_CU(dib.alloc(std::max<size_t>((size_t)p->nspecial * nsets * 54, 1), st));
+  OMB_CU(dout.alloc(nm, st));
+  OMB_CU(cudaMemcpyAsync(dmat.p, mat_vals, nm * sizeof(double), cudaMemcpyHostToDevice, st));
+  OMB_CU(cudaMemcpyAsync(dy.p, eps_bar, ny * sizeof(double), cudaMemcpyHostToDevice, st));
+  sm::k_vjp_tiles<<<dim3((unsigned)ntiles, (unsigned)nsets), sm::BULK_NT, 0, st>>>(p->code.p, N, nmat, dy.p, dpart.p);
+  OMB_CU(cudaGetLastError());
+  if (p->nspecial > 0) {
+    const long long work = (long long)p->nspecial * nsets * 54;
+    sm::k_vjp_interface<<<(unsigned)((work + sm::SPECIAL_NT - 1) / sm::SPECIAL_NT), sm::SPECIAL_NT, 0, st>>>(
+        p->special.p, p->nspecial, nsets, p->code.p, p->rvol.p, p->nrm.p, N, dmat.p, nmat, dy.p, dib.p);
+    OMB_CU(cudaGetLastError());
+  }
+  sm::k_vjp_reduce<<<(unsigned)((nm + 127) / 128), 128, 0, st>>>(dpart.p, ntiles, dib.p, p->special.p, p->nspecial,
+                                                                p->code.p, nmat, nsets, dout.p);
+  OMB_CU(cudaGetLastError());
+  OMB_CU(cudaMemcpyAsync(mat_vals_bar, dout.p, nm * sizeof(double), cudaMemcpyDeviceToHost, st));
+  OMB_CU(cudaStreamSynchronize(st));
+  return OMB_OK;
 }
 
 extern "C" int omb_smoothing_plan_destroy(omb_smoothing_plan* p) {

@@ -190,6 +190,30 @@ class SmoothingPlan:
             ctypes.c_void_p(epsinv_out.data_ptr()) if epsinv_out is not None else None, st))
 
 
+    def smooth_eps_vjp(self, mat_vals, eps_bar):
+        """Material-data VJP of :meth:`smooth_eps` (``_plan_vjp``): the cotangent
+        (3, 3, 3, Nx, Ny[, n_sets]) of its output → (27, n_materials[, n_sets])."""
+        M, single = self._mats(mat_vals)
+        nmat, nsets = M.shape[1], M.shape[2]
+        g = self.grid
+        Y = np.asarray(eps_bar, dtype=np.float64)
+        if single:
+            Y = Y[..., None]
+        if Y.shape != (3, 3, 3, g.Nx, g.Ny, nsets):
+            raise ValueError(f"eps_bar must have shape (3, 3, 3, {g.Nx}, {g.Ny}[, n_sets])")
+        Y = np.asfortranarray(Y)
+        out = np.empty((27, nmat, nsets), order="F")
+        _lib.check(_lib.load().omb_smooth_eps_vjp(self._h, _lib.dptr(M), nmat, nsets, _lib.dptr(Y), _lib.dptr(out)))
+        return out[..., 0] if single else out
+
+    def smooth_eps_rrule(self, mat_vals):
+        """(smooth_ε(plan, mat_vals), pullback) like ``rrule(smooth_ε, plan, mat_vals)``
+        (``smoothing_plan.jl:206-218``): the pullback maps the output's cotangent to the
+        material data's."""
+        y = self.smooth_eps(mat_vals)
+        return y, (lambda ybar: self.smooth_eps_vjp(mat_vals, ybar))
+
+
 def smoothing_plan(shapes: Sequence, minds: Sequence[int], grid: Grid, fill: str = "plane",
                    device: int = 0) -> SmoothingPlan:
     """``smoothing_plan(shapes, minds, grid)`` (0-based ``minds``)."""

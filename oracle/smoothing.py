@@ -248,6 +248,37 @@ def smoothing_plan(shapes: Sequence, minds: Sequence[int], grid, fill: str = FIL
 
 # ---- the Kottke kernel with a second-order Taylor jet ------------------------------------
 
+class Dual:
+    """A value and its forward derivatives along several directions at once (``d`` is an
+    array, one entry per direction; every entry follows the scalar rule)."""
+
+    __slots__ = ("v", "d")
+
+    def __init__(self, v, d):
+        self.v, self.d = v, d
+
+    def __add__(self, o):
+        return Dual(self.v + o.v, self.d + o.d)
+
+    def __sub__(self, o):
+        return Dual(self.v - o.v, self.d - o.d)
+
+    def __neg__(self):
+        return Dual(-self.v, -self.d)
+
+    def __mul__(self, o):
+        if isinstance(o, Dual):
+            return Dual(self.v * o.v, self.d * o.v + self.v * o.d)
+        return Dual(self.v * o, self.d * o)
+
+    def __rmul__(self, f):
+        return Dual(f * self.v, f * self.d)
+
+    def __rtruediv__(self, f):
+        i = f / self.v
+        return Dual(i, -(i * self.d) / self.v)
+
+
 class J2:
     """Truncated Taylor number (v, d, dd) = (f, f′, f″), closed under + − × / inv."""
 
@@ -306,13 +337,18 @@ def normcart(nx: float, ny: float):
     return [[n[0], h[0], v[0]], [n[1], h[1], v[1]], [n[2], h[2], v[2]]]
 
 
+def _scalar(x):
+    return x if isinstance(x, Dual) else float(x)
+
+
 def _slice(col, s):
     """3×3 matrix of slice s (0 = ε, 1 = ∂ωε, 2 = ∂²ωε) of a 27-entry material column."""
-    return [[float(col[9 * s + r + 3 * c]) for c in range(3)] for r in range(3)]
+    return [[_scalar(col[9 * s + r + 3 * c]) for c in range(3)] for r in range(3)]
 
 
-def kottke_jet(r1: float, S, col1, col2) -> np.ndarray:
-    """εₑ_∂ωεₑ_∂²ωεₑ(r₁, S, col₁, col₂): 27 values vcat(vec(εₑ), vec(∂ωεₑ), vec(∂²ωεₑ))."""
+def kottke_jet(r1: float, S, col1, col2, dual: bool = False):
+    """εₑ_∂ωεₑ_∂²ωεₑ(r₁, S, col₁, col₂): 27 values vcat(vec(εₑ), vec(∂ωεₑ), vec(∂²ωεₑ))
+    (a list of :class:`Dual` when the columns hold Duals and ``dual`` is set)."""
     St = _T(S)
     rot1 = [_matmul(St, _matmul(_slice(col1, s), S)) for s in range(3)]
     rot2 = [_matmul(St, _matmul(_slice(col2, s), S)) for s in range(3)]
@@ -322,7 +358,7 @@ def kottke_jet(r1: float, S, col1, col2) -> np.ndarray:
     ra, rb = J2(r1), J2(1.0 - r1)
     tav = [[ra * t1[r][c] + rb * t2[r][c] for c in range(3)] for r in range(3)]
     e = _tau_inv(tav)
-    out = np.empty(27)
+    out = [None] * 27 if dual else np.empty(27)
     for s, part in enumerate(("v", "d", "dd")):
         X = [[getattr(e[r][c], part) for c in range(3)] for r in range(3)]
         Y = _matmul(S, _matmul(X, St))
@@ -359,6 +395,39 @@ def apply_plan(plan: Plan, mat_vals: np.ndarray) -> np.ndarray:
         for c in plan.mats[v]:
             acc = acc + M[:, c]
         out[:, v] = acc / 4.0
+    return out
+
+
+def plan_vjp(plan: Plan, mat_vals: np.ndarray, ybar: np.ndarray) -> np.ndarray:
+    """Material-data VJP of ``smooth_ε(plan, mat_vals)`` (``_plan_vjp``,
+    ``DS/src/smoothing_plan.jl:160-203``): ``ybar`` (27, N) → (27, n_materials).  Uniform
+    pixels pass their cotangent to their column, multi-material pixels a quarter to each corner
+    column, interface pixels Jᵀȳ of the Taylor-jet kernel for both columns, here by forward
+    derivatives along all 54 column entries at once.  Contributions are summed in pixel
+    order."""
+    M = np.asarray(mat_vals, dtype=np.float64)
+    Y = np.asarray(ybar, dtype=np.float64)
+    out = np.zeros(M.shape)
+    eye = np.eye(54)
+    for v in range(plan.kind.size):
+        kd = plan.kind[v]
+        y = Y[:, v]
+        if kd == PLAN_UNIFORM:
+            out[:, plan.mats[v, 0]] += y
+        elif kd == PLAN_MULTI:
+            for c in plan.mats[v]:
+                out[:, c] += y / 4.0
+        else:
+            a, b = plan.mats[v, 0], plan.mats[v, 1]
+            c1 = [Dual(float(M[q, a]), eye[q]) for q in range(27)]
+            c2 = [Dual(float(M[q, b]), eye[27 + q]) for q in range(27)]
+            S = normcart(float(plan.normal[v, 0]), float(plan.normal[v, 1]))
+            r = kottke_jet(float(plan.rvol[v]), S, c1, c2, dual=True)
+            g = np.zeros(54)
+            for q in range(27):
+                g = g + y[q] * r[q].d
+            out[:, a] += g[:27]
+            out[:, b] += g[27:]
     return out
 
 

@@ -146,3 +146,35 @@ def test_smooth_solve_group_index_pipeline():
     assert 1.444 < neff < 2.1
     ng = omb200.group_index(km[0], kv[0], w, np.ascontiguousarray(ei), g, np.ascontiguousarray(sm[:, :, 1]))
     assert neff < ng < 3.0
+
+
+@pytest.mark.parametrize("case", ["ridge_wg", "multi_material", "repeated_columns"])
+def test_material_vjp_matches_oracle(case):
+    """Device ``_plan_vjp`` against the oracle's (same per-pixel operations, a different
+    summation order over pixels: relative 1e-12)."""
+    import omb200
+    rng = np.random.default_rng(21)
+    if case == "ridge_wg":
+        g, og = _grid(6.0, 4.0, 32, 24)
+        shapes, minds = ridge_wg(P0), [0, 1, 2, 3]
+    elif case == "multi_material":
+        g, og = _grid(2.0, 2.0, 16, 16)
+        shapes = [np.array([[-1.0, -1.0], [0.1, -1.0], [0.1, 1.0], [-1.0, 1.0]]),
+                  np.array([[0.1, -1.0], [1.0, -1.0], [1.0, 0.12], [0.1, 0.12]])]
+        minds = [0, 1, 2]
+    else:
+        g, og = _grid(6.0, 4.0, 40, 24)
+        shapes, minds = ridge_wg([1.3, 0.55, math.pi / 9, 0.3]), [2, 2, 0, 2]
+    nmat = max(minds) + 1
+    plan = omb200.SmoothingPlan(shapes, minds, g)
+    ref = S.smoothing_plan(shapes, minds, og)
+    sets = np.stack([random_mats(rng, nmat) for _ in range(2)], axis=2)
+    ybar = rng.standard_normal((3, 3, 3, g.Nx, g.Ny, 2))
+    got = plan.smooth_eps_vjp(sets, ybar)
+    for s in range(2):
+        yf = ybar[..., s].reshape(27, g.N, order="F")
+        exp = S.plan_vjp(ref, sets[:, :, s], yf)
+        assert np.allclose(got[:, :, s], exp, rtol=1e-12, atol=1e-12 * np.abs(exp).max())
+    # the rrule form on one set
+    y, pb = plan.smooth_eps_rrule(sets[:, :, 0])
+    assert np.array_equal(pb(ybar[..., 0]), plan.smooth_eps_vjp(sets[:, :, 0], ybar[..., 0]))

@@ -192,3 +192,20 @@ def test_inverse_matches_numpy():
         A = sym(rng, 1, 6, 0.5)
         got = np.array(S.inv3(list(A.reshape(9, order="F")))).reshape(3, 3, order="F")
         assert np.allclose(got, np.linalg.inv(A), rtol=1e-12, atol=1e-14)
+
+
+def test_plan_vjp_matches_finite_differences():
+    """runtests.jl:266-290's material-data gradient through the cached apply, here as a
+    directional central difference of ⟨ȳ, smooth_ε(plan, M + hD)⟩ against ⟨VJP(ȳ), D⟩."""
+    rng = np.random.default_rng(8)
+    g = Grid(6.0, 4.0, 24, 16)
+    plan = S.smoothing_plan(ridge_wg(P0), [0, 1, 2, 3], g)
+    assert plan.counts[1] > 0
+    M = random_mats(rng, 4, aniso=0.2)
+    Y = rng.standard_normal((27, g.Nx * g.Ny))
+    D = rng.standard_normal(M.shape)
+    grad = S.plan_vjp(plan, M, Y)
+    h = 1e-6
+    f = lambda X: float(np.sum(Y * S.apply_plan(plan, X)))
+    fd = (f(M + h * D) - f(M - h * D)) / (2 * h)
+    assert float(np.sum(grad * D)) == pytest.approx(fd, rel=1e-7)
