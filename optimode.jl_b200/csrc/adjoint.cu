@@ -36,8 +36,17 @@ struct MinresState {
   double beta1, beta, oldb, alfa, dbar, epsln, oldeps, phibar, cs, sn, gamma, delta, phi;
   double dot_ey_r, dot_ey_i, dot_ez_r, dot_ez_i;
   double rtol;
+  double phibar_mark;  // phibar at itn_mark (stagnation test)
   int itn, maxit, done, status;  // status: 0 running, 1 converged, 2 maxiter, 3 breakdown
+  int itn_mark;
 };
+
+// Below rtol the recurrence residual phibar can flatten at the rounding floor of the FP64
+// operator (≈1e-12 of β₁ for right-hand sides dominated by modes near the deflated
+// eigenvalue), while the iterate has long converged.  The solve also ends, converged, when
+// phibar ≤ STALL_TOL·β₁ and did not halve over the last STALL_WINDOW iterations.
+constexpr double STALL_TOL = 1e-10;
+constexpr int STALL_WINDOW = 50;
 
 // block-reduce two complex partial sums (4 doubles) into part[blockIdx.x*4 + 0..3]
 __device__ __forceinline__ void block_reduce4(double a, double b, double c, double d, double* part) {
@@ -107,6 +116,8 @@ __global__ void k_minres_init_scalar(MinresState* S, const double* part, int nb)
   }
   S->beta1 = S->beta = sqrt(b2);
   S->phibar = S->beta1;
+  S->phibar_mark = S->beta1;
+  S->itn_mark = 0;
 }
 
 // v = (z − ⟨e,z⟩e)/beta  (start of the first iteration)
@@ -187,6 +198,13 @@ __global__ void k_minres_b_scalar(MinresState* S, const double* part, int nb) {
   S->itn++;
   if (!isfinite(S->phibar) || !isfinite(S->phi)) { S->done = 1; S->status = 3; return; }
   if (S->phibar <= S->rtol * S->beta1) { S->done = 2; S->status = 1; return; }  // finish this update
+  if (S->itn - S->itn_mark >= STALL_WINDOW) {
+    if (S->phibar <= STALL_TOL * S->beta1 && S->phibar > 0.5 * S->phibar_mark) {
+      S->done = 2; S->status = 1; return;
+    }
+    S->phibar_mark = S->phibar;
+    S->itn_mark = S->itn;
+  }
   if (S->beta == 0.0) { S->done = 2; S->status = 1; return; }                   // invariant subspace
   if (S->itn >= S->maxit) { S->done = 2; S->status = 2; }
 }

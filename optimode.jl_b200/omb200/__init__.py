@@ -11,7 +11,7 @@ from .grid import Grid  # noqa: F401
 from .ops import apply, apply_M, apply_P, HMkH, E_field, profile_apply  # noqa: F401
 from .solver import B200Solver, Batch, solve_k, solve_k_batch, solve_omega2  # noqa: F401
 from .adjoint import pullback, solve_k_rrule  # noqa: F401
-from .analysis import group_index  # noqa: F401
+from .analysis import group_index, ng_gvd  # noqa: F401
 from .geometry import (  # noqa: F401
     Polygon, SmoothingPlan, smoothing_plan, smooth_eps, smooth_epsinv, material_column,
 )

@@ -191,3 +191,37 @@ def test_group_index_matches_finite_difference():
         # without dispersion the formula reduces to 2ω/(∂ω²/∂k)
         ng0 = O.group_index(km[b], kv[b], w0, _epsinv_at(eps0, deps, w0, w0), None, g)
         assert ng0 < ng
+
+
+def _dispersive2_case():
+    g, eps0, deps = _dispersive_case()
+    dd = np.zeros_like(deps)
+    for a in range(3):
+        dd[a, a] = 0.3 * deps[a, a] - 0.05
+    dd[0, 1] = dd[1, 0] = 0.02
+    return g, eps0, deps, dd
+
+
+def _epsinv_at2(eps0, deps, dd, w, w0):
+    d = w - w0
+    e = eps0 + deps * d + dd * d * d / 2
+    return np.moveaxis(np.linalg.inv(np.moveaxis(e, (0, 1), (-2, -1))), (-2, -1), (0, 1))
+
+
+def test_ng_gvd_matches_finite_difference():
+    """GVD = ∂n_g/∂ω (ng_gvd, lib/ModeAnalysis/src/group_index.jl:112-168) against central
+    differences of n_g(ω) from modes re-solved with ε(ω) = ε₀ + ∂ε δ + ∂²ε δ²/2; the
+    difference shrinks 4× per halving of the step (truncation), ~1e-7 at h = 2.5e-4."""
+    from oracle.analysis import ng_gvd
+    g, eps0, deps, dd = _dispersive2_case()
+    w0, h = 1 / 1.55, 2.5e-4
+    km, kv = O.solve_k(w0, _epsinv_at2(eps0, deps, dd, w0, w0), g, nev=1, k_tol=1e-13, eig_tol=1e-12)
+    ng, gvd = ng_gvd(w0, km[0], kv[0], _epsinv_at2(eps0, deps, dd, w0, w0), deps, dd, g)
+    assert ng == pytest.approx(O.group_index(km[0], kv[0], w0, _epsinv_at2(eps0, deps, dd, w0, w0), deps, g),
+                               rel=1e-13)
+    ngs = []
+    for w in (w0 + h, w0 - h):
+        k2, v2 = O.solve_k(w, _epsinv_at2(eps0, deps, dd, w, w0), g, nev=1, k_tol=1e-13, eig_tol=1e-12)
+        ngs.append(O.group_index(k2[0], v2[0], w, _epsinv_at2(eps0, deps, dd, w, w0), deps + dd * (w - w0), g))
+    fd = (ngs[0] - ngs[1]) / (2 * h)
+    assert gvd == pytest.approx(fd, rel=5e-7)
