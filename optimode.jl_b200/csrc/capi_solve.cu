@@ -299,6 +299,7 @@ int omb_batch_results(omb_batch* b, omb_result* out) {
       const int rc = e->canonicalize_results();
       if (rc) return rc;
     }
+  std::vector<D2HPiece> pieces;
   for (size_t w = 0; w < b->who.size(); ++w) {
     const int i = b->who[w].inst, band0 = b->who[w].band0;
     Engine& E = *b->engines[b->who[w].eng];
@@ -321,16 +322,14 @@ int omb_batch_results(omb_batch* b, omb_result* out) {
       all_ok = all_ok && s.status == TS_CONVERGED;
       if (r.evecs) {
         // (phase gauge already applied on the device above)
-        const int rc = E.fetch_result_async(t, rb, r.evecs + 2 * n2 * band);
-        if (rc) return rc;
+        pieces.push_back({E.result_dev(t, rb), r.evecs + 2 * n2 * band, n2 * sizeof(double2)});
         b->d2h += (int64_t)(2 * n2 * sizeof(double)) + (b->canon ? 24 : 0);
       }
     }
   }
-  for (auto& e : b->engines) {
-    const int rc = e->sync();
-    if (rc) return rc;
-  }
+  // the engines' work (canonicalisation) is on the context stream, ahead of the gather
+  const int grc = gather_to_host(b->ctx, pieces.data(), pieces.size());
+  if (grc) return grc;
   if (!all_ok) return fail(OMB_ERR_NOT_CONVERGED, "one or more bands did not converge (see the per-band status)");
   return OMB_OK;
 }

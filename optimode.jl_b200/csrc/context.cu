@@ -1,8 +1,10 @@
 // Context lifetime, error reporting, twiddle tables and ε⁻¹ upload.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "context.h"
@@ -130,6 +132,50 @@ int check_grid(const omb_grid* g) {
                                          std::to_string(g->Ny) + " (see omb_fft_size_supported)");
   if (!(g->Dx > 0) || !(g->Dy > 0) || !std::isfinite(g->Dx) || !std::isfinite(g->Dy))
     return fail(OMB_ERR_INVALID_ARG, "cell sizes Dx, Dy must be finite and positive");
+  return OMB_OK;
+}
+
+int gather_to_host(omb_ctx* ctx, const D2HPiece* pieces, size_t n) {
+  size_t total = 0;
+  for (size_t i = 0; i < n; ++i) total += (pieces[i].bytes + 255) & ~(size_t)255;
+  if (total == 0) return OMB_OK;
+  if (total > ctx->pinned_bytes) {
+    OMB_CU(cudaStreamSynchronize(ctx->stream));
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    ctx->pinned = nullptr;
+    ctx->pinned_bytes = 0;
+    const size_t want = total + total / 4;
+    OMB_CU(cudaHostAlloc(&ctx->pinned, want, cudaHostAllocDefault));
+    ctx->pinned_bytes = want;
+  }
+  char* stage = static_cast<char*>(ctx->pinned);
+  std::vector<size_t> off(n);
+  size_t o = 0;
+  for (size_t i = 0; i < n; ++i) {
+    off[i] = o;
+    if (pieces[i].bytes)
+      OMB_CU(cudaMemcpyAsync(stage + o, pieces[i].src, pieces[i].bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    o += (pieces[i].bytes + 255) & ~(size_t)255;
+  }
+  OMB_CU(cudaStreamSynchronize(ctx->stream));
+  // copy out with a few threads, each over a contiguous share of the bytes
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const int nth = (int)std::min<size_t>(std::min(8u, hw), std::max<size_t>(1, total >> 23));
+  auto work = [&](int id) {
+    const size_t lo = total * id / nth, hi = total * (id + 1) / nth;
+    for (size_t i = 0; i < n; ++i) {
+      const size_t a = std::max(lo, off[i]), b = std::min(hi, off[i] + pieces[i].bytes);
+      if (a < b) std::memcpy(static_cast<char*>(pieces[i].dst) + (a - off[i]), stage + a, b - a);
+    }
+  };
+  if (nth == 1) {
+    work(0);
+  } else {
+    std::vector<std::thread> th;
+    for (int id = 1; id < nth; ++id) th.emplace_back(work, id);
+    work(0);
+    for (auto& t : th) t.join();
+  }
   return OMB_OK;
 }
 
@@ -301,6 +347,7 @@ int omb_ctx_destroy(omb_ctx* ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   if (ctx->tw_mem) cudaFree(ctx->tw_mem);
+  if (ctx->pinned) cudaFreeHost(ctx->pinned);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
   return OMB_OK;

@@ -15,6 +15,9 @@ struct omb_ctx {
   omb::TwTables tw{};
   void* tw_mem = nullptr;
   int num_sms = 0;
+  // page-locked staging for result downloads (grown on demand, kept for the context's life)
+  void* pinned = nullptr;
+  size_t pinned_bytes = 0;
 };
 
 namespace omb {
@@ -28,6 +31,16 @@ int cuda_fail(cudaError_t e, const char* what);
     cudaError_t e__ = (x);                                   \
     if (e__ != cudaSuccess) return ::omb::cuda_fail(e__, #x); \
   } while (0)
+
+// A device→host gather: every piece lands in the context's page-locked staging buffer at
+// full link speed (one synchronisation), then host threads copy the pieces to the caller's
+// (pageable) buffers in parallel.
+struct D2HPiece {
+  const void* src;  // device
+  void* dst;        // host
+  size_t bytes;
+};
+int gather_to_host(omb_ctx* ctx, const D2HPiece* pieces, size_t n);
 
 // Large device blocks (≥ BIG_BLOCK bytes) come from a per-device cache of cudaMalloc'd
 // blocks that are kept for the life of the process and handed out best-fit, so the

@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(PLAN_NT) k_smooth_plan(Shapes sh, Axis ax, Axi
 
 struct Dual {
   double v, d;
-  __device__ Dual() = default;
+  Dual() = default;
   __device__ constexpr Dual(double x) : v(x), d(0.0) {}
   __device__ constexpr Dual(double x, double y) : v(x), d(y) {}
 };

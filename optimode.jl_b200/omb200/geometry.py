@@ -234,13 +234,15 @@ def smooth_eps(shapes, mat_vals, minds=None, grid: Grid | None = None, fill: str
 
 def smooth_epsinv(shapes: Sequence[Polygon], background_eps, grid: Grid, fill: str = "plane",
                   device: int = 0) -> np.ndarray:
-    """Smoothed ε⁻¹ (reference index semantics (3, 3, Nx, Ny)) of shapes with constant ε
-    (``shape.eps``) in a constant background, computed on the GPU."""
+    """Smoothed ε⁻¹ (reference index semantics (3, 3, Nx, Ny), Fortran-ordered like the
+    reference's arrays) of shapes with constant ε (``shape.eps``) in a constant background,
+    computed on the GPU."""
     cols = [material_column(s.eps) for s in shapes] + [material_column(background_eps)]
     M = np.stack(cols, axis=1)
     plan = SmoothingPlan(shapes, list(range(len(cols))), grid, fill, device)
     try:
-        return np.ascontiguousarray(plan.smooth_eps(M, eps=False, epsinv=True))
+        # column-major, the memory layout the solver's C ABI reads (no conversion copy there)
+        return plan.smooth_eps(M, eps=False, epsinv=True)
     finally:
         plan.close()
 
