@@ -279,23 +279,27 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
   const int grid_u = std::max(1, occ_u) * ctx_->num_sms;
   OMB_CU(gram_acc_.zero());
   OMB_CU(res_acc_.zero());
-  // Two lanes of tracks (split by Σ M², the Gram cost) run their iterations on two streams,
+  // Lanes of tracks (split by Σ M², the Gram cost) run their iterations on separate streams,
   // so one lane's latency-bound kernels (k_rr, k_control, k_newton, the prefix) overlap the
-  // other lane's streaming kernels.
-  int nl = nt_ >= 2 ? 2 : 1;
-  int lane_lo[2] = {0, nt_}, lane_hi[2] = {nt_, nt_};
-  if (nl == 2) {
+  // other lanes' streaming kernels.
+  const int nl = std::max(1, std::min(LANES, nt_));
+  int lane_lo[LANES], lane_hi[LANES];
+  {
     double tot = 0, acc = 0;
     for (int gi = 0; gi < nt_; ++gi) tot += (double)tracks_[order_[gi]].M * tracks_[order_[gi]].M;
-    int h = 1;
-    for (int gi = 0; gi < nt_ - 1; ++gi) {
-      acc += (double)tracks_[order_[gi]].M * tracks_[order_[gi]].M;
-      h = gi + 1;
-      if (acc >= 0.5 * tot) break;
+    int gi = 0;
+    for (int L = 0; L < nl; ++L) {
+      lane_lo[L] = gi;
+      if (L == nl - 1) { gi = nt_; }
+      else {
+        // at least one track per lane, and leave one for each later lane
+        do { acc += (double)tracks_[order_[gi]].M * tracks_[order_[gi]].M; ++gi; }
+        while (gi < nt_ - (nl - 1 - L) && acc < tot * (L + 1) / nl);
+      }
+      lane_hi[L] = gi;
     }
-    lane_hi[0] = h; lane_lo[1] = h; lane_hi[1] = nt_;
   }
-  OMB_CU(d_pre_.alloc(4 * ((size_t)nt_ + 1), st));
+  OMB_CU(d_pre_.alloc(2 * (size_t)LANES * ((size_t)nt_ + 1), st));
 
   const char* step = "";
   auto iteration = [&](int par, int L, cudaStream_t s) -> cudaError_t {
@@ -350,29 +354,35 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
     }
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
-  cudaStream_t st2 = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  OMB_CU(cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking));
-  OMB_CU(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
-  OMB_CU(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+  cudaStream_t lst[LANES] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join[LANES] = {};
+  lst[0] = st;
   auto release = [&]() {
     if (ev_fork) cudaEventDestroy(ev_fork);
-    if (ev_join) cudaEventDestroy(ev_join);
-    if (st2) cudaStreamDestroy(st2);
+    for (int L = 1; L < LANES; ++L) {
+      if (ev_join[L]) cudaEventDestroy(ev_join[L]);
+      if (lst[L]) cudaStreamDestroy(lst[L]);
+    }
   };
+  {
+    cudaError_t ce0 = cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming);
+    for (int L = 1; L < nl && ce0 == cudaSuccess; ++L) {
+      ce0 = cudaStreamCreateWithFlags(&lst[L], cudaStreamNonBlocking);
+      if (ce0 == cudaSuccess) ce0 = cudaEventCreateWithFlags(&ev_join[L], cudaEventDisableTiming);
+    }
+    if (ce0 != cudaSuccess) { release(); return cuda_fail(ce0, "lane streams"); }
+  }
   OMB_CU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
   cudaError_t ce = cudaSuccess;
-  if (nl == 2) {
+  if (nl > 1) {
     ce = cudaEventRecord(ev_fork, st);
-    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(st2, ev_fork, 0);
+    for (int L = 1; L < nl && ce == cudaSuccess; ++L) ce = cudaStreamWaitEvent(lst[L], ev_fork, 0);
   }
-  for (int par = 0; par < 2 && ce == cudaSuccess; ++par) {
-    ce = iteration(par, 0, st);
-    if (ce == cudaSuccess && nl == 2) ce = iteration(par, 1, st2);
-  }
-  if (nl == 2) {
-    const cudaError_t j1 = cudaEventRecord(ev_join, st2);
-    const cudaError_t j2 = cudaStreamWaitEvent(st, ev_join, 0);
+  for (int par = 0; par < 2 && ce == cudaSuccess; ++par)
+    for (int L = 0; L < nl && ce == cudaSuccess; ++L) ce = iteration(par, L, lst[L]);
+  for (int L = 1; L < nl; ++L) {
+    const cudaError_t j1 = cudaEventRecord(ev_join[L], lst[L]);
+    const cudaError_t j2 = cudaStreamWaitEvent(st, ev_join[L], 0);
     if (ce == cudaSuccess) ce = j1 != cudaSuccess ? j1 : j2;
   }
   cudaError_t ee = cudaStreamEndCapture(st, &graph);

@@ -31,6 +31,7 @@ namespace omb {
 
 constexpr int MMAX = 12;         // block columns per track
 constexpr int NMAX = 3 * MMAX;   // Rayleigh–Ritz basis size
+constexpr int LANES = 2;         // track lanes (streams) of an engine's iteration graph
 constexpr int RR_NT = 128;
 
 enum TrackStatus : int {
