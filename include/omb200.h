@@ -121,6 +121,11 @@ int omb_apply_M_noalloc(int32_t Nx, int32_t Ny, double Dx, double Dy, double k, 
                             first, the others start from its eigenvectors (on the device)
                             with k_b + (ω − ω_a)·2ω_a/(∂ω²/∂k)_b per band; instances with
                             their own Hguess or kguess_bands keep them                  */
+#define OMB_WARM_CELLS 2 /* instances with the same ω and grid form a stack of cells (an
+                            eigenmode-expansion cross-section series): the middle one is
+                            solved first and the others start from its eigenvectors and
+                            per-band k — the batched form of the reference's per-cell warm
+                            start (lib/EigenmodeExpansion/src/eme.jl:58-72)             */
 
 typedef struct {
   double k_tol;           /* Newton tolerance on |Δk|                       (1e-8) */
@@ -135,7 +140,7 @@ typedef struct {
   uint64_t seed;          /* random start blocks                              (0)    */
   int32_t guard_bands;    /* extra block columns beyond the wanted bands of a
                              Newton track (OMB_NEWTON_INNER)                  (1)    */
-  int32_t warm_start;     /* OMB_WARM_NONE or OMB_WARM_SWEEP                  (NONE) */
+  int32_t warm_start;     /* OMB_WARM_NONE / OMB_WARM_SWEEP / OMB_WARM_CELLS  (NONE) */
 } omb_options;
 
 /* One solve_k problem: the lowest `nev` guided modes of one cell at frequency ω. */

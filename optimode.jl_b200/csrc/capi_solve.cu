@@ -50,8 +50,8 @@ static int options_from(const omb_options* o, SolveOptions& so) {
   so.seed = o->seed;
   if (o->guard_bands < 0 || o->guard_bands > 4) return fail(OMB_ERR_INVALID_ARG, "guard_bands must be in 0..4");
   so.guard = o->guard_bands;
-  if (o->warm_start != OMB_WARM_NONE && o->warm_start != OMB_WARM_SWEEP)
-    return fail(OMB_ERR_INVALID_ARG, "warm_start must be OMB_WARM_NONE or OMB_WARM_SWEEP");
+  if (o->warm_start != OMB_WARM_NONE && o->warm_start != OMB_WARM_SWEEP && o->warm_start != OMB_WARM_CELLS)
+    return fail(OMB_ERR_INVALID_ARG, "warm_start must be OMB_WARM_NONE, OMB_WARM_SWEEP or OMB_WARM_CELLS");
   return OMB_OK;
 }
 
@@ -201,9 +201,11 @@ int omb_batch_run(omb_batch* b) {
   b->who.clear();
   b->engines.clear();
   const int n_inst = (int)b->inst.size();
-  // sweep groups: same ε⁻¹ pointer, grid and band count, no warm start of their own
+  // warm-start groups (no warm start of their own, same grid and band count): a frequency
+  // sweep shares one ε⁻¹ pointer; a stack of cells shares one ω
   std::vector<int> anchor(n_inst, -1);  // stage-2 instance → its stage-1 neighbour
-  if (b->warm == OMB_WARM_SWEEP) {
+  if (b->warm == OMB_WARM_SWEEP || b->warm == OMB_WARM_CELLS) {
+    const bool cells = b->warm == OMB_WARM_CELLS;
     std::vector<std::vector<int>> groups;
     std::vector<int> gid(n_inst, -1);
     for (int i = 0; i < n_inst; ++i) {
@@ -211,8 +213,9 @@ int omb_batch_run(omb_batch* b) {
       if (I.nguess > 0 || !b->kbands[i].empty()) continue;
       for (size_t g = 0; g < groups.size() && gid[i] < 0; ++g) {
         const omb_instance& J = b->inst[groups[g][0]];
-        if (b->src_eps[groups[g][0]] == b->src_eps[i] && J.grid.Nx == I.grid.Nx && J.grid.Ny == I.grid.Ny &&
-            J.grid.Dx == I.grid.Dx && J.grid.Dy == I.grid.Dy && J.nev == I.nev)
+        const bool same = cells ? J.omega == I.omega : b->src_eps[groups[g][0]] == b->src_eps[i];
+        if (same && J.grid.Nx == I.grid.Nx && J.grid.Ny == I.grid.Ny && J.grid.Dx == I.grid.Dx &&
+            J.grid.Dy == I.grid.Dy && J.nev == I.nev)
           gid[i] = (int)g;
       }
       if (gid[i] < 0) { gid[i] = (int)groups.size(); groups.push_back({i}); }
@@ -220,12 +223,16 @@ int omb_batch_run(omb_batch* b) {
     }
     for (const auto& g : groups) {
       if (g.size() < 2) continue;
-      double mean = 0;
-      for (int i : g) mean += b->inst[i].omega;
-      mean /= (double)g.size();
-      int a = g[0];
-      for (int i : g)
-        if (std::fabs(b->inst[i].omega - mean) < std::fabs(b->inst[a].omega - mean)) a = i;
+      // sweep: the member nearest the mean ω; cells: the middle of the stack
+      int a = g[g.size() / 2];
+      if (!cells) {
+        double mean = 0;
+        for (int i : g) mean += b->inst[i].omega;
+        mean /= (double)g.size();
+        a = g[0];
+        for (int i : g)
+          if (std::fabs(b->inst[i].omega - mean) < std::fabs(b->inst[a].omega - mean)) a = i;
+      }
       for (int i : g)
         if (i != a) anchor[i] = a;
     }

@@ -55,7 +55,7 @@ end
 const _PREC = Dict(:fp32 => Int32(0), :fp64 => Int32(1), :mixed => Int32(2))
 const _PRECOND = Dict(:mpb => Int32(1), :diag => Int32(2))
 const _NEWTON = Dict(:inner => Int32(0), :outer => Int32(1))
-const _WARM = Dict(:none => Int32(0), :sweep => Int32(1))
+const _WARM = Dict(:none => Int32(0), :sweep => Int32(1), :cells => Int32(2))
 
 """
     B200Solver(; precision=:mixed, preconditioner=:diag, newton=:inner, device=0,
@@ -64,7 +64,8 @@ const _WARM = Dict(:none => Int32(0), :sweep => Int32(1))
 NVIDIA B200 (sm_100a) backend: batched device LOBPCG with Newton steps on k inside the
 iteration, FP32 iterations polished in FP64 to the requested tolerance.  `warm_start=:sweep`
 makes `solve_k_batch` start the instances that share one ε⁻¹ array from the solved instance
-nearest their mean ω (a frequency sweep).
+nearest their mean ω (a frequency sweep); `warm_start=:cells` starts instances that share ω
+from the middle one (the cells of an eigenmode expansion, `eme(...; warmstart=true)`).
 """
 struct B200Solver{L<:AbstractLogger} <: AbstractEigensolver{L}
     logger::L

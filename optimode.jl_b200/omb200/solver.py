@@ -16,7 +16,7 @@ from .ops import epsinv_host
 
 _PRECOND = {"mpb": 1, "diag": 2}
 _NEWTON = {"inner": 0, "outer": 1}
-_WARM = {"none": 0, "sweep": 1}
+_WARM = {"none": 0, "sweep": 1, "cells": 2}
 
 
 @dataclasses.dataclass(frozen=True)
@@ -32,7 +32,9 @@ class B200Solver:
     * ``warm_start``: ``"none"`` or ``"sweep"``: in a batch, problems that share one
       ``eps_inv`` array (the same object) and grid form a frequency sweep; the one nearest
       the group's mean ω is solved first and the others start from its eigenvectors and a
-      first-order k per band (``OMB_WARM_SWEEP``).
+      first-order k per band (``OMB_WARM_SWEEP``); ``"cells"``: problems with the same ω
+      and grid form a stack of cross-sections (eigenmode expansion); the middle one is solved
+      first and the others start from its eigenvectors and k (``OMB_WARM_CELLS``).
     """
 
     precision: str = "mixed"

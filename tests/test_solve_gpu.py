@@ -152,6 +152,29 @@ def test_sweep_warm_start(omb, case, newton):
     assert it_w.sum() < it_c.sum()
 
 
+def test_cells_warm_start(omb):
+    """A taper of cross-sections at one ω in one batch (OMB_WARM_CELLS, the batched form of
+    eme(...; warmstart=true)): every cell matches its own oracle solve, and the cells started
+    from the middle one need fewer iterations than their cold solves."""
+    from conftest import gaussian_epsinv
+    grid = O.Grid(6.0, 4.0, 24, 16)
+    g = omb.Grid(6.0, 4.0, 24, 16)
+    cells = [gaussian_epsinv((4.2, 2.1, 1.0 + 0.04 * c, 0.6)) for c in range(5)]
+    probs = [{"omega": OMEGA0, "eps_inv": e, "grid": g, "nev": 2} for e in cells]
+    cold, info_c = omb.solve_k_batch(probs, omb.B200Solver(), return_info=True)
+    warm, info_w = omb.solve_k_batch(probs, omb.B200Solver(warm_start="cells"), return_info=True)
+    for e, (kc, _), (kw, vw), iw in zip(cells, cold, warm, info_w):
+        assert np.all(iw["status"] == 0)
+        assert np.allclose(kw, kc, rtol=1e-9)
+        ref, _ = O.solve_k(OMEGA0, e, grid, nev=2, k_tol=1e-12, eig_tol=1e-11)
+        assert np.allclose(kw, ref, rtol=1e-9)
+        for b in range(2):
+            assert _resid(kw[b], e, grid, vw[b], OMEGA0 ** 2) < 2e-8
+    it_c = np.array([i["iterations"].sum() for i in info_c])
+    it_w = np.array([i["iterations"].sum() for i in info_w])
+    assert it_w.sum() < it_c.sum()
+
+
 def test_kguess_bands(omb, case):
     """Per-band Newton starts reach the same k."""
     grid, ei, km_ref, _ = case
