@@ -317,10 +317,14 @@ __global__ void k_control(TrackState* const* __restrict__ states, double* const*
     const double dw2 = s.lam[s.band] - s.omega2;
     if (last) {
       // final steps from converged eigenpairs; earlier ones while the k mismatch dominates
-      // the eigen-residual, plus at most one early step per phase near the tolerance
-      if (maxres < prm.tol) s.hmkh_ncol = 1;
-      else if (s.since_newton >= 2 && maxres < 0.1 * fabs(dw2)) s.hmkh_ncol = 1;
-      else if (s.since_newton >= 2 && s.newton_phase == 0 && maxres < 100 * prm.tol) s.hmkh_ncol = 1;
+      // the eigen-residual, plus at most one early step per phase near the tolerance.  The
+      // track returns band `band` only, and that Ritz pair's own residual bounds its error,
+      // so the polish watches it alone; the lower bands (resolved to the FP32 floor before
+      // the hand-over, which keeps the Ritz ordering) keep iterating beside it.
+      const double rb = s.resid[s.band];
+      if (rb < prm.tol) s.hmkh_ncol = 1;
+      else if (s.since_newton >= 2 && rb < 0.1 * fabs(dw2)) s.hmkh_ncol = 1;
+      else if (s.since_newton >= 2 && s.newton_phase == 0 && rb < 100 * prm.tol) s.hmkh_ncol = 1;
     } else {
       if (s.newton_steps > 0 && maxres < prm.tau_phase && fabs(s.dk_last) < prm.dk_phase) {
         finish(s, TS_PHASE_DONE); return;
@@ -370,6 +374,7 @@ __global__ void k_newton(TrackState* const* __restrict__ states, double* const* 
   if (s.mode == MODE_NEWTON_OUTER) s.iter_phase = 0;  // the reference budgets each eigensolve
   double maxres = 0;
   for (int i = 0; i < s.need; ++i) maxres = fmax(maxres, s.resid[i]);
+  if (s.mode == MODE_NEWTON_INNER) maxres = s.resid[j];  // the returned band (see k_control)
   if (!(s.k > 0)) { finish(s, TS_NAN); return; }
   if (prm.last_phase && maxres < prm.tol && fabs(dk) < prm.k_tol) { finish(s, TS_CONVERGED); return; }
   if (s.newton_steps >= prm.max_newton) { finish(s, prm.last_phase ? TS_MAXITER : TS_PHASE_DONE); return; }
