@@ -249,6 +249,8 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
   prm.tau_phase = tau;
   prm.dk_phase = 1e-6;
   prm.gram_drop = std::is_same<T, float>::value ? 1e-6 : 1e-12;
+  // an FP32 block's Gram matrices carry FP32 products: rotating below 1e-9 of ‖A‖ buys nothing
+  prm.jacobi_tol2 = std::is_same<T, float>::value ? 1e-18 : 1e-26;
   prm.maxiter = opt_.maxiter;
   prm.max_newton = opt_.max_newton;
   prm.last_phase = last ? 1 : 0;

@@ -44,6 +44,7 @@ __global__ void __launch_bounds__(RR_NT) k_rr(TrackState* const* __restrict__ st
   if (s.done) return;
   const int M = s.M;
   const int n = M + s.nWa + s.nP;
+  const double jtol2 = prm.jacobi_tol2;
   constexpr int ld = NMAX;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* G = reinterpret_cast<double2*>(smem_raw);
@@ -162,7 +163,7 @@ __global__ void __launch_bounds__(RR_NT) k_rr(TrackState* const* __restrict__ st
       }
     }
     __syncthreads();
-    jacobi_eigh(B, V, r, ld, S, ri, red);  // S is free once B = L⁻¹ S L⁻ᴴ
+    jacobi_eigh(B, V, r, ld, S, ri, red, jtol2);  // S is free once B = L⁻¹ S L⁻ᴴ
     Ev = V;
     Av = B;
   } else {
@@ -172,7 +173,7 @@ __global__ void __launch_bounds__(RR_NT) k_rr(TrackState* const* __restrict__ st
       G[a * ld + b] = B[a * ld + b];
     }
     __syncthreads();
-    jacobi_eigh(G, V, n, ld, B, ri, red);  // B's copy of G is back in G
+    jacobi_eigh(G, V, n, ld, B, ri, red, jtol2);  // B's copy of G is back in G
     if (tid == 0) {
       double tmax = 0;
       for (int i = 0; i < n; ++i) { theta[i] = G[i * ld + i].x; tmax = fmax(tmax, theta[i]); }
@@ -221,7 +222,7 @@ __global__ void __launch_bounds__(RR_NT) k_rr(TrackState* const* __restrict__ st
       G[i * ld + j] = acc;
     }
     __syncthreads();
-    jacobi_eigh(G, V, r, ld, S, ri, red);  // S is folded into G = Bᴴ S B
+    jacobi_eigh(G, V, r, ld, S, ri, red, jtol2);  // S is folded into G = Bᴴ S B
     Ev = V;
     Av = G;
   }

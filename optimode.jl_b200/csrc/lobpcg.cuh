@@ -79,6 +79,7 @@ struct IterParams {
   double tau_phase;    // phase-A exit residual (FP32 floor) — equals tol in the last phase
   double dk_phase;     // phase-A exit Newton step
   double gram_drop;    // relative Gram eigenvalue floor
+  double jacobi_tol2;  // k_rr's Jacobi stops at ‖offdiag‖²_F ≤ jacobi_tol2·‖A‖²_F
   int maxiter, max_newton, last_phase, prec_diag;
 };
 

@@ -38,8 +38,9 @@ __device__ __forceinline__ double2 zmul(double2 a, double2 b) {
 // Jacobi eigen-decomposition of the n×n Hermitian matrix A (overwritten with its
 // eigenvalues on the diagonal); V (n×n) receives the eigenvectors as columns.
 // `A2` is n×n scratch (leading dimension ld), `ri` ≥ n entries, `red` ≥ 2·(warps) doubles.
+// Sweeps stop once ‖offdiag‖²_F ≤ tol2·‖A‖²_F.
 __device__ inline void jacobi_eigh(double2* A, double2* V, int n, int ld, double2* A2, RotIdx* ri, double* red,
-                                   int max_sweeps = 20) {
+                                   double tol2 = 1e-26, int max_sweeps = 20) {
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int e = tid; e < n * n; e += nt) {
     const int r = e / n, c = e % n;
@@ -71,7 +72,7 @@ __device__ inline void jacobi_eigh(double2* A, double2* V, int n, int ld, double
     double so = 0, st = 0;
     for (int w = 0; w < (nt + 31) / 32; ++w) { so += red[2 * w]; st += red[2 * w + 1]; }
     __syncthreads();
-    if (so <= 1e-26 * st || so == 0.0) break;
+    if (so <= tol2 * st || so == 0.0) break;
     for (int round = 0; round < ne - 1; ++round) {
       // 1. rotations of this round (identity for the odd player out and settled pairs)
       for (int i = tid; i < npair; i += nt) {
