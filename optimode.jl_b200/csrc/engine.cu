@@ -593,18 +593,6 @@ int Engine::fetch_block_column(int t, int col, double* out) {
   return OMB_OK;
 }
 
-int Engine::fetch_result_async(int t, int b, double* out) {
-  const size_t n2 = 2 * (*probs_)[tracks_[t].prob].N();
-  OMB_CU(cudaMemcpyAsync(out, store_.p + store_off_[t] + (size_t)b * n2, n2 * sizeof(double2),
-                         cudaMemcpyDeviceToHost, ctx_->stream));
-  return OMB_OK;
-}
-
-int Engine::sync() {
-  OMB_CU(cudaStreamSynchronize(ctx_->stream));
-  return OMB_OK;
-}
-
 int Engine::canonicalize_results() {
   cudaStream_t st = ctx_->stream;
   // finished results (track, band), grouped by grid

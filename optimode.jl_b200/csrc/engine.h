@@ -59,9 +59,6 @@ class Engine {
   // phase gauge of every finished result on the device: the largest E component of each
   // becomes real and positive (batched per grid: one E-field pass, one argmax, one sync)
   int canonicalize_results();
-  // queue the copy of result b of track t into host memory (no synchronisation)
-  int fetch_result_async(int t, int b, double* out);
-  int sync();
   int64_t graph_launches() const { return launches_; }
   int64_t kernel_launches() const { return kernels_; }
   int max_iterations() const;
