@@ -305,6 +305,13 @@ int omb_smooth_eps_device(omb_smoothing_plan* plan, const double* mat_vals, int3
 int omb_smooth_eps_vjp(omb_smoothing_plan* plan, const double* mat_vals, int32_t nmat, int32_t nsets,
                        const double* eps_bar, double* mat_vals_bar);
 
+/* Scalar material property (e.g. the Kerr coefficient n₂) on the plan's pixels: out (Nx, Ny)
+ * from vals[nmat] — uniform pixels take their material's value, interface pixels
+ * r·v_a + (1 − r)·v_b, multi-material pixels the mean of their four corners' values.
+ * Replaces smooth_scalar / smooth_scalar_single (lib/DielectricSmoothing/src/smooth.jl:232-263)
+ * on a plan's geometry. */
+int omb_smooth_scalar(omb_smoothing_plan* plan, const double* vals, int32_t nmat, double* out);
+
 /* Waits for the device, then frees the plan. */
 int omb_smoothing_plan_destroy(omb_smoothing_plan* plan);
 

@@ -445,6 +445,28 @@ __global__ void __launch_bounds__(SPECIAL_NT) k_smooth_special(const int* __rest
   }
 }
 
+// Scalar material property on the plan (`smooth_scalar_single`): uniform pixels take their
+// material's value, interface pixels r·v_a + (1 − r)·v_b, multi-material pixels the mean of
+// their four corners' values (summed in corner order).
+__global__ void k_smooth_scalar(const uint2* __restrict__ code, const double* __restrict__ rvol, long long N,
+                                const double* __restrict__ vals, double* __restrict__ out) {
+  const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= N) return;
+  const uint2 cd = code[v];
+  const int kind = cd.x & 0xff;
+  const double a = vals[(cd.x >> 8) & 0xff];
+  double o;
+  if (kind == KIND_UNIFORM) {
+    o = a;
+  } else if (kind == KIND_INTERFACE) {
+    const double r = rvol[v];
+    o = r * a + (1.0 - r) * vals[(cd.x >> 16) & 0xff];
+  } else {
+    o = (((a + vals[(cd.x >> 16) & 0xff]) + vals[(cd.x >> 24) & 0xff]) + vals[cd.y & 0xff]) / 4.0;
+  }
+  out[v] = o;
+}
+
 // ---- material-data VJP of the material pass (`_plan_vjp`) ------------------------------
 
 // Part 1: per tile of 256 pixels and set, the uniform and multi-material pixels' cotangents
@@ -846,6 +868,24 @@ extern "C" int omb_smooth_eps_vjp(omb_smoothing_plan* p, const double* mat_vals,
                                                                 p->code.p, nmat, nsets, dout.p);
   OMB_CU(cudaGetLastError());
   OMB_CU(cudaMemcpyAsync(mat_vals_bar, dout.p, nm * sizeof(double), cudaMemcpyDeviceToHost, st));
+  OMB_CU(cudaStreamSynchronize(st));
+  return OMB_OK;
+}
+
+extern "C" int omb_smooth_scalar(omb_smoothing_plan* p, const double* vals, int32_t nmat, double* out) {
+  int rc = check_apply_args(p, vals, nmat, 1);
+  if (rc) return rc;
+  if (!out) return fail(OMB_ERR_INVALID_ARG, "out is NULL");
+  cudaStream_t st = p->ctx->stream;
+  OMB_CU(cudaSetDevice(p->ctx->device));
+  const long long N = (long long)p->Nx * p->Ny;
+  DevBuf<double> dv, dout;
+  OMB_CU(dv.alloc(nmat, st));
+  OMB_CU(dout.alloc(N, st));
+  OMB_CU(cudaMemcpyAsync(dv.p, vals, nmat * sizeof(double), cudaMemcpyHostToDevice, st));
+  sm::k_smooth_scalar<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(p->code.p, p->rvol.p, N, dv.p, dout.p);
+  OMB_CU(cudaGetLastError());
+  OMB_CU(cudaMemcpyAsync(out, dout.p, N * sizeof(double), cudaMemcpyDeviceToHost, st));
   OMB_CU(cudaStreamSynchronize(st));
   return OMB_OK;
 }

@@ -233,6 +233,7 @@ def _declare_smoothing(lib):
         "omb_smooth_eps": (ctypes.c_int, [vp, _dp, ctypes.c_int32, ctypes.c_int32, _dp, _dp]),
         "omb_smooth_eps_device": (ctypes.c_int, [vp, _dp, ctypes.c_int32, ctypes.c_int32, vp, vp, vp]),
         "omb_smooth_eps_vjp": (ctypes.c_int, [vp, _dp, ctypes.c_int32, ctypes.c_int32, _dp, _dp]),
+        "omb_smooth_scalar": (ctypes.c_int, [vp, _dp, ctypes.c_int32, _dp]),
         "omb_smoothing_plan_destroy": (ctypes.c_int, [vp]),
     }
     for name, (res, args) in sig.items():
@@ -242,5 +243,6 @@ def _declare_smoothing(lib):
 
 
 EXPORTS = EXPORTS + ("omb_smoothing_plan_create", "omb_smoothing_plan_query", "omb_smooth_eps",
-                     "omb_smooth_eps_device", "omb_smooth_eps_vjp", "omb_smoothing_plan_destroy")
+                     "omb_smooth_eps_device", "omb_smooth_eps_vjp", "omb_smooth_scalar",
+                     "omb_smoothing_plan_destroy")
 _DECLARERS.append(_declare_smoothing)

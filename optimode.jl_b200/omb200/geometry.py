@@ -206,6 +206,15 @@ class SmoothingPlan:
         _lib.check(_lib.load().omb_smooth_eps_vjp(self._h, _lib.dptr(M), nmat, nsets, _lib.dptr(Y), _lib.dptr(out)))
         return out[..., 0] if single else out
 
+    def smooth_scalar(self, vals):
+        """``smooth_scalar`` on the plan's geometry: a per-material scalar (indexed like the
+        material columns) → the (Nx, Ny) map, mixed linearly by fill fraction at interfaces."""
+        v = np.ascontiguousarray(np.asarray(vals, dtype=np.float64).reshape(-1))
+        g = self.grid
+        out = np.empty((g.Nx, g.Ny), order="F")
+        _lib.check(_lib.load().omb_smooth_scalar(self._h, _lib.dptr(v), v.size, _lib.dptr(out)))
+        return out
+
     def smooth_eps_rrule(self, mat_vals):
         """(smooth_ε(plan, mat_vals), pullback) like ``rrule(smooth_ε, plan, mat_vals)``
         (``smoothing_plan.jl:206-218``): the pullback maps the output's cotangent to the

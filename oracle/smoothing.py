@@ -22,6 +22,7 @@ What it follows (paths relative to the OptiMode.jl project root, ``DS`` =
 * ``smoothing_plan`` and the plan apply ``smooth_ε(plan, mat_vals)``
   (``DS/src/smoothing_plan.jl:26-140``): kinds 1 = uniform, 2 = interface, 3 = multi; the
   multi-material pixel sums its four corner columns in corner order and divides by 4;
+* ``smooth_scalar`` (``DS/src/smooth.jl:232-263``) on a plan;
 * ``sliceinv_3x3`` (``lib/MaxwellEigenmodes/src/linalg.jl:126-147``), here written as the
   adjugate over the determinant.
 
@@ -429,6 +430,24 @@ def plan_vjp(plan: Plan, mat_vals: np.ndarray, ybar: np.ndarray) -> np.ndarray:
             out[:, a] += g[:27]
             out[:, b] += g[27:]
     return out
+
+
+def apply_scalar(plan: Plan, vals) -> np.ndarray:
+    """``smooth_scalar`` (``DS/src/smooth.jl:232-263``) on a plan: (Nx, Ny) map of a
+    per-material scalar, r·v_a + (1 − r)·v_b at interfaces, the corner mean elsewhere."""
+    v = [float(x) for x in np.asarray(vals, dtype=np.float64).reshape(-1)]
+    N = plan.kind.size
+    out = np.empty(N)
+    for p in range(N):
+        kd, m = plan.kind[p], plan.mats[p]
+        if kd == PLAN_UNIFORM:
+            out[p] = v[m[0]]
+        elif kd == PLAN_INTERFACE:
+            r = float(plan.rvol[p])
+            out[p] = r * v[m[0]] + (1.0 - r) * v[m[1]]
+        else:
+            out[p] = (((v[m[0]] + v[m[1]]) + v[m[2]]) + v[m[3]]) / 4.0
+    return out.reshape(plan.grid.Nx, plan.grid.Ny, order="F")
 
 
 def inv3(m) -> list:

@@ -58,3 +58,16 @@ def test_no_cpu_fallback_without_gpu(cuda_available):
     with pytest.raises(_lib.OmbError) as ei:
         _lib.Context(0)
     assert "CUDA" in str(ei.value)
+
+
+def test_smoothing_needs_the_gpu(cuda_available):
+    """The device smoothing has no CPU fallback either."""
+    if cuda_available:
+        pytest.skip("a GPU is present")
+    _ensure_built()
+    import numpy as np
+    import omb200
+    square = np.array([[-0.5, -0.5], [0.5, -0.5], [0.5, 0.5], [-0.5, 0.5]])
+    with pytest.raises(omb200.OmbError) as ei:
+        omb200.SmoothingPlan([square], [0, 1], omb200.Grid(2.0, 2.0, 8, 8))
+    assert "CUDA" in str(ei.value)

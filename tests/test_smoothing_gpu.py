@@ -178,3 +178,14 @@ def test_material_vjp_matches_oracle(case):
     # the rrule form on one set
     y, pb = plan.smooth_eps_rrule(sets[:, :, 0])
     assert np.array_equal(pb(ybar[..., 0]), plan.smooth_eps_vjp(sets[:, :, 0], ybar[..., 0]))
+
+
+@pytest.mark.parametrize("name", ["ridge_wg_odd_37x23", "six_polygons_64x48"])
+def test_smooth_scalar_bit_exact(name):
+    import omb200
+    shapes, (Dx, Dy, Nx, Ny) = _cases()[name]
+    g, og = _grid(Dx, Dy, Nx, Ny)
+    minds = list(range(len(shapes) + 1))
+    vals = np.random.default_rng(5).uniform(0.5, 2.0, len(minds))
+    plan = omb200.SmoothingPlan(shapes, minds, g)
+    assert np.array_equal(plan.smooth_scalar(vals), S.apply_scalar(S.smoothing_plan(shapes, minds, og), vals))

@@ -209,3 +209,16 @@ def test_plan_vjp_matches_finite_differences():
     f = lambda X: float(np.sum(Y * S.apply_plan(plan, X)))
     fd = (f(M + h * D) - f(M - h * D)) / (2 * h)
     assert float(np.sum(grad * D)) == pytest.approx(fd, rel=1e-7)
+
+
+def test_smooth_scalar_properties():
+    """runtests.jl:130-141: a per-material scalar map (Kerr n₂) takes the material value in
+    uniform pixels, stays within the material extremes and mixes at interfaces."""
+    vals = np.array([2.5e-19, 2.6e-20, 1.8e-19, 0.0])
+    plan = S.smoothing_plan(ridge_wg(P0), [0, 1, 2, 3], GRID)
+    n2 = S.apply_scalar(plan, vals)
+    assert n2.shape == (GRID.Nx, GRID.Ny)
+    assert n2[15, 12] == vals[0]   # core
+    assert n2[15, 3] == vals[2]    # substrate
+    assert np.all((n2 >= vals.min() - 1e-15) & (n2 <= vals.max() + 1e-15))
+    assert np.any((n2 > vals.min() + 1e-12 * vals.max()) & (n2 < vals.max() * (1 - 1e-12)) & ~np.isin(n2, vals))
