@@ -135,30 +135,24 @@ int check_grid(const omb_grid* g) {
   return OMB_OK;
 }
 
-int gather_to_host(omb_ctx* ctx, const D2HPiece* pieces, size_t n) {
-  size_t total = 0;
-  for (size_t i = 0; i < n; ++i) total += (pieces[i].bytes + 255) & ~(size_t)255;
-  if (total == 0) return OMB_OK;
-  if (total > ctx->pinned_bytes) {
-    OMB_CU(cudaStreamSynchronize(ctx->stream));
-    if (ctx->pinned) cudaFreeHost(ctx->pinned);
-    ctx->pinned = nullptr;
-    ctx->pinned_bytes = 0;
-    const size_t want = total + total / 4;
-    OMB_CU(cudaHostAlloc(&ctx->pinned, want, cudaHostAllocDefault));
-    ctx->pinned_bytes = want;
-  }
+namespace {
+
+constexpr size_t STAGE_CAP = (size_t)512 << 20;  // page-locked staging kept per context
+inline size_t padded(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// One batch of pieces that fits the staging buffer: queue the copies, synchronise once,
+// then copy out with a few host threads, each over a contiguous share of the bytes.
+int gather_batch(omb_ctx* ctx, const D2HPiece* pieces, size_t n) {
   char* stage = static_cast<char*>(ctx->pinned);
   std::vector<size_t> off(n);
-  size_t o = 0;
+  size_t total = 0;
   for (size_t i = 0; i < n; ++i) {
-    off[i] = o;
+    off[i] = total;
     if (pieces[i].bytes)
-      OMB_CU(cudaMemcpyAsync(stage + o, pieces[i].src, pieces[i].bytes, cudaMemcpyDeviceToHost, ctx->stream));
-    o += (pieces[i].bytes + 255) & ~(size_t)255;
+      OMB_CU(cudaMemcpyAsync(stage + total, pieces[i].src, pieces[i].bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    total += padded(pieces[i].bytes);
   }
   OMB_CU(cudaStreamSynchronize(ctx->stream));
-  // copy out with a few threads, each over a contiguous share of the bytes
   const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
   const int nth = (int)std::min<size_t>(std::min(8u, hw), std::max<size_t>(1, total >> 23));
   auto work = [&](int id) {
@@ -175,6 +169,49 @@ int gather_to_host(omb_ctx* ctx, const D2HPiece* pieces, size_t n) {
     for (int id = 1; id < nth; ++id) th.emplace_back(work, id);
     work(0);
     for (auto& t : th) t.join();
+  }
+  return OMB_OK;
+}
+
+}  // namespace
+
+int gather_to_host(omb_ctx* ctx, const D2HPiece* pieces, size_t n) {
+  size_t total = 0, largest = 0;
+  for (size_t i = 0; i < n; ++i) {
+    total += padded(pieces[i].bytes);
+    largest = std::max(largest, padded(pieces[i].bytes));
+  }
+  if (total == 0) return OMB_OK;
+  const size_t want = std::max(std::min(total, STAGE_CAP), largest);
+  if (want > ctx->pinned_bytes) {
+    OMB_CU(cudaStreamSynchronize(ctx->stream));
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    ctx->pinned = nullptr;
+    ctx->pinned_bytes = 0;
+    if (cudaHostAlloc(&ctx->pinned, want, cudaHostAllocDefault) != cudaSuccess) {
+      // no page-locked memory to be had: plain copies into the caller's buffers
+      ctx->pinned = nullptr;
+      cudaGetLastError();
+      for (size_t i = 0; i < n; ++i)
+        if (pieces[i].bytes)
+          OMB_CU(cudaMemcpyAsync(pieces[i].dst, pieces[i].src, pieces[i].bytes, cudaMemcpyDeviceToHost, ctx->stream));
+      OMB_CU(cudaStreamSynchronize(ctx->stream));
+      return OMB_OK;
+    }
+    ctx->pinned_bytes = want;
+  }
+  // batches of pieces that fit the staging buffer
+  size_t first = 0, bytes = 0;
+  for (size_t i = 0; i <= n; ++i) {
+    if (i == n || bytes + padded(pieces[i].bytes) > ctx->pinned_bytes) {
+      if (i > first) {
+        const int rc = gather_batch(ctx, pieces + first, i - first);
+        if (rc) return rc;
+      }
+      first = i;
+      bytes = 0;
+    }
+    if (i < n) bytes += padded(pieces[i].bytes);
   }
   return OMB_OK;
 }
