@@ -210,6 +210,8 @@ end
 # computed by libomb200.  Shapes are passed as convex polygons: one (n, 2) vertex matrix per
 # shape in priority order (a GeometryPrimitives Polygon's vertices, or a Cuboid's four
 # corners); `minds` are the reference's 1-based material columns, the background last.
+# `smooth_ε` gains a method for the device plan (MaxwellEigenmodes already has
+# `using DielectricSmoothing`, src/MaxwellEigenmodes.jl:29).
 
 mutable struct B200SmoothingPlan
     h::Ptr{Cvoid}
@@ -240,7 +242,7 @@ end
 The `(3, 3, 3, Nx, Ny)` smoothed (ε, ∂ωε, ∂²ωε) of `smooth_ε(plan, mat_vals)`, computed on
 the device; `sliceinv_3x3` of its ε slice comes from `b200_smooth_epsinv`.
 """
-function smooth_ε(plan::B200SmoothingPlan, mat_vals::AbstractMatrix{<:Real})
+function DielectricSmoothing.smooth_ε(plan::B200SmoothingPlan, mat_vals::AbstractMatrix{<:Real})
     M = Matrix{Float64}(mat_vals)
     out = Array{Float64}(undef, 3, 3, 3, plan.grid.Nx, plan.grid.Ny)
     _omb_check(ccall((:omb_smooth_eps, OMB200_LIB), Cint,
