@@ -71,3 +71,22 @@ def test_smoothing_needs_the_gpu(cuda_available):
     with pytest.raises(omb200.OmbError) as ei:
         omb200.SmoothingPlan([square], [0, 1], omb200.Grid(2.0, 2.0, 8, 8))
     assert "CUDA" in str(ei.value)
+
+
+def test_smoothing_argument_checks_without_gpu():
+    """Host-side argument checks of the smoothing binding run before any device call."""
+    import numpy as np
+    import omb200
+    g = omb200.Grid(2.0, 2.0, 8, 8)
+    square = np.array([[-0.5, -0.5], [0.5, -0.5], [0.5, 0.5], [-0.5, 0.5]])
+    with pytest.raises(ValueError):
+        omb200.SmoothingPlan([square], [0, 1], g, fill="area")
+    with pytest.raises(ValueError):
+        omb200.SmoothingPlan([square], [0], g)
+    with pytest.raises(ValueError):
+        omb200.material_column(np.eye(2))
+    col = omb200.material_column(np.diag([1.0, 2.0, 3.0]), np.eye(3))
+    assert col.shape == (27,) and col[4] == 2.0 and col[9] == 1.0 and col[18:].sum() == 0.0
+    # clockwise outlines are stored counter-clockwise
+    p = omb200.Polygon(square[::-1])
+    assert np.array_equal(p.vertices, square)
