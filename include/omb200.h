@@ -2,9 +2,9 @@
  * libomb200 — B200 (sm_100a) plane-wave Helmholtz eigensolver, C ABI.
  *
  * The drop-in boundary for OptiMode.jl's `solve_ω²` / `solve_k` hot path and its adjoint
- * pull-back.  Julia binds these with `ccall` from a new `B200Solver <: AbstractEigensolver`
- * (see INTEGRATION.md); Python binds them with ctypes.  Every symbol takes plain pointers
- * and sizes; no torch or CUDA types cross the boundary.
+ * pull-back.  Julia binds these with `ccall` from a new `B200Solver <: AbstractEigensolver`;
+ * Python binds them with ctypes.  Every symbol takes plain pointers and sizes; no torch or
+ * CUDA types cross the boundary.
  *
  * Conventions
  *  - Host arrays are the reference's column-major Julia arrays, passed as raw memory:
@@ -69,6 +69,18 @@ const char* omb_last_error(void);
 int omb_ctx_create(int device, omb_ctx** out);
 int omb_ctx_destroy(omb_ctx* ctx);
 
+/* Limit of every bounded wait in the context's streaming kernels (the Gram and update
+ * pipelines: a wait for a bulk copy to land or a stage to be released), in seconds, (0, 60];
+ * 1 s by default.  A wait that runs out makes its kernel record an error and return, and the
+ * call that launched it returns OMB_ERR_TIMEOUT with the context still usable.  No reference
+ * counterpart (its solvers have no device-side waits). */
+int omb_ctx_set_wait_limit(omb_ctx* ctx, double seconds);
+/* Self-test of that failure path: one kernel waits, with the context's limit, on a barrier
+ * phase that nothing completes.  Returns OMB_ERR_TIMEOUT and the kernel's error code in
+ * *code (1: a full-stage wait ran out); OMB_OK would mean the wait completed.  No reference
+ * counterpart. */
+int omb_selftest_wait(omb_ctx* ctx, int32_t* code);
+
 /* Hout = op(k) Hin for `ncol` columns.
  * Replaces HelmholtzMap(Hout, Hin) / _M! (lib/MaxwellEigenmodes/src/maxwell.jl:471-481,
  * 1007-1025; device form _gpu_M!, src/solvers/gpu.jl:157-166) for OMB_OP_M, and
@@ -89,17 +101,18 @@ int omb_efield(omb_ctx* ctx, int precision, const omb_grid* grid, double k,
 
 /* Allocation-free FP32 Hout = M̂(k) Hin on caller-owned device memory.  No counterpart in
  * the reference: it exists for callers that cannot allocate device memory when they need
- * the operator — code inside a CUDA stream capture (allocations are not capturable), host
- * frameworks that own the device pool and forbid foreign cudaMalloc/cudaFree, and hot
- * loops that must not pay allocation latency.  It allocates nothing: its scratch is a
- * fixed static device array (6 MiB) held by every GPU that loads the library until exit.
+ * the operator — host frameworks that own the whole device pool and forbid foreign
+ * cudaMalloc/cudaFree (a Julia or PyTorch caching allocator), callers whose device-memory
+ * budget is fixed up front, and hot loops that must not pay the latency and implicit device
+ * synchronisation of cudaMalloc/cudaFree.  It allocates nothing: its scratch is a fixed
+ * static device array (6 MiB) held by every GPU that loads the library until exit.
  *   d_epsinv : device Float32 (3, 3, Nx, Ny), symmetric per pixel
  *   d_H_in, d_H_out : device ComplexF32 (2, Nx, Ny), ncol columns each
  *   stream   : a cudaStream_t, or NULL for the legacy default stream
  * Limit: Nx·Ny·ncol ≤ OMB_NOALLOC_MAX_PIXEL_COLUMNS, else OMB_ERR_INVALID_ARG.  All calls
- * share the scratch, so calls that overlap on the GPU race; the first call on a device
- * sets up the scratch address and twiddle tables (blocking) and must precede any stream
- * capture. */
+ * share the scratch, so calls that overlap on the GPU race.  The first call in a CUDA
+ * context sets up the scratch address and twiddle tables with a blocking copy; make it
+ * before any stream capture (a first call on a capturing stream is refused). */
 #define OMB_NOALLOC_MAX_PIXEL_COLUMNS 262144
 int omb_apply_M_noalloc(int32_t Nx, int32_t Ny, double Dx, double Dy, double k, const float* d_epsinv,
                         int32_t ncol, const void* d_H_in, void* d_H_out, void* stream);

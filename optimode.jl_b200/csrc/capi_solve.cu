@@ -411,7 +411,10 @@ int omb_solve_omega2(omb_ctx* ctx, const omb_grid* grid, double k, const double*
       if (rc) return rc;
     }
   }
-  if (s.status != TS_CONVERGED) return fail(OMB_ERR_NOT_CONVERGED, "solve_omega2 did not converge");
+  if (s.status != TS_CONVERGED)
+    return fail(status_code(s.status), s.status == TS_ORTHO ? "solve_omega2: the block lost rank (orthonormalisation failed)"
+                                       : s.status == TS_NAN ? "solve_omega2: non-finite Ritz values"
+                                                            : "solve_omega2 did not converge");
   return OMB_OK;
 }
 

@@ -18,6 +18,8 @@ struct omb_ctx {
   // page-locked staging for result downloads (grown on demand, kept for the context's life)
   void* pinned = nullptr;
   size_t pinned_bytes = 0;
+  // limit of every bounded wait in the streaming kernels (omb_ctx_set_wait_limit)
+  uint64_t wait_ns = 1000000000ull;
 };
 
 namespace omb {

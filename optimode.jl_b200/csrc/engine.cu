@@ -336,12 +336,14 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
       return e;
     k_live_prefix<<<1, 1024, 0, s>>>(d_state_ptrs_.p + a, d_n2_.p + a, n, rg, UpdCfg<T>::R, preg, preu);
     if (!ok("k_live_prefix", cudaGetLastError())) return e;
-    k_gram<T><<<grid_g, GramCfg<T>::NT, sm_gram, s>>>(d_descs.p + a, preg, n, par, nmax, rg, gstages, d_err_.p);
+    k_gram<T><<<grid_g, GramCfg<T>::NT, sm_gram, s>>>(d_descs.p + a, preg, n, par, nmax, rg, gstages, d_err_.p,
+                                                       ctx_->wait_ns);
     if (!ok("k_gram", cudaGetLastError())) return e;
     k_rr<<<n, RR_NT, sm_rr, s>>>(d_state_ptrs_.p + a, d_gram_ptrs_.p + a, d_coef_ptrs_.p + a, d_coef32_ptrs_.p + a, n,
                                  prm);
     if (!ok("k_rr", cudaGetLastError())) return e;
-    update_kernel<<<grid_u, UpdCfg<T>::NT, sm_upd, s>>>(d_descs.p + a, preu, n, par, prm.prec_diag, d_err_.p);
+    update_kernel<<<grid_u, UpdCfg<T>::NT, sm_upd, s>>>(d_descs.p + a, preu, n, par, prm.prec_diag, d_err_.p,
+                                                        ctx_->wait_ns);
     if (!ok("k_update", cudaGetLastError())) return e;
     k_control<<<(n + 3) / 4, 128, 0, s>>>(d_state_ptrs_.p + a, d_res_ptrs_.p + a, n, prm);
     ok("k_control", cudaGetLastError());
@@ -423,7 +425,8 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
   int perr = 0;
   OMB_CU(cudaMemcpy(&perr, d_err_.p, sizeof(int), cudaMemcpyDeviceToHost));
   if (perr != PIPE_OK)
-    return fail(OMB_ERR_CUDA, "streaming kernel pipeline wait timed out (code " + std::to_string(perr) + ")");
+    return fail(OMB_ERR_TIMEOUT, "a streaming kernel's pipeline wait ran out after " +
+                                     std::to_string(ctx_->wait_ns / 1e9) + " s (code " + std::to_string(perr) + ")");
   last_prec_ = std::is_same<T, float>::value ? 0 : 1;
   return rc_out;
 }

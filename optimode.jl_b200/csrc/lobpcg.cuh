@@ -176,7 +176,7 @@ __device__ __forceinline__ void gram_item(int q, int nblk, int nb4, int& which, 
 template <typename T>
 __global__ void __launch_bounds__(GramCfg<T>::NT, 1)
     k_gram(const TrackDesc<T>* __restrict__ D, const int* __restrict__ pre, int ntracks, int par, int nmax,
-           int R, int stages, int* __restrict__ err) {
+           int R, int stages, int* __restrict__ err, uint64_t wait_ns) {
   using C = cplx<T>;
   using Cfg = GramCfg<T>;
   const int CS = R + Cfg::PAD;
@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(GramCfg<T>::NT, 1)
       const long long r0 = w.row0();
       const int rows = (int)min((long long)R, d.n2 - r0);
       if (lane == 0) {
-        ok = mbar_wait(&empty[q], ph ^ 1);
+        ok = mbar_wait(&empty[q], ph ^ 1, wait_ns);
         if (ok) mbar_arrive_expect_tx(&full[q], (uint32_t)(2 * n * rows * sizeof(C)));
         else pipe_fail(err, PIPE_EMPTY_TIMEOUT);
       }
@@ -224,7 +224,8 @@ __global__ void __launch_bounds__(GramCfg<T>::NT, 1)
     // leave no copy in flight: the last fill of every stage has landed
     if (lane == 0)
       for (int k = 0; k < stages; ++k)
-        if (fills[k] > 0 && !mbar_wait(&full[k], (uint32_t)((fills[k] - 1) & 1))) pipe_fail(err, PIPE_DRAIN_TIMEOUT);
+        if (fills[k] > 0 && !mbar_wait(&full[k], (uint32_t)((fills[k] - 1) & 1), drain_limit(wait_ns)))
+          pipe_fail(err, PIPE_DRAIN_TIMEOUT);
     return;
   }
   // ---- consumers: thread (item, sub) accumulates one 4×4 block over rows sub, sub+split, …
@@ -259,7 +260,7 @@ __global__ void __launch_bounds__(GramCfg<T>::NT, 1)
         for (int j = 0; j < 4; ++j) acc[i][j] = mk<C>(0, 0);
     }
     const int rows = (int)min((long long)R, d.n2 - w.row0());
-    bool ok = failed ? false : mbar_wait(&full[q], ph);
+    bool ok = failed ? false : mbar_wait(&full[q], ph, wait_ns);
     ok = __all_sync(0xffffffffu, ok);
     if (!ok && !failed) { pipe_fail(err, PIPE_FULL_TIMEOUT); failed = true; }
     if (!failed) {
@@ -342,7 +343,7 @@ template <typename T, int M, int MB>
 __device__ __forceinline__ void update_tile(const TrackDesc<T>& d, const TrackState& s, long long r0, int rows,
                                             int par, int prec_diag, const cplx<T>* stage0, uint64_t* full,
                                             uint64_t* empty, int& q, uint32_t& ph, bool& failed,
-                                            double (&racc)[MB], int* err) {
+                                            double (&racc)[MB], int* err, uint64_t wait_ns) {
   using C = cplx<T>;
   using Cfg = UpdCfg<T>;
   constexpr int R = Cfg::R, LG = Cfg::LG, S = Cfg::STAGES;
@@ -352,7 +353,7 @@ __device__ __forceinline__ void update_tile(const TrackDesc<T>& d, const TrackSt
 #pragma unroll
   for (int m = 0; m < M; ++m) x[m] = ax[m] = p[m] = ap[m] = mk<C>(0, 0);
   for (int l0 = 0; l0 < n; l0 += LG) {
-    bool ok = failed ? false : mbar_wait(&full[q], ph);
+    bool ok = failed ? false : mbar_wait(&full[q], ph, wait_ns);
     ok = __all_sync(0xffffffffu, ok);
     if (!ok && !failed) { pipe_fail(err, PIPE_FULL_TIMEOUT); failed = true; }
     if (!failed) {
@@ -422,7 +423,7 @@ __device__ __forceinline__ void update_tile(const TrackDesc<T>& d, const TrackSt
 template <typename T, int MB>
 __global__ void __launch_bounds__(UpdCfg<T>::NT, 1)
     k_update(const TrackDesc<T>* __restrict__ D, const int* __restrict__ pre, int ntracks, int par,
-             int prec_diag, int* __restrict__ err) {
+             int prec_diag, int* __restrict__ err, uint64_t wait_ns) {
   using C = cplx<T>;
   using Cfg = UpdCfg<T>;
   constexpr int R = Cfg::R, LG = Cfg::LG, S = Cfg::STAGES;
@@ -453,7 +454,7 @@ __global__ void __launch_bounds__(UpdCfg<T>::NT, 1)
       for (int l0 = 0; l0 < n && ok; l0 += LG) {
         const int nl = min(LG, n - l0);
         if (lane == 0) {
-          ok = mbar_wait(&empty[q], ph ^ 1);
+          ok = mbar_wait(&empty[q], ph ^ 1, wait_ns);
           if (ok)
             mbar_arrive_expect_tx(&full[q], (uint32_t)((2 * nl * rows + 2 * nl * MMAX) * sizeof(C)));
           else
@@ -478,7 +479,8 @@ __global__ void __launch_bounds__(UpdCfg<T>::NT, 1)
     }
     if (lane == 0)
       for (int k = 0; k < S; ++k)
-        if (fills[k] > 0 && !mbar_wait(&full[k], (uint32_t)((fills[k] - 1) & 1))) pipe_fail(err, PIPE_DRAIN_TIMEOUT);
+        if (fills[k] > 0 && !mbar_wait(&full[k], (uint32_t)((fills[k] - 1) & 1), drain_limit(wait_ns)))
+          pipe_fail(err, PIPE_DRAIN_TIMEOUT);
     return;
   }
   // ---- consumers: thread r owns row row0 + r of each tile
@@ -499,7 +501,7 @@ __global__ void __launch_bounds__(UpdCfg<T>::NT, 1)
   case MM:                                                                                              \
     if constexpr (MM <= MB)                                                                             \
       update_tile<T, (MM <= MB ? MM : 1), MB>(d, s, r0, rows, par, prec_diag, stage0, full, empty, q, ph, \
-                                              failed, racc, err);                                       \
+                                              failed, racc, err, wait_ns);                              \
     break;
       OMB_UPD_CASE(1) OMB_UPD_CASE(2) OMB_UPD_CASE(3) OMB_UPD_CASE(4) OMB_UPD_CASE(5) OMB_UPD_CASE(6)
       OMB_UPD_CASE(7) OMB_UPD_CASE(8) OMB_UPD_CASE(9) OMB_UPD_CASE(10) OMB_UPD_CASE(11) OMB_UPD_CASE(12)

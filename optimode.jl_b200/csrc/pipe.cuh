@@ -1,10 +1,12 @@
 // Bulk-copy pipeline primitives (sm_90+/sm_100a): mbarrier phases and 1D bulk copies
 // (cp.async.bulk, the TMA's untiled form) from global into this CTA's shared memory.
 //
-// Every wait is bounded in time: a wait that has not completed after WAIT_NS nanoseconds
-// of the global timer returns false, and the caller records an error and leaves the
-// pipeline instead of spinning on (a poll of mbarrier.try_wait may itself suspend, so a
-// bound on the number of polls would not bound the time).
+// Every wait is bounded in time: a wait that has not completed after its limit (a kernel
+// argument, WAIT_NS = 1 s by default) of the global timer returns false, and the caller
+// records an error and leaves the pipeline instead of spinning on (a poll of
+// mbarrier.try_wait may itself suspend, so a bound on the number of polls would not bound
+// the time).  The final drain of a producer, which makes sure none of its own bulk copies
+// is still in flight when the CTA exits, always waits up to at least WAIT_NS.
 #pragma once
 
 #include <stdint.h>
@@ -49,14 +51,16 @@ __device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Wait for the phase with the given parity to complete; false after WAIT_NS.
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity) {
+// Wait for the phase with the given parity to complete; false after limit_ns.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, uint64_t limit_ns = WAIT_NS) {
   if (mbar_test(b, parity)) return true;
   const uint64_t t0 = global_ns();
   while (!mbar_test(b, parity))
-    if (global_ns() - t0 > WAIT_NS) return false;
+    if (global_ns() - t0 > limit_ns) return false;
   return true;
 }
+// Limit of a producer's final drain wait.
+__device__ __forceinline__ uint64_t drain_limit(uint64_t limit_ns) { return limit_ns > WAIT_NS ? limit_ns : WAIT_NS; }
 // Bulk copy of `bytes` (multiple of 16; both addresses 16-byte aligned) completing on `b`.
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* b) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(

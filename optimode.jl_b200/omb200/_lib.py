@@ -246,3 +246,21 @@ EXPORTS = EXPORTS + ("omb_smoothing_plan_create", "omb_smoothing_plan_query", "o
                      "omb_smooth_eps_device", "omb_smooth_eps_vjp", "omb_smooth_scalar",
                      "omb_smoothing_plan_destroy")
 _DECLARERS.append(_declare_smoothing)
+
+
+def _declare_diag(lib):
+    f = lib.omb_ctx_set_wait_limit
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_void_p, ctypes.c_double]
+    f = lib.omb_selftest_wait
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]
+
+
+EXPORTS = EXPORTS + ("omb_ctx_set_wait_limit", "omb_selftest_wait")
+_DECLARERS.append(_declare_diag)
+
+
+def set_wait_limit(seconds: float, device: int = 0) -> None:
+    """Limit (seconds) of the streaming kernels' bounded waits on this device's context."""
+    check(load().omb_ctx_set_wait_limit(context(device).handle, float(seconds)))
