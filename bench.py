@@ -3,7 +3,8 @@
 
 One *step* is one batched ``solve_k`` over a fixed batch of synthetic cross-sections of the
 x-cut LiNbO₃ ridge family (8×5 μm cell, 256×256 grid, 4 bands, film 0.6 μm, etch 0.3 μm,
-70° sidewalls, top widths {1.0, 1.5, 2.0} μm, ω swept over [1/1.60, 1/1.50] μm⁻¹), solved
+70° sidewalls, top widths {1.0, 1.5, 2.0} μm, ω = 1/λ with λ stepping by 0.025 μm around
+1.55 μm: {1.50, 1.525, 1.55, 1.575} on one GPU, ω = 1/1.55 always included), solved
 with the batched, mixed-precision, inner-Newton B200 solver.  ``value`` counts converged
 modes (Newton |Δk| < 1e-8 and FP64 residual < 1e-8) per device second with the inputs
 resident (``omb_batch_run``); ``e2e`` is the same metric through ``omb_solve_k`` with host
@@ -23,7 +24,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import re
 import subprocess
 import sys
 import threading
@@ -44,11 +44,14 @@ FALLBACK_HBM_GBS = 6650.0
 
 
 def rank_omegas(n_om: int, rank: int = 0, world: int = 1):
-    """The ω values of one rank: the whole job sweeps n_om·world frequencies uniform in
-    [1/1.60, 1/1.50] μm⁻¹ and rank r takes the r-th contiguous block of n_om (weak scaling:
-    every rank gets the same amount of work, no two ranks solve the same instance)."""
-    allw = np.linspace(1 / 1.60, 1 / 1.50, n_om * world)
-    return allw[rank * n_om:(rank + 1) * n_om]
+    """The ω values of one rank: the whole job sweeps n_om·world wavelengths
+    λ_j = 1.55 + 0.025·(j − ⌊n_om·world/2⌋) μm (so ω = 1/1.55, the oracle's comparison point,
+    is always in the job, on rank ⌊world/2⌋) and rank r takes the r-th contiguous block of
+    n_om (weak scaling: every rank gets the same amount of work, no two ranks solve the same
+    instance)."""
+    n = n_om * world
+    lam = 1.55 + 0.025 * (np.arange(n) - n // 2)
+    return (1.0 / lam)[rank * n_om:(rank + 1) * n_om]
 
 
 def ridge_epsinv(g, width: float, smoothing: str = "gpu"):
@@ -79,18 +82,21 @@ def workload(n_inst: int, rank: int = 0, world: int = 1, smoothing: str = "gpu")
     return g, probs
 
 
-def combine_ranks(dev_s: float, converged: int, e2e_s: float, dist=None, device="cpu"):
-    """Whole-job numbers from each rank's own: the slowest rank's device and end-to-end
-    times (max over ranks) and the converged modes of all ranks (sum).  Every rank calls
-    this once, at the same point, so the collectives line up."""
+def combine_ranks(times, counts, dist=None, device="cpu"):
+    """Whole-job numbers from each rank's own: every entry of `times` maxed over ranks (the
+    slowest rank's device and end-to-end seconds) and every entry of `counts` summed over
+    ranks (converged modes).  Every rank calls this once, at the same point, so the
+    collectives line up."""
+    times = [float(x) for x in times]
+    counts = [int(x) for x in counts]
     if dist is None:
-        return dev_s, converged, e2e_s
+        return times, counts
     import torch
-    t = torch.tensor([dev_s, e2e_s], dtype=torch.float64, device=device)
+    t = torch.tensor(times, dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    c = torch.tensor([converged], dtype=torch.int64, device=device)
+    c = torch.tensor(counts, dtype=torch.int64, device=device)
     dist.all_reduce(c, op=dist.ReduceOp.SUM)
-    return float(t[0].item()), int(c.item()), float(t[1].item())
+    return [float(x) for x in t.tolist()], [int(x) for x in c.tolist()]
 
 
 def sample_clocks(stop: threading.Event, out: list, index: int):
@@ -132,14 +138,13 @@ def measured_peak_hbm():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per operator apply from the committed ncu summary (null if absent)."""
-    p = os.path.join(ROOT, "profiles", "operator_apply_256x256_fp32.md")
-    try:
-        m = re.search(r"traffic_bytes_per_apply:\s*([0-9.eE+]+)", open(p).read())
-        return float(m.group(1)) if m else None
-    except Exception:
-        return None
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one roofline launch of the
+# operator apply (4 columns x 64 cells of 256x256, FP32), from an ncu capture of
+#   python bench.py --case apply --steps 3 --apply-cells 16
+# (the three passes k_row_in2 / k_col2 / k_row_out2, 413.2 MB per 16-cell apply) scaled by
+# the cells processed (x4).  A fixed per-apply constant of the current kernels: bench runs
+# are never profiled, and the figure changes only when the apply kernels change.
+APPLY_TRAFFIC_BYTES = 1.6528e9
 
 
 def smoothing_materials(n_shapes: int, nsets: int) -> np.ndarray:
@@ -216,21 +221,66 @@ def smoothing_measure(device: int, nsets: int = 64, reps: int = 10):
                            "kind": "port"}}
 
 
-def cpu_baseline(seconds_budget: float):
-    """FP64 oracle (the reference algorithm restated in NumPy/SciPy) on one mode of the
-    workload: band 0 of the 1.5 μm ridge at ω = 1/1.55, all host threads for the FFTs."""
+def cpu_baseline_and_errors(probs, results, infos):
+    """The FP64 oracle (the reference algorithm restated in NumPy/SciPy, all host threads for
+    the FFTs) as the timed CPU baseline and as the checker of the device results.
+
+    Timed: one mode of the workload, band 0 of the 1.5 μm ridge at ω = 1/1.55.  Checked:
+    that mode's k, group index n_g = 2ω/(∂ω²/∂k) and field against the device's result for
+    the same instance, and for every device result (all instances and bands of the step) the
+    residual ‖M̂h − ω²h‖ of the returned unit eigenvector under the oracle's FP64 operator,
+    with the a-posteriori bounds it gives for a Hermitian operator: eigenvalue error
+    ≤ r²/gap and so |δk| ≤ r²/(gap·∂ω²/∂k), field angle ≤ r/gap, the gap to the instance's
+    other computed bands estimated to first order in k."""
     sys.path.insert(0, ROOT)
     import oracle as O
-    from omb200 import Grid
-    g = Grid(DX, DY, NX, NY)
-    ei = ridge_epsinv(g, 1.5, "oracle")
+    og = O.Grid(DX, DY, NX, NY)
     cores = os.cpu_count() or 1
     O.maxwell.FFT_WORKERS = cores
+    from omb200 import Grid
+    ei = ridge_epsinv(Grid(DX, DY, NX, NY), 1.5, "oracle")
     t0 = time.perf_counter()
-    O.solve_k(1 / 1.55, ei, O.Grid(DX, DY, NX, NY), nev=1)
+    kr, vr = O.solve_k(1 / 1.55, ei, og, nev=1)
     dt = time.perf_counter() - t0
-    return {"value": 1.0 / dt, "unit": UNIT, "cores": cores, "kind": "port",
+    base = {"value": 1.0 / dt, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"1 converged mode (band 0, 1.5 um ridge, omega=1/1.55, 256^2) in {dt:.1f} s"}
+    # the device's result for the same instance (same ε⁻¹: the device smoothing is held
+    # bit-identical to the oracle's by the GPU tests; compared here by value)
+    errs = {"vs_oracle_solve": None}
+    for pr, (km, kv), inf in zip(probs, results, infos):
+        if abs(pr["omega"] - 1 / 1.55) < 1e-15 and np.array_equal(np.asarray(pr["eps_inv"]), ei):
+            d_ref = 2 * O.Operator(kr[0], ei, og).HMkH(vr[0])
+            ng_ref = 2 * pr["omega"] / d_ref
+            ng = 2 * pr["omega"] / inf["dw2dk"][0]
+            errs["vs_oracle_solve"] = {
+                "instance": "1.5 um ridge, omega=1/1.55, band 0",
+                "rel_err_k": abs(km[0] - kr[0]) / kr[0], "rel_err_neff": abs(km[0] - kr[0]) / kr[0],
+                "rel_err_ng": abs(ng - ng_ref) / ng_ref,
+                "field_err": float(np.sqrt(max(0.0, 1 - abs(np.vdot(vr[0], kv[0])) ** 2)))}
+            break
+    worst = {"resid": 0.0, "k_bound": 0.0, "field_bound": 0.0}
+    per = []
+    for pr, (km, kv), inf in zip(probs, results, infos):
+        w2 = pr["omega"] ** 2
+        e = np.asarray(pr["eps_inv"])
+        for b in range(len(km)):
+            r = float(np.linalg.norm(O.Operator(km[b], e, og).M(kv[b]) - w2 * kv[b]))
+            # gap at k_b to the instance's other computed bands, to first order in k:
+            # ω_j²(k_b) − ω² ≈ (k_b − k_j)·(∂ω²/∂k)_j
+            gaps = [abs(km[b] - km[j]) * inf["dw2dk"][j] for j in range(len(km)) if j != b]
+            gap = min(gaps) if gaps else w2
+            kb = r * r / gap / inf["dw2dk"][b]
+            per.append({"omega": pr["omega"], "band": b, "resid": r,
+                        "k_err_bound": kb / km[b], "field_angle_bound": r / gap})
+            worst["resid"] = max(worst["resid"], r)
+            worst["k_bound"] = max(worst["k_bound"], kb / km[b])
+            worst["field_bound"] = max(worst["field_bound"], r / gap)
+    errs.update({"results_checked": len(per), "max_resid_oracle_fp64": worst["resid"],
+                 "max_rel_err_k_bound": worst["k_bound"], "max_field_angle_bound": worst["field_bound"],
+                 "note": "residuals of the device's unit eigenvectors under the oracle's FP64 operator "
+                         "at the device's k; bounds r^2/gap (eigenvalue, then k via d omega^2/dk) "
+                         "and r/gap (field angle)"})
+    return base, errs
 
 
 def run_reference(args, rank):
@@ -275,7 +325,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--instances", type=int, default=12)
-    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=None, help="end-to-end steps (default: --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-smoothing", action="store_true")
@@ -338,26 +388,33 @@ def main():
     th.start()
     dev_s = 0.0
     kernels = 0
+    converged = 0
     for _ in range(args.steps):
         batch.run()
         st = batch.stats()
-        dev_s += st["run_seconds"]
+        dev_s += st["run_seconds"]  # CUDA events around the device run on the library stream
         kernels += st["kernel_launches"]
+        # this step's converged modes (the download is outside the device-timed region)
+        _, info = batch.results(return_info=True, raise_on_failure=False)
+        converged += int(sum(int(np.sum(i["status"] == 0)) for i in info))
     barrier()
     stop.set()
     th.join(timeout=5)
-    res, info = batch.results(return_info=True, raise_on_failure=False)
-    converged = int(sum(int(np.sum(i["status"] == 0)) for i in info))
     batch.close()
 
-    # end to end through the public C ABI call with host buffers
+    # end to end through the public C ABI call with host buffers, every step's converged
+    # modes counted from its own results
+    e2e_steps = args.e2e_steps if args.e2e_steps is not None else args.steps
     e2e_s = 0.0
-    for _ in range(args.e2e_steps):
+    e2e_conv = 0
+    res = info = None
+    for _ in range(e2e_steps):
         barrier()
         t0 = time.perf_counter()
-        omb200.solve_k_batch(probs, solver, raise_on_failure=False)
+        res, info = omb200.solve_k_batch(probs, solver, raise_on_failure=False, return_info=True)
         torch.cuda.synchronize(local)
         e2e_s += time.perf_counter() - t0
+        e2e_conv += int(sum(int(np.sum(i["status"] == 0)) for i in info))
     # byte counts of one end-to-end step from a staged run of the same batch
     b4 = omb200.Batch(probs, solver)
     b4.run()
@@ -365,9 +422,10 @@ def main():
     st4 = b4.stats()
     h2d, d2h = st4["h2d_bytes"], st4["d2h_bytes"]
     b4.close()
-    max_dev_s, converged_all, max_e2e_s = combine_ranks(dev_s, converged, e2e_s, dist, f"cuda:{local}")
-    value = converged_all * args.steps / max_dev_s
-    e2e_val = converged_all * args.e2e_steps / max_e2e_s
+    (max_dev_s, max_e2e_s), (converged_all, e2e_conv_all) = combine_ranks(
+        [dev_s, e2e_s], [converged, e2e_conv], dist, f"cuda:{local}")
+    value = converged_all / max_dev_s
+    e2e_val = e2e_conv_all / max_e2e_s
 
     out = None
     if rank == 0:
@@ -380,7 +438,7 @@ def main():
         alg = (32 * N * ncol + 24 * N) * nbatch
         peak, peak_kind = measured_peak_hbm()
         achieved = alg / t_apply / 1e9
-        traffic = profiled_traffic()
+        traffic = APPLY_TRAFFIC_BYTES
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "traffic": traffic,
                     "kernel": "operator apply M(k) (row_in + col + row_out, FP32), 4 columns x 64 cells",
@@ -400,7 +458,7 @@ def main():
                      "what": "one instance, FP64, reference band-by-band Newton loop, same kernels",
                      "seconds": pst["run_seconds"], "converged": pconv}
             pb.close()
-        cpu = None if args.no_cpu_baseline or world > 1 else cpu_baseline(30.0)
+        cpu, errors = (None, None) if args.no_cpu_baseline or world > 1 else cpu_baseline_and_errors(probs, res, info)
         smoothing = None if args.no_smoothing else smoothing_measure(local, nsets=args.smoothing_sets)
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -415,13 +473,14 @@ def main():
                                      "the others start from its device-resident eigenvectors and a first-order k",
                        "l2": "working set per step is GBs (inputs larger than L2)",
                        "parallelism": f"instances sharded, {world} rank(s)"},
-            "converged_modes_per_step": converged_all, "modes_per_step": len(probs) * NEV * world,
+            "converged_modes_per_step": converged_all / args.steps, "modes_per_step": len(probs) * NEV * world,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": int(kernels),
             "roofline": roofline,
             "plain_fp64_single": plain,
             "smoothing": smoothing,
             "cpu_baseline": cpu,
+            "errors_vs_oracle": errors,
             "clocks": clock_summary(samples),
         }
         print(json.dumps(out), flush=True)

@@ -32,11 +32,15 @@ def _rank_main(rank: int, world: int, port: int, q):
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
                             timeout=datetime.timedelta(seconds=60))
     try:
-        # every rank reports made-up per-rank timings; the reduction must give the max/sum
-        dev_s, conv, e2e_s = 1.0 + rank, 10 * (rank + 1), 2.0 + 3 * rank
-        out = bench.combine_ranks(dev_s, conv, e2e_s, dist, "cpu")
+        # every rank builds its own shard of the job exactly as bench.py does (ε⁻¹ from the
+        # oracle's smoothing here, the device smoothing on a GPU box: bit-identical)
+        g, probs = bench.workload(12, rank, world, smoothing="oracle")
+        shard = sorted((round(1 / p["omega"], 6), float(np.sum(p["eps_inv"]))) for p in probs)
+        # per-rank timings and counts; the reduction must give the max / sum over ranks
+        times, counts = [1.0 + rank, 2.0 + 3 * rank], [10 * (rank + 1), 7 + rank]
+        out = bench.combine_ranks(times, counts, dist, "cpu")
         om = bench.rank_omegas(4, rank, world)
-        q.put((rank, out, om.tolist()))
+        q.put((rank, out, om.tolist(), shard))
     finally:
         dist.barrier()
         dist.destroy_process_group()
@@ -53,15 +57,20 @@ def test_two_rank_reduction_and_sharding():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    got.sort()
-    for rank, out, _ in got:
+    got.sort(key=lambda x: x[0])
+    for rank, out, _, _ in got:
         # max of device and e2e times over ranks, sum of converged modes
-        assert out == (2.0, 30, 5.0)
-    oms = [np.array(o) for _, _, o in got]
+        assert out == ([2.0, 5.0], [30, 15])
+    oms = [np.array(o) for _, _, o, _ in got]
     assert len(set(oms[0]) & set(oms[1])) == 0                       # disjoint shards
-    assert np.allclose(np.sort(np.concatenate(oms)), bench.rank_omegas(8, 0, 1))  # cover the job
+    assert np.allclose(np.sort(np.concatenate(oms)), np.sort(bench.rank_omegas(8, 0, 1)))  # cover the job
+    shards = [set(s) for _, _, _, s in got]
+    assert all(len(s) == 12 for s in shards) and not (shards[0] & shards[1])
+    # 3 ridge widths × 8 wavelengths over the job; ω = 1/1.55 (the oracle's check) on one rank
+    assert len(shards[0] | shards[1]) == 24
+    assert sum(any(abs(lam - 1.55) < 1e-9 for lam, _ in s) for s in shards) == 1
 
 
 def test_single_rank_is_identity_and_one_shard():
-    assert bench.combine_ranks(1.5, 7, 2.5) == (1.5, 7, 2.5)
-    assert np.allclose(bench.rank_omegas(4, 0, 1), np.linspace(1 / 1.60, 1 / 1.50, 4))
+    assert bench.combine_ranks([1.5, 2.5], [7, 3]) == ([1.5, 2.5], [7, 3])
+    assert np.allclose(1 / bench.rank_omegas(4, 0, 1), [1.50, 1.525, 1.55, 1.575])

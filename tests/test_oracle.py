@@ -3,6 +3,7 @@
 
 from __future__ import annotations
 
+import os
 import numpy as np
 import pytest
 
@@ -225,3 +226,24 @@ def test_ng_gvd_matches_finite_difference():
         ngs.append(O.group_index(k2[0], v2[0], w, _epsinv_at2(eps0, deps, dd, w, w0), deps + dd * (w - w0), g))
     fd = (ngs[0] - ngs[1]) / (2 * h)
     assert gvd == pytest.approx(fd, rel=5e-7)
+
+
+def test_golden_config1_reproduced_by_oracle():
+    """The committed config-1 fixture (128² Si₃N₄ rectangle, 2 bands) is what the oracle
+    computes now: k to 1e-12, n_g to 1e-10, field probes to 1e-8 (the fixture generator
+    itself is ``tests/golden/make_golden.py``)."""
+    import json
+
+    from golden.make_golden import OMEGA, config_inputs, epsinv_checksum, field_probes
+    gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "solve_k_configs.json")))["config1"]
+    g, nev, ei = config_inputs("config1")
+    assert np.allclose(epsinv_checksum(ei), gold["epsinv_checksum"], rtol=1e-12)
+    og = O.Grid(g.Dx, g.Dy, g.Nx, g.Ny)
+    km, kv = O.solve_k(OMEGA, ei, og, nev=nev, k_tol=1e-12, eig_tol=1e-11)
+    assert np.allclose(km, gold["kmags"], rtol=1e-12, atol=0)
+    pr = field_probes(2 * g.N)
+    for b in range(nev):
+        d = 2 * O.Operator(km[b], ei, og).HMkH(kv[b])
+        assert abs(2 * OMEGA / d - gold["n_g"][b]) <= 1e-10 * gold["n_g"][b]
+        ref = np.array([complex(*p) for p in gold["field_probes"][b]])
+        assert np.max(np.abs(pr.conj() @ kv[b] - ref) / np.linalg.norm(pr, axis=1)) < 1e-8
