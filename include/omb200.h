@@ -99,6 +99,12 @@ int omb_HMkH(omb_ctx* ctx, int precision, const omb_grid* grid, double k,
 int omb_efield(omb_ctx* ctx, int precision, const omb_grid* grid, double k,
                const double* epsinv, const double* H, double* E);
 
+/* Real-space Cartesian magnetic field H(r) = fft(h1 m̂ + h2 n̂) of `ncol` columns (FP64), as
+ * ComplexF64 (3, Nx, Ny) per column, un-normalised (the same transform as E).  Replaces
+ * H⃗(ms; svecs=false) = fft(tc(H, mn)) (lib/MaxwellEigenmodes/src/fields.jl:125-126, tc at
+ * src/maxwell.jl:184-186); builds the learned warm start's training targets. */
+int omb_hfield(omb_ctx* ctx, const omb_grid* grid, double k, int ncol, const double* H, double* Hr);
+
 /* Allocation-free FP32 Hout = M̂(k) Hin on caller-owned device memory.  No counterpart in
  * the reference: it exists for callers that cannot allocate device memory when they need
  * the operator — host frameworks that own the whole device pool and forbid foreign
@@ -139,6 +145,11 @@ int omb_apply_M_noalloc(int32_t Nx, int32_t Ny, double Dx, double Dy, double k, 
                             solved first and the others start from its eigenvectors and
                             per-band k — the batched form of the reference's per-cell warm
                             start (lib/EigenmodeExpansion/src/eme.jl:58-72)             */
+#define OMB_WARM_LEARNED 3 /* instances without guesses of their own on 128² or 256² grids start
+                            from the learned network attached to the context
+                            (omb_ctx_set_warmstart): its (Hx, Hy) fields of bands 0..3 projected
+                            on the plane waves at k = n_eff·ω, and those k as Newton starts;
+                            the solve itself is unchanged (same tolerances)            */
 
 typedef struct {
   double k_tol;           /* Newton tolerance on |Δk|                       (1e-8) */
@@ -327,6 +338,52 @@ int omb_smooth_scalar(omb_smoothing_plan* plan, const double* vals, int32_t nmat
 
 /* Waits for the device, then frees the plan. */
 int omb_smoothing_plan_destroy(omb_smoothing_plan* plan);
+
+/* ---------------------------------------------------------------------------------
+ * Learned warm start (no reference counterpart: the reference starts every solve from
+ * random blocks or the caller's Hguess, lib/MaxwellEigenmodes/src/solve.jl:201-210).
+ * A six-layer BF16 convolutional network on the tensor cores maps the ε⁻¹ map and ω of a
+ * 128² or 256² cross-section to initial (Hx, Hy) fields and effective indices of the four
+ * lowest bands.  Device pointers throughout; calls are ordered on the context's stream.
+ * --------------------------------------------------------------------------------- */
+
+typedef struct omb_warmstart omb_warmstart;
+
+/* The network's matrix product on the tensor cores (tcgen05.mma, TMA-loaded operands, FP32
+ * accumulation in tensor memory): D[M×N] = A[M×K]·B[N×K]ᵀ (+ bias[N], then ReLU if relu),
+ * A and B row-major BF16 device matrices (K a multiple of 64, 16-byte aligned), D row-major
+ * with leading dimension ldd.  epi: 0 store FP32, 1 store BF16, 2 add atomically into FP32 D
+ * (needed when splits > 1, the K range being cut over `splits` CTAs per tile).  Waits for
+ * the context's stream. */
+int omb_tc_gemm(omb_ctx* ctx, const void* d_A, const void* d_B, void* d_D, int32_t M, int32_t N, int32_t K,
+                int64_t ldd, const float* d_bias, int32_t relu, int32_t epi, int32_t splits);
+
+/* Network with He-initialised weights (seeded) and buffers for up to batch_cap images. */
+int omb_warmstart_create(omb_ctx* ctx, int32_t batch_cap, uint64_t seed, omb_warmstart** out);
+int omb_warmstart_destroy(omb_warmstart* ws);
+/* Attach (or, with NULL, detach) the network OMB_WARM_LEARNED uses on this context; the
+ * context does not own it (destroying the network detaches it). */
+int omb_ctx_set_warmstart(omb_ctx* ctx, omb_warmstart* ws);
+/* Number of parameters; get/set exchange them as FP32, layer by layer: the weights as
+ * [cout × 9·cin] row-major (column = tap·cin + c, taps row-major over the 3×3 window),
+ * then the cout biases. */
+int64_t omb_warmstart_num_params(void);
+int omb_warmstart_get_params(omb_warmstart* ws, float* host);
+int omb_warmstart_set_params(omb_warmstart* ws, const float* host);
+/* One input image (128×128×8 BF16, NHWC) from a device ε⁻¹ (3, 3, Nx, Ny) Float64 array of a
+ * 128² or 256² grid and ω, on `stream` (NULL: the context's stream). */
+int omb_warmstart_features(omb_warmstart* ws, const double* d_epsinv, int32_t Nx, int32_t Ny, double omega,
+                           void* d_feat, void* stream);
+/* Network output for `batch` images: d_out [batch·64·64 × 16] FP32, channels 2b, 2b+1 the
+ * (Hx, Hy) field of band b, 8+b its n_eff map (the band's n_eff is its mean). */
+int omb_warmstart_forward(omb_warmstart* ws, const void* d_feat, int32_t batch, float* d_out);
+/* One training step on `batch` images with targets d_tfield [batch·64·64 × 8] FP32 (the
+ * bands' real-space (Hx, Hy), unit RMS per band) and d_tneff [batch × 4]: forward, loss,
+ * backward and (update != 0) an Adam step with learning rate lr.  *loss (host, may be NULL)
+ * receives the batch loss; grads (host, may be NULL) the parameter gradients in the
+ * get_params layout. */
+int omb_warmstart_train_step(omb_warmstart* ws, const void* d_feat, const float* d_tfield, const float* d_tneff,
+                             int32_t batch, float lr, int32_t update, float* loss, float* grads);
 
 #ifdef __cplusplus
 }

@@ -259,6 +259,45 @@ int omb_profile_apply(omb_ctx* ctx, int op, int precision, const omb_grid* grid,
                                     : run_profile<float>(ctx, op, P, k, ncol, nbatch, reps, seconds);
 }
 
+int omb_hfield(omb_ctx* ctx, const omb_grid* grid, double k, int ncol, const double* H, double* Hr) {
+  int rc = check_common(ctx, OMB_PREC_FP64, k);
+  if (rc) return rc;
+  rc = check_grid(grid);
+  if (rc) return rc;
+  if (!H || !Hr || ncol <= 0) return fail(OMB_ERR_INVALID_ARG, "need ncol > 0 and non-NULL H, Hr");
+  const size_t N = (size_t)grid->Nx * grid->Ny, n = 2 * N * (size_t)ncol;
+  cudaStream_t st = ctx->stream;
+  DevBuf<double2> hin, scr;
+  OMB_CU(hin.alloc(n, st));
+  OMB_CU(cudaMemcpyAsync(hin.p, H, n * sizeof(double2), cudaMemcpyHostToDevice, st));
+  OMB_CU(scr.alloc(3 * N * (size_t)ncol, st));
+  DevBuf<double> kd;
+  OMB_CU(kd.alloc(1, st));
+  OMB_CU(cudaMemcpyAsync(kd.p, &k, sizeof(double), cudaMemcpyHostToDevice, st));
+  OpUnit<double> u{};
+  u.in = hin.p; u.scr = scr.p; u.k_dev = kd.p;
+  u.in_cs = (long long)(2 * N); u.scr_cs = (long long)(3 * N); u.ncol = ncol;
+  u.Nx = grid->Nx; u.Ny = grid->Ny;
+  u.inv_dx = 1.0 / grid->Dx; u.inv_dy = 1.0 / grid->Dy;
+  u.part_stride = row_blocks(grid->Nx, grid->Ny);
+  DevBuf<OpUnit<double>> du;
+  OMB_CU(du.alloc(1, st));
+  OMB_CU(cudaMemcpyAsync(du.p, &u, sizeof(u), cudaMemcpyHostToDevice, st));
+  OMB_CU(launch_op<double>(OP_HFIELD, du.p, 1, grid->Nx, grid->Ny, ncol, ctx->tw, st));
+  std::vector<double2> h(3 * N * (size_t)ncol);
+  OMB_CU(cudaMemcpyAsync(h.data(), scr.p, h.size() * sizeof(double2), cudaMemcpyDeviceToHost, st));
+  OMB_CU(cudaStreamSynchronize(st));
+  // planar [c][p] per column → interleaved (3, Nx, Ny) per column
+  for (int j = 0; j < ncol; ++j)
+    for (size_t p = 0; p < N; ++p)
+      for (int c = 0; c < 3; ++c) {
+        const double2 v = h[(size_t)j * 3 * N + c * N + p];
+        Hr[2 * (3 * N * j + 3 * p + c)] = v.x;
+        Hr[2 * (3 * N * j + 3 * p + c) + 1] = v.y;
+      }
+  return OMB_OK;
+}
+
 int omb_efield(omb_ctx* ctx, int precision, const omb_grid* grid, double k, const double* epsinv,
                const double* H, double* E) {
   int rc = check_common(ctx, precision, k);

@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "warmstart.h"
 
 struct omb_batch {
   struct Who { int inst, band0, eng, track; };  // a track's instance, first band, engine, index
@@ -20,6 +21,8 @@ struct omb_batch {
   bool canon = true;
   int warm = OMB_WARM_NONE;
   std::vector<std::unique_ptr<omb::Engine>> engines;  // one per stage
+  omb::DevBuf<double2> learned;                      // learned starting columns (OMB_WARM_LEARNED)
+  int learned_instances = 0;
   std::vector<Who> who;
   int64_t h2d = 0, d2h = 0;
   double run_seconds = 0;
@@ -50,8 +53,10 @@ static int options_from(const omb_options* o, SolveOptions& so) {
   so.seed = o->seed;
   if (o->guard_bands < 0 || o->guard_bands > 4) return fail(OMB_ERR_INVALID_ARG, "guard_bands must be in 0..4");
   so.guard = o->guard_bands;
-  if (o->warm_start != OMB_WARM_NONE && o->warm_start != OMB_WARM_SWEEP && o->warm_start != OMB_WARM_CELLS)
-    return fail(OMB_ERR_INVALID_ARG, "warm_start must be OMB_WARM_NONE, OMB_WARM_SWEEP or OMB_WARM_CELLS");
+  if (o->warm_start != OMB_WARM_NONE && o->warm_start != OMB_WARM_SWEEP && o->warm_start != OMB_WARM_CELLS &&
+      o->warm_start != OMB_WARM_LEARNED)
+    return fail(OMB_ERR_INVALID_ARG,
+                "warm_start must be OMB_WARM_NONE, OMB_WARM_SWEEP, OMB_WARM_CELLS or OMB_WARM_LEARNED");
   return OMB_OK;
 }
 
@@ -241,10 +246,55 @@ int omb_batch_run(omb_batch* b) {
   OMB_CU(cudaEventCreate(&e0));
   OMB_CU(cudaEventCreate(&e1));
   OMB_CU(cudaEventRecord(e0, ctx->stream));
+  // learned warm start: the network's starting block and per-band k for every instance
+  // without guesses of its own on a grid the network reads
+  std::vector<int> learned_of(n_inst, -1);
+  std::vector<size_t> loff;
+  std::vector<std::array<double, 4>> lk;
+  b->learned_instances = 0;
+  if (b->warm == OMB_WARM_LEARNED) {
+    if (!ctx->ws) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return fail(OMB_ERR_INVALID_ARG, "OMB_WARM_LEARNED needs a network attached with omb_ctx_set_warmstart");
+    }
+    std::vector<const Problem*> lp;
+    std::vector<double> lw;
+    for (int i = 0; i < n_inst; ++i) {
+      const omb_instance& I = b->inst[i];
+      const Problem& P = b->probs[b->pidx[i]];
+      if (I.nguess > 0 || !b->kbands[i].empty()) continue;
+      if (!((P.Nx == 128 && P.Ny == 128) || (P.Nx == 256 && P.Ny == 256))) continue;
+      learned_of[i] = (int)lp.size();
+      lp.push_back(&P);
+      lw.push_back(I.omega);
+    }
+    const int lrc = ws_guesses(ctx->ws, lp, lw, b->learned, loff, lk);
+    if (lrc) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return lrc;
+    }
+    b->learned_instances = (int)lp.size();
+  }
   // stage 1: every instance without a neighbour to start from
   std::vector<TrackSpec> tracks;
-  for (int i = 0; i < n_inst; ++i)
-    if (anchor[i] < 0) add_tracks(b, i, own_k0(b, i), nullptr, 0, 0, tracks);
+  for (int i = 0; i < n_inst; ++i) {
+    if (anchor[i] >= 0) continue;
+    if (learned_of[i] >= 0) {
+      const int l = learned_of[i];
+      const size_t n2 = 2 * b->probs[b->pidx[i]].N();
+      std::vector<double> k0 = own_k0(b, i);
+      const double2* gdev[4];
+      for (int j = 0; j < 4; ++j) {
+        if (j < (int)k0.size()) k0[j] = lk[l][j];
+        gdev[j] = b->learned.p + loff[l] + (size_t)j * n2;
+      }
+      add_tracks(b, i, k0, gdev, 4, 0, tracks);
+    } else {
+      add_tracks(b, i, own_k0(b, i), nullptr, 0, 0, tracks);
+    }
+  }
   b->engines.emplace_back(new Engine(ctx, &b->probs, tracks, b->so));
   int rc = b->engines[0]->run();
   // stage 2: the rest of each sweep group, from its anchor's eigenvectors and k

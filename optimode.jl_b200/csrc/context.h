@@ -20,6 +20,8 @@ struct omb_ctx {
   size_t pinned_bytes = 0;
   // limit of every bounded wait in the streaming kernels (omb_ctx_set_wait_limit)
   uint64_t wait_ns = 1000000000ull;
+  // learned warm-start network used by OMB_WARM_LEARNED (not owned)
+  struct omb_warmstart* ws = nullptr;
 };
 
 namespace omb {

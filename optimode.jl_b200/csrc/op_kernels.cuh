@@ -44,7 +44,7 @@ template <typename T> struct OpUnit {
   T inv_dx, inv_dy;
 };
 
-enum RowIn : int { RI_KXTC = 0, RI_KXINV = 1, RI_ZXTC = 2, RI_LOAD3 = 3 };
+enum RowIn : int { RI_KXTC = 0, RI_KXINV = 1, RI_ZXTC = 2, RI_LOAD3 = 3, RI_HCART = 4 };
 enum RowOut : int { RO_KXCT = 0, RO_KXINVCT = 1, RO_STORE3 = 2, RO_KXCT_DOT = 3 };
 enum ColStep : int { CS_NONE = 0, CS_FWD = 1, CS_INV = 2 };
 enum ColPw : int { PW_NONE = 0, PW_EPS = 1, PW_EAVE = 2, PW_EPS9 = 3 };
@@ -112,6 +112,10 @@ __global__ void __launch_bounds__(NT) k_row_in(const OpUnit<T>* __restrict__ uni
           d0 = (h1 * b.nx - h2 * b.mx) * s_;
           d1 = (h1 * b.ny - h2 * b.my) * s_;
           d2 = h2 * (-b.mz * s_);
+        } else if constexpr (MODE == RI_HCART) {  // Cartesian H = h1 m̂ + h2 n̂
+          d0 = h1 * b.mx + h2 * b.nx;
+          d1 = h1 * b.my + h2 * b.ny;
+          d2 = h1 * b.mz;
         } else {  // RI_ZXTC: ẑ × (h1 m̂ + h2 n̂)
           d0 = (h1 * b.my + h2 * b.ny) * T(-1);
           d1 = h1 * b.mx + h2 * b.nx;

@@ -89,6 +89,10 @@ __device__ __forceinline__ void prologue_at(const OpUnit<T>& U, const cplx<T>* _
       d0 = (h1 * b.nx - h2 * b.mx) * s_;
       d1 = (h1 * b.ny - h2 * b.my) * s_;
       d2 = h2 * (-b.mz * s_);
+    } else if constexpr (MODE == RI_HCART) {  // Cartesian H = h1 m̂ + h2 n̂
+      d0 = h1 * b.mx + h2 * b.nx;
+      d1 = h1 * b.my + h2 * b.ny;
+      d2 = h1 * b.mz;
     } else {  // RI_ZXTC: ẑ × (h1 m̂ + h2 n̂)
       d0 = (h1 * b.my + h2 * b.ny) * T(-1);
       d1 = h1 * b.mx + h2 * b.nx;

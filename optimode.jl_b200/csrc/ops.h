@@ -14,6 +14,8 @@ enum OpKind : int {
   OP_H2D = 4,     // scratch ← fft2(kx_tc Hin)                (_H2d!)
   OP_D2E = 5,     // out (planar 3N) ← bfft2(ε⁻¹·scratch)     (_d2ẽ!)
   OP_MDOT = 6,    // like OP_M but reduces ⟨Hin, M̂ Hin⟩ partials instead of storing
+  OP_HFIELD = 7,  // scratch ← fft2(h1 m̂ + h2 n̂): the Cartesian H field in real space
+  OP_R2G = 8,     // scratch ← bfft2(planar 3-component in): real space back to plane waves
 };
 
 // Twiddle tables exp(-2πi m/L) for every supported length, per precision.

@@ -44,6 +44,8 @@ static cudaError_t row_in_nx(int mode, const OpUnit<T>* u, int nunits, int Ny, i
       case RI_KXTC: return launch_pass<T>(k_row_in2<T, NX, RI_KXTC, false>, g, NT, sm, st, u, tw);
       case RI_KXINV: return launch_pass<T>(k_row_in2<T, NX, RI_KXINV, true>, g, NT, sm, st, u, tw);
       case RI_ZXTC: return launch_pass<T>(k_row_in2<T, NX, RI_ZXTC, false>, g, NT, sm, st, u, tw);
+      case RI_HCART: return launch_pass<T>(k_row_in2<T, NX, RI_HCART, false>, g, NT, sm, st, u, tw);
+      case RI_LOAD3: return launch_pass<T>(k_row_in2<T, NX, RI_LOAD3, true>, g, NT, sm, st, u, tw);
       default: return cudaErrorInvalidValue;
     }
   } else {
@@ -54,6 +56,8 @@ static cudaError_t row_in_nx(int mode, const OpUnit<T>* u, int nunits, int Ny, i
       case RI_KXTC: return launch_pass<T>(k_row_in<T, NX, ROWS, NT_ROW, RI_KXTC, false>, g, NT_ROW, sm, st, u, tw);
       case RI_KXINV: return launch_pass<T>(k_row_in<T, NX, ROWS, NT_ROW, RI_KXINV, true>, g, NT_ROW, sm, st, u, tw);
       case RI_ZXTC: return launch_pass<T>(k_row_in<T, NX, ROWS, NT_ROW, RI_ZXTC, false>, g, NT_ROW, sm, st, u, tw);
+      case RI_HCART: return launch_pass<T>(k_row_in<T, NX, ROWS, NT_ROW, RI_HCART, false>, g, NT_ROW, sm, st, u, tw);
+      case RI_LOAD3: return launch_pass<T>(k_row_in<T, NX, ROWS, NT_ROW, RI_LOAD3, true>, g, NT_ROW, sm, st, u, tw);
       default: return cudaErrorInvalidValue;
     }
   }
@@ -88,7 +92,7 @@ static cudaError_t row_out_nx(int mode, const OpUnit<T>* u, int nunits, int Ny, 
 }
 
 // column-pass modes
-enum ColMode : int { CM_M = 0, CM_P = 1, CM_E = 2, CM_FWD = 3, CM_EPSINV = 4 };
+enum ColMode : int { CM_M = 0, CM_P = 1, CM_E = 2, CM_FWD = 3, CM_EPSINV = 4, CM_BWD = 5 };
 
 template <typename T, int NY>
 static cudaError_t col_ny(int mode, const OpUnit<T>* u, int nunits, int Nx, int maxcol,
@@ -103,6 +107,7 @@ static cudaError_t col_ny(int mode, const OpUnit<T>* u, int nunits, int Nx, int 
       case CM_E: return launch_pass<T>(k_col2<T, NY, CS_FWD, PW_EPS, CS_NONE>, g, NT, sm, st, u, tw);
       case CM_FWD: return launch_pass<T>(k_col2<T, NY, CS_FWD, PW_NONE, CS_NONE>, g, NT, sm, st, u, tw);
       case CM_EPSINV: return launch_pass<T>(k_col2<T, NY, CS_NONE, PW_EPS, CS_INV>, g, NT, sm, st, u, tw);
+      case CM_BWD: return launch_pass<T>(k_col2<T, NY, CS_INV, PW_NONE, CS_NONE>, g, NT, sm, st, u, tw);
       default: return cudaErrorInvalidValue;
     }
   } else {
@@ -115,6 +120,7 @@ static cudaError_t col_ny(int mode, const OpUnit<T>* u, int nunits, int Nx, int 
       case CM_E: return launch_pass<T>(k_col<T, NY, TX, NT_COL, CS_FWD, PW_EPS, CS_NONE>, g, NT_COL, sm, st, u, tw);
       case CM_FWD: return launch_pass<T>(k_col<T, NY, TX, NT_COL, CS_FWD, PW_NONE, CS_NONE>, g, NT_COL, sm, st, u, tw);
       case CM_EPSINV: return launch_pass<T>(k_col<T, NY, TX, NT_COL, CS_NONE, PW_EPS, CS_INV>, g, NT_COL, sm, st, u, tw);
+      case CM_BWD: return launch_pass<T>(k_col<T, NY, TX, NT_COL, CS_INV, PW_NONE, CS_NONE>, g, NT_COL, sm, st, u, tw);
       default: return cudaErrorInvalidValue;
     }
   }
@@ -187,6 +193,12 @@ cudaError_t launch_op(OpKind op, const OpUnit<T>* u, int nunits, int Nx, int Ny,
     case OP_D2E:
       OMB_TRY(col<T>(CM_EPSINV, u, nunits, Nx, Ny, maxcol, t, st));
       return row_out<T>(RO_STORE3, u, nunits, Nx, Ny, maxcol, t, st);
+    case OP_HFIELD:
+      OMB_TRY(row_in<T>(RI_HCART, u, nunits, Nx, Ny, maxcol, t, st));
+      return col<T>(CM_FWD, u, nunits, Nx, Ny, maxcol, t, st);
+    case OP_R2G:
+      OMB_TRY(row_in<T>(RI_LOAD3, u, nunits, Nx, Ny, maxcol, t, st));
+      return col<T>(CM_BWD, u, nunits, Nx, Ny, maxcol, t, st);
     default:
       return cudaErrorInvalidValue;
   }

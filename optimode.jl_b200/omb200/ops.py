@@ -82,6 +82,17 @@ def E_field(k, epsinv, grid, H, precision="fp64", device=0):
     return out
 
 
+def H_field(k, grid, H, device=0):
+    """Real-space Cartesian H = fft(h1 m̂ + h2 n̂) per column (``omb_hfield``), shaped
+    ``(ncol, 3·Nx·Ny)`` (each row a flat ``(3, Nx, Ny)`` column-major field), FP64."""
+    lib = _lib.load()
+    ctx = _lib.context(device)
+    B, ncol, vec = block_host(H, 2 * grid.N)
+    out = np.empty((ncol, 3 * grid.N), dtype=np.complex128)
+    _lib.check(lib.omb_hfield(ctx.handle, ctypes.byref(grid.c()), float(k), int(ncol), _dptr(B), _dptr(out)))
+    return out[0] if vec else out
+
+
 def profile_apply(op: str, k, epsinv, grid: Grid, ncol: int, nbatch: int, reps: int = 20,
                   precision: str = "fp32", device: int = 0) -> float:
     """Mean device seconds of one application of ``op`` ("M" or "P") to ``ncol`` columns on

@@ -16,7 +16,7 @@ from .ops import epsinv_host
 
 _PRECOND = {"mpb": 1, "diag": 2}
 _NEWTON = {"inner": 0, "outer": 1}
-_WARM = {"none": 0, "sweep": 1, "cells": 2}
+_WARM = {"none": 0, "sweep": 1, "cells": 2, "learned": 3}
 
 
 @dataclasses.dataclass(frozen=True)
@@ -34,7 +34,10 @@ class B200Solver:
       the group's mean ω is solved first and the others start from its eigenvectors and a
       first-order k per band (``OMB_WARM_SWEEP``); ``"cells"``: problems with the same ω
       and grid form a stack of cross-sections (eigenmode expansion); the middle one is solved
-      first and the others start from its eigenvectors and k (``OMB_WARM_CELLS``).
+      first and the others start from its eigenvectors and k (``OMB_WARM_CELLS``);
+      ``"learned"``: problems on 128² or 256² grids start from the learned network's fields and
+      effective indices (``OMB_WARM_LEARNED``; the trained parameters committed with the
+      package, or a ``omb200.warmstart.WarmStartNet`` attached by the caller).
     """
 
     precision: str = "mixed"
@@ -88,6 +91,9 @@ class Batch:
         self.solver = solver or B200Solver()
         self._lib = _lib.load()
         self._ctx = _lib.context(self.solver.device)
+        if self.solver.warm_start == "learned":
+            from .warmstart import ensure_attached
+            ensure_attached(self.solver.device)
         insts, results, keep, outs = _marshal(problems)
         self._insts, self._results, self._keep, self._outs = insts, results, keep, outs
         opt = self.solver.options(k_tol, eig_tol, max_eigsolves, maxiter, canonicalize)
@@ -192,6 +198,9 @@ def solve_k_batch(problems, solver: B200Solver | None = None, k_tol=1e-8, eig_to
     solver = solver or B200Solver()
     lib = _lib.load()
     ctx = _lib.context(solver.device)
+    if solver.warm_start == "learned":
+        from .warmstart import ensure_attached
+        ensure_attached(solver.device)
     insts, results, keep, outs = _marshal(problems)
     opt = solver.options(k_tol, eig_tol, max_eigsolves, maxiter, canonicalize)
     rc = lib.omb_solve_k(ctx.handle, insts, len(problems), ctypes.byref(opt), results)
