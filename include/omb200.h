@@ -266,6 +266,16 @@ int omb_batch_destroy(omb_batch* b);
 int omb_profile_apply(omb_ctx* ctx, int op, int precision, const omb_grid* grid, double k,
                       const double* epsinv, int ncol, int nbatch, int reps, double* seconds);
 
+/* The eigensolver's Gram products on caller blocks: G = ZᴴZ and S = ZᴴAZ of `n` columns
+ * (≤ 36) of n2 complex rows (host ComplexF64, column after column), computed by the same
+ * streaming kernel as a LOBPCG iteration (n2 even, as every solver vector is) in FP32
+ * (operands rounded to FP32, products summed
+ * per tile and the tile sums compensated by two-sum) or FP64.  G and S receive n×n ComplexF64,
+ * column-major.  No reference counterpart (accuracy check of the FP32 reductions; the
+ * reference's products are BLAS calls, ME/src/solvers/dftk.jl:129-132). */
+int omb_gram_blocks(omb_ctx* ctx, int precision, int64_t n2, int32_t n, const double* Z, const double* AZ,
+                    double* G, double* S);
+
 /* ---------------------------------------------------------------------------------
  * Kottke sub-pixel smoothing (the solver's input generator, lib/DielectricSmoothing)
  * --------------------------------------------------------------------------------- */

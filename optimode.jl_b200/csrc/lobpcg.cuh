@@ -141,7 +141,8 @@ __global__ void k_live_prefix(TrackState* const* __restrict__ states, const long
 // so their partial sums meet in a shuffle reduction (FP64) before the atomics.
 template <typename T> struct GramCfg {
   static constexpr int NCW = 15;                                 // consumer warps
-  static constexpr int NT = (NCW + 1) * 32;                      // + the producer warp (16 warps: 128 regs)
+  static constexpr int NT = (NCW + 1) * 32;                      // + the producer warp (16 warps: 128 regs;
+                                                                 // FP32 keeps its compensation terms in local memory)
   static constexpr int PAD = 16 / (int)sizeof(cplx<T>);          // column pad: 16 bytes
   // Z columns at [0, n), AZ columns at [n4, n4 + n) with n4 = 4·⌈n/4⌉: the 4×4 blocks read
   // up to column 2·n4 − 1, so a stage holds 2·4·⌈nmax/4⌉ columns of R + PAD elements
@@ -171,6 +172,15 @@ __device__ __forceinline__ void gram_item(int q, int nblk, int nb4, int& which, 
   bi = 0;
   while (r >= nb4 - bi) { r -= nb4 - bi; ++bi; }
   bj = bi + r;
+}
+
+// s + lo += x with the rounding error of the FP32 addition carried in lo (two-sum: Knuth,
+// TAOCP vol. 2, 4.2.2; the error of s + x is exact in FP32).
+__device__ __forceinline__ void two_sum_acc(float& s, float& lo, float x) {
+  const float t = s + x;
+  const float xp = t - s, sp = t - xp;
+  lo += (s - sp) + (x - xp);
+  s = t;
 }
 
 template <typename T>
@@ -237,7 +247,11 @@ __global__ void __launch_bounds__(GramCfg<T>::NT, 1)
   int q = 0;
   uint32_t ph = 0;
   bool failed = false;
-  C acc[4][4];
+  // FP32: each tile's rows are summed into t, and the tile sums into the compensated pair
+  // (acc, lo) by two-sum (Knuth), so the rounding error of the track's sum stays at the
+  // FP32 level of one tile instead of growing with the number of tiles; FP64 sums directly.
+  constexpr bool COMP = sizeof(T) == 4;
+  C acc[4][4], lo[COMP ? 4 : 1][COMP ? 4 : 1];
   int cur = -1, items = 0, split = 1, nblk = 0, nb4 = 1, n = 0, item = 0, sub = 0, which = 0, bi = 0, bj = 0;
   bool active = false;
   for (; w.valid(); w.next()) {
@@ -258,6 +272,12 @@ __global__ void __launch_bounds__(GramCfg<T>::NT, 1)
       for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j] = mk<C>(0, 0);
+      if constexpr (COMP) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) lo[i][j] = mk<C>(0, 0);
+      }
     }
     const int rows = (int)min((long long)R, d.n2 - w.row0());
     bool ok = failed ? false : mbar_wait(&full[q], ph, wait_ns);
@@ -268,18 +288,46 @@ __global__ void __launch_bounds__(GramCfg<T>::NT, 1)
         const C* st = stage0 + (size_t)q * sel;
         const C* za = st + (size_t)(4 * bi) * CS;
         const C* zb = st + (size_t)((which ? Cfg::n4(n) : 0) + 4 * bj) * CS;
-#pragma unroll 2
-        for (int r = sub; r < rows; r += split) {
-          C a[4], b[4];
-#pragma unroll
-          for (int i = 0; i < 4; ++i) { a[i] = za[i * CS + r]; b[i] = zb[i * CS + r]; }
+        if constexpr (COMP) {
+          C t[4][4];
 #pragma unroll
           for (int i = 0; i < 4; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {  // conj(a)·b
-              acc[i][j].x += a[i].x * b[j].x + a[i].y * b[j].y;
-              acc[i][j].y += a[i].x * b[j].y - a[i].y * b[j].x;
+            for (int j = 0; j < 4; ++j) t[i][j] = mk<C>(0, 0);
+#pragma unroll 2
+          for (int r = sub; r < rows; r += split) {
+            C a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) { a[i] = za[i * CS + r]; b[i] = zb[i * CS + r]; }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+              for (int j = 0; j < 4; ++j) {  // conj(a)·b
+                t[i][j].x += a[i].x * b[j].x + a[i].y * b[j].y;
+                t[i][j].y += a[i].x * b[j].y - a[i].y * b[j].x;
+              }
+          }
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              two_sum_acc(acc[i][j].x, lo[i][j].x, t[i][j].x);
+              two_sum_acc(acc[i][j].y, lo[i][j].y, t[i][j].y);
             }
+        } else {
+#pragma unroll 2
+          for (int r = sub; r < rows; r += split) {
+            C a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) { a[i] = za[i * CS + r]; b[i] = zb[i * CS + r]; }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+              for (int j = 0; j < 4; ++j) {  // conj(a)·b
+                acc[i][j].x += a[i].x * b[j].x + a[i].y * b[j].y;
+                acc[i][j].y += a[i].x * b[j].y - a[i].y * b[j].x;
+              }
+          }
         }
       }
       __syncwarp();
@@ -294,8 +342,10 @@ __global__ void __launch_bounds__(GramCfg<T>::NT, 1)
         for (int i = 0; i < 4; ++i)
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
-            atomicAdd(&red[item * 16 + i * 4 + j].x, (double)acc[i][j].x);
-            atomicAdd(&red[item * 16 + i * 4 + j].y, (double)acc[i][j].y);
+            double vx = (double)acc[i][j].x, vy = (double)acc[i][j].y;
+            if constexpr (COMP) { vx += (double)lo[i][j].x; vy += (double)lo[i][j].y; }
+            atomicAdd(&red[item * 16 + i * 4 + j].x, vx);
+            atomicAdd(&red[item * 16 + i * 4 + j].y, vy);
           }
       }
       bar_sync_count(1, NC);

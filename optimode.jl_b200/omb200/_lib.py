@@ -27,7 +27,7 @@ OPS = {"M": 0, "P": 1, "P_diag": 2}
 #: every symbol ``include/omb200.h`` declares (checked by the CPU test suite)
 EXPORTS = (
     "omb_version", "omb_fft_size_supported", "omb_last_error", "omb_ctx_create",
-    "omb_ctx_destroy", "omb_apply", "omb_HMkH", "omb_efield", "omb_hfield",
+    "omb_ctx_destroy", "omb_apply", "omb_HMkH", "omb_efield", "omb_hfield", "omb_gram_blocks",
 )
 
 
@@ -73,6 +73,7 @@ def load():
                                         _dp, _dp]),
             "omb_efield": (ctypes.c_int, [vp, ctypes.c_int, gp, ctypes.c_double, _dp, _dp, _dp]),
             "omb_hfield": (ctypes.c_int, [vp, gp, ctypes.c_double, ctypes.c_int, _dp, _dp]),
+            "omb_gram_blocks": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int64, ctypes.c_int32, _dp, _dp, _dp, _dp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)

@@ -104,3 +104,18 @@ def profile_apply(op: str, k, epsinv, grid: Grid, ncol: int, nbatch: int, reps: 
     _lib.check(lib.omb_profile_apply(ctx.handle, _lib.OPS[op], _lib.PREC[precision], ctypes.byref(grid.c()),
                                      float(k), _dptr(e), int(ncol), int(nbatch), int(reps), _dptr(out)))
     return float(out[0])
+
+
+def gram_blocks(Z, AZ, precision: str = "fp32", device: int = 0):
+    """(G, S) = (ZᴴZ, ZᴴAZ) from the eigensolver's streaming Gram kernel (``omb_gram_blocks``)
+    for complex blocks Z, AZ of shape (n2, n)."""
+    lib = _lib.load()
+    ctx = _lib.context(device)
+    Z = np.asfortranarray(np.asarray(Z, dtype=np.complex128))
+    AZ = np.asfortranarray(np.asarray(AZ, dtype=np.complex128))
+    n2, n = Z.shape
+    G = np.zeros((n, n), dtype=np.complex128, order="F")
+    S = np.zeros((n, n), dtype=np.complex128, order="F")
+    _lib.check(lib.omb_gram_blocks(ctx.handle, _lib.PREC[precision], int(n2), int(n), _dptr(Z), _dptr(AZ),
+                                   _dptr(G), _dptr(S)))
+    return G, S

@@ -145,6 +145,57 @@ def train(F, TF, TN, epochs: int, batch: int = 32, lr: float = 1e-3, seed: int =
     return net, hist, time.perf_counter() - t0
 
 
+def heldout_problems(n: int, seed: int, ngrid: int = NGRID, device: int = 0):
+    """n seeded held-out cross-sections (the training distribution, another seed)."""
+    grid = Grid(CELL[0], CELL[1], ngrid, ngrid)
+    rng = np.random.default_rng(seed)
+    probs = []
+    for _ in range(n):
+        shapes, bg, desc = random_ridge(rng, grid)
+        om = float(rng.uniform(0.5, 1.0))
+        probs.append({"omega": om, "eps_inv": G.smooth_epsinv(shapes, bg, grid, device=device), "grid": grid,
+                      "nev": 4})
+    return probs
+
+
+def evaluate(probs, device: int = 0, d_omega: float = 0.01):
+    """Iterations to the 1e-8 tolerance and device seconds of one batched solve of `probs` from
+    three starts: random (``none``), the learned network (``learned``), and the previous
+    frequency's converged modes (``previous_omega``: each problem solved first at ω − d_omega,
+    untimed, then at ω from those eigenvectors and k·ω/ω_prev).  Every arm is checked to
+    converge every band, and the arms' k to agree."""
+    import omb200
+    out = {}
+    ks = {}
+
+    def run(arm, problems, solver):
+        b = omb200.Batch(problems, solver)
+        b.run()
+        st = b.stats()
+        res, info = b.results(return_info=True, raise_on_failure=False)
+        b.close()
+        conv = int(sum(int(np.sum(i["status"] == 0)) for i in info))
+        its = [int(x) for i in info for x in i["iterations"]]
+        out[arm] = {"device_seconds": st["run_seconds"], "converged": conv, "modes": 4 * len(problems),
+                    "iterations_total": int(sum(its)), "iterations_mean": float(np.mean(its)),
+                    "iterations_max": int(max(its))}
+        ks[arm] = np.array([r[0] for r in res])
+        return res
+
+    run("none", probs, omb200.B200Solver(precision="mixed", warm_start="none", device=device))
+    run("learned", probs, omb200.B200Solver(precision="mixed", warm_start="learned", device=device))
+    prev = [{**p, "omega": p["omega"] - d_omega} for p in probs]
+    pres = omb200.solve_k_batch(prev, omb200.B200Solver(precision="mixed", device=device), raise_on_failure=False)
+    warm = [{**p, "Hguess": np.stack(kv, axis=1), "kguess_bands": km * p["omega"] / q["omega"]}
+            for p, q, (km, kv) in zip(probs, prev, pres)]
+    run("previous_omega", warm, omb200.B200Solver(precision="mixed", warm_start="none", device=device))
+    for arm in ("learned", "previous_omega"):
+        out[arm]["max_rel_k_diff_vs_none"] = float(np.max(np.abs(ks[arm] - ks["none"]) / ks["none"]))
+    out["instances"] = len(probs)
+    out["grid"] = [probs[0]["grid"].Nx, probs[0]["grid"].Ny]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--samples", type=int, default=4096)
@@ -154,6 +205,7 @@ def main():
     ap.add_argument("--seed", type=int, default=20)
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--out", default=WEIGHTS_PATH)
+    ap.add_argument("--heldout", type=int, default=64, help="held-out cross-sections evaluated after training")
     args = ap.parse_args()
     print(f"generating {args.samples} samples (seed {args.seed})", flush=True)
     F, TF, TN, recs, t_gen = generate(args.samples, args.seed, device=args.device,
@@ -168,6 +220,11 @@ def main():
     np.savez_compressed(args.out, params=net.get_params(), record=json.dumps(record))
     print(json.dumps({k: v for k, v in record.items() if k != "history"}), flush=True)
     print(f"final val loss {hist[-1]['val_loss']:.4f}; wrote {args.out}", flush=True)
+    if args.heldout > 0:
+        net.attach()
+        for ngrid in (128, 256):
+            ev = evaluate(heldout_problems(args.heldout, args.seed + 1000, ngrid, args.device), args.device)
+            print("heldout", json.dumps(ev), flush=True)
 
 
 if __name__ == "__main__":

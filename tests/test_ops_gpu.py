@@ -132,3 +132,22 @@ def test_hfield_matches_oracle():
         cart = h[..., 0:1] * m + h[..., 1:2] * n
         ref = O.maxwell.fft2(cart).reshape(-1)
         assert np.linalg.norm(got[j] - ref) / np.linalg.norm(ref) < 1e-12
+
+
+@pytest.mark.parametrize("n2,n", [(131072, 12), (65536 * 3, 15), (4096, 36)])
+def test_gram_blocks_accuracy(n2, n):
+    """The eigensolver's streaming Gram kernel on FP32-exact random blocks against the exact
+    (FP64) products: FP32 with compensated tile sums within 5e-7·‖z_a‖‖z_b‖ (the FP32 rounding
+    of one tile's partial sums), FP64 within 1e-13."""
+    import omb200
+    from omb200.ops import gram_blocks
+    rng = np.random.default_rng(n2 + n)
+    Z = (rng.standard_normal((n2, n)) + 1j * rng.standard_normal((n2, n))).astype(np.complex64).astype(np.complex128)
+    AZ = (rng.standard_normal((n2, n)) + 1j * rng.standard_normal((n2, n))).astype(np.complex64).astype(np.complex128)
+    Ge, Se = Z.conj().T @ Z, Z.conj().T @ AZ
+    nz, naz = np.linalg.norm(Z, axis=0), np.linalg.norm(AZ, axis=0)
+    for prec, tol in (("fp32", 5e-7), ("fp64", 1e-13)):
+        G, S = gram_blocks(Z, AZ, prec)
+        eg = np.max(np.abs(G - Ge) / np.outer(nz, nz))
+        es = np.max(np.abs(S - Se) / np.outer(nz, naz))
+        assert eg < tol and es < tol, (prec, eg, es)
