@@ -124,6 +124,31 @@ int omb_apply_M_noalloc(int32_t Nx, int32_t Ny, double Dx, double Dy, double k, 
                         int32_t ncol, const void* d_H_in, void* d_H_out, void* stream);
 
 /* ---------------------------------------------------------------------------------
+ * Autotuning of the FP32 operator passes (the counterpart of the reference's FFTW PATIENT
+ * planning at ModeSolver construction, lib/MaxwellEigenmodes/src/maxwell.jl:940-943).
+ * Per (device name, Nx, Ny) the nine combinations of row-pass variant (0, 1, 2: half,
+ * default, double the grid rows per CTA) and column-pass variant (0, 1, 2: 4, 8, 16 columns
+ * per CTA) of an M̂ application are timed and the fastest is kept in a process-wide table,
+ * persisted in a text cache (OMB_TUNE_CACHE, else $XDG_CACHE_HOME/omb200/tiles.txt, else
+ * ~/.cache/omb200/tiles.txt).  omb_batch_create tunes every grid it has not seen (unless
+ * omb_ctx_set_autotune(ctx, 0)), outside the timed solve.
+ * --------------------------------------------------------------------------------- */
+
+/* Tune one grid now for `ncol`-column applications; the chosen variants and, if `seconds` is
+ * not NULL, the nine timings (row-major: row variant, then column variant) are returned. */
+int omb_autotune(omb_ctx* ctx, const omb_grid* grid, int32_t ncol, int32_t* row_variant, int32_t* col_variant,
+                 double* seconds);
+int omb_ctx_set_autotune(omb_ctx* ctx, int32_t enabled);
+/* Host-side table access (no device work). */
+int omb_tune_set(const char* device_name, int32_t Nx, int32_t Ny, int32_t row_variant, int32_t col_variant);
+int omb_tune_get(const char* device_name, int32_t Nx, int32_t Ny, int32_t* row_variant, int32_t* col_variant);
+int omb_tune_clear(void);
+/* Write / merge the table to / from a cache file (NULL: the default path); malformed lines
+ * are skipped; *entries (may be NULL) receives the number of lines read. */
+int omb_tune_save(const char* path);
+int omb_tune_load(const char* path, int32_t* entries);
+
+/* ---------------------------------------------------------------------------------
  * Eigensolves
  * --------------------------------------------------------------------------------- */
 

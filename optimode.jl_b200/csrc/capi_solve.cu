@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "ops.h"
 #include "warmstart.h"
 
 struct omb_batch {
@@ -195,6 +196,15 @@ int omb_batch_create(omb_ctx* ctx, const omb_instance* inst, int n_inst, const o
     b->src_eps[i] = I.epsinv;
     I.epsinv = nullptr;  // uploaded; the caller's array is not kept
   }
+  // the FP32 operator tiles of every grid not tuned yet on this device (once per process and
+  // device, kept in the tuning cache), outside the timed solve like the reference's FFTW plans
+  if (ctx->autotune && b->so.precision != OMB_PREC_FP64)
+    for (const Problem& P : b->probs)
+      if (!tune_known(ctx->device, P.Nx, P.Ny)) {
+        const omb_grid g{P.Nx, P.Ny, P.Dx, P.Dy};
+        rc = autotune_grid(ctx, &g, 4, 16, nullptr, nullptr);
+        if (rc) return rc;
+      }
   *out = b.release();
   return OMB_OK;
 }

@@ -22,6 +22,8 @@ struct omb_ctx {
   uint64_t wait_ns = 1000000000ull;
   // learned warm-start network used by OMB_WARM_LEARNED (not owned)
   struct omb_warmstart* ws = nullptr;
+  // tune the FP32 operator tiles of a grid on its first batched solve (omb_ctx_set_autotune)
+  int autotune = 1;
 };
 
 namespace omb {
@@ -112,5 +114,8 @@ int upload_problem(omb_ctx* ctx, const omb_grid* g, const double* epsinv, Proble
 
 // Fill an OpUnit for one problem (pointers to block buffers set by the caller).
 template <typename T> OpUnit<T> make_unit(const Problem& P);
+// Autotuner (tune.cu): has (device, Nx, Ny) been tuned; tune it now (9 timed variants).
+bool tune_known(int dev, int Nx, int Ny);
+int autotune_grid(omb_ctx* ctx, const omb_grid* g, int ncol, int units, struct TileChoice* best, double* times);
 
 }  // namespace omb

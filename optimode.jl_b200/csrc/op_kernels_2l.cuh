@@ -41,10 +41,12 @@ template <typename C, int L, int TX> __host__ __device__ constexpr int l2_col_ls
 __host__ __device__ constexpr int l2_rows(int NX) {
   return plan2_max(NX) == 0 ? 1 : (128 / plan2_max(NX) > 0 ? 128 / plan2_max(NX) : 1);
 }
-__host__ __device__ constexpr int l2_row_threads(int NX) { return (l2_rows(NX) * plan2_max(NX) + 31) / 32 * 32; }
+__host__ __device__ constexpr int l2_row_threads(int NX, int G) { return (G * plan2_max(NX) + 31) / 32 * 32; }
+__host__ __device__ constexpr int l2_row_threads(int NX) { return l2_row_threads(NX, l2_rows(NX)); }
 template <typename T> __host__ __device__ constexpr int l2_tx(int NY) { return 8; }
+__host__ __device__ constexpr int l2_col_threads_tx(int NY, int TX) { return (TX * plan2_max(NY) + 31) / 32 * 32; }
 template <typename T> __host__ __device__ constexpr int l2_col_threads(int NY) {
-  return (l2_tx<T>(NY) * plan2_max(NY) + 31) / 32 * 32;
+  return l2_col_threads_tx(NY, l2_tx<T>(NY));
 }
 
 // Transverse basis for the pass kernels.  FP64 is basis_at itself; FP32 takes 1/|k+G| and
@@ -103,11 +105,11 @@ __device__ __forceinline__ void prologue_at(const OpUnit<T>& U, const cplx<T>* _
 
 // ------------------------------------------------------------------------------------
 // row_in.  Grid: (ceil(Ny/G), max columns, units); l2_row_threads(NX) threads.
-template <typename T, int NX, int MODE, bool INV>
-__global__ void __launch_bounds__(l2_row_threads(NX)) k_row_in2(const OpUnit<T>* __restrict__ units,
-                                                               const cplx<T>* __restrict__ tw_g) {
+template <typename T, int NX, int MODE, bool INV, int G = l2_rows(NX)>
+__global__ void __launch_bounds__(l2_row_threads(NX, G)) k_row_in2(const OpUnit<T>* __restrict__ units,
+                                                                  const cplx<T>* __restrict__ tw_g) {
   using C = cplx<T>;
-  constexpr int A = plan2_a(NX), B = NX / A, G = l2_rows(NX), NT = l2_row_threads(NX);
+  constexpr int A = plan2_a(NX), B = NX / A, NT = l2_row_threads(NX, G);
   constexpr int LS = l2_row_lstr<C, NX>();
   constexpr bool REG3 = sizeof(T) == 4;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -199,11 +201,12 @@ __device__ __forceinline__ void pointwise_at(const OpUnit<T>& U, size_t p, cplx<
 
 // ------------------------------------------------------------------------------------
 // col.  Grid: (ceil(Nx/TX), max columns, units); l2_col_threads(NY) threads.
-template <typename T, int NY, int S1, int PW, int S2>
-__global__ void __launch_bounds__(l2_col_threads<T>(NY), sizeof(T) == 4 ? 3 : 1)
+template <typename T, int NY, int S1, int PW, int S2, int TX = l2_tx<T>(NY)>
+__global__ void __launch_bounds__(l2_col_threads_tx(NY, TX),
+                                  sizeof(T) == 4 ? (384 / l2_col_threads_tx(NY, TX) > 1 ? 384 / l2_col_threads_tx(NY, TX) : 1) : 1)
     k_col2(const OpUnit<T>* __restrict__ units, const cplx<T>* __restrict__ tw_g) {
   using C = cplx<T>;
-  constexpr int A = plan2_a(NY), B = NY / A, TX = l2_tx<T>(NY), NT = l2_col_threads<T>(NY);
+  constexpr int A = plan2_a(NY), B = NY / A, NT = l2_col_threads_tx(NY, TX);
   constexpr int LS = l2_col_lstr<C, NY, TX>();
   constexpr bool REG3 = sizeof(T) == 4;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -332,11 +335,11 @@ __global__ void __launch_bounds__(l2_col_threads<T>(NY), sizeof(T) == 4 ? 3 : 1)
 
 // ------------------------------------------------------------------------------------
 // row_out.  Grid: (ceil(Ny/G), max columns, units); l2_row_threads(NX) threads.
-template <typename T, int NX, int MODE, bool INV>
-__global__ void __launch_bounds__(l2_row_threads(NX)) k_row_out2(const OpUnit<T>* __restrict__ units,
-                                                                const cplx<T>* __restrict__ tw_g) {
+template <typename T, int NX, int MODE, bool INV, int G = l2_rows(NX)>
+__global__ void __launch_bounds__(l2_row_threads(NX, G)) k_row_out2(const OpUnit<T>* __restrict__ units,
+                                                                   const cplx<T>* __restrict__ tw_g) {
   using C = cplx<T>;
-  constexpr int A = plan2_a(NX), B = NX / A, G = l2_rows(NX), NT = l2_row_threads(NX);
+  constexpr int A = plan2_a(NX), B = NX / A, NT = l2_row_threads(NX, G);
   constexpr int LS = l2_row_lstr<C, NX>();
   constexpr bool REG3 = sizeof(T) == 4;
   extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -25,6 +25,14 @@ struct TwTables {
 };
 
 bool fft_size_supported(int L);
+
+// Tile variants of the FP32 M̂ passes (0, 1, 2: half, default, double the rows per CTA of the
+// row passes / columns per CTA of the column pass), chosen per grid by the autotuner
+// (tune.cu); grids never tuned use the defaults.
+struct TileChoice {
+  int row = 1, col = 1;
+};
+TileChoice tiles_for(int Nx, int Ny);  // for the calling thread's current device
 // Raise a kernel's dynamic shared-memory limit once per (kernel, device); later calls for
 // the same or a smaller size return without touching the driver (so they are safe inside
 // a stream capture after a warm-up launch).

@@ -33,9 +33,43 @@ static cudaError_t launch_pass(PassKernel<T> kern, dim3 g, int nt, size_t smem, 
   return cudaGetLastError();
 }
 
+// Tunable tiles (FP32, the eigensolver's M̂ passes): row passes with G/2, G or 2G rows per CTA,
+// the column pass with TX/2, TX or 2·TX columns (variant 0, 1, 2; 1 is the default).
+template <int NX> __host__ __device__ constexpr int row_g_variant(int v) {
+  return v == 0 ? (l2_rows(NX) / 2 > 0 ? l2_rows(NX) / 2 : 1) : (v == 2 ? 2 * l2_rows(NX) : l2_rows(NX));
+}
+template <int NY> __host__ __device__ constexpr int col_tx_variant(int v) { return v == 0 ? 4 : (v == 2 ? 16 : 8); }
+
+template <typename T, int NX, int G, int MODE, bool INV>
+static cudaError_t row_in_g(const OpUnit<T>* u, int nunits, int Ny, int maxcol, const cplx<T>* tw, cudaStream_t st) {
+  constexpr int NT = l2_row_threads(NX, G);
+  const size_t sm = (size_t)3 * G * l2_row_lstr<cplx<T>, NX>() * sizeof(cplx<T>);
+  const dim3 g((Ny + G - 1) / G, maxcol, nunits);
+  return launch_pass<T>(k_row_in2<T, NX, MODE, INV, G>, g, NT, sm, st, u, tw);
+}
+template <typename T, int NX, int G, int MODE, bool INV>
+static cudaError_t row_out_g(const OpUnit<T>* u, int nunits, int Ny, int maxcol, const cplx<T>* tw, cudaStream_t st) {
+  constexpr int NT = l2_row_threads(NX, G);
+  const size_t sm = (size_t)3 * G * l2_row_lstr<cplx<T>, NX>() * sizeof(cplx<T>);
+  const dim3 g((Ny + G - 1) / G, maxcol, nunits);
+  return launch_pass<T>(k_row_out2<T, NX, MODE, INV, G>, g, NT, sm, st, u, tw);
+}
+template <typename T, int NY, int TX, int S1, int PW, int S2>
+static cudaError_t col_tx(const OpUnit<T>* u, int nunits, int Nx, int maxcol, const cplx<T>* tw, cudaStream_t st) {
+  constexpr int NT = l2_col_threads_tx(NY, TX);
+  const size_t sm = (size_t)3 * TX * l2_col_lstr<cplx<T>, NY, TX>() * sizeof(cplx<T>);
+  const dim3 g((Nx + TX - 1) / TX, maxcol, nunits);
+  return launch_pass<T>(k_col2<T, NY, S1, PW, S2, TX>, g, NT, sm, st, u, tw);
+}
+
 template <typename T, int NX>
 static cudaError_t row_in_nx(int mode, const OpUnit<T>* u, int nunits, int Ny, int maxcol,
-                             const cplx<T>* tw, cudaStream_t st) {
+                             const cplx<T>* tw, cudaStream_t st, int gv = 1) {
+  if constexpr (plan2_a(NX) != 0 && sizeof(T) == 4) {
+    if (mode == RI_KXTC && gv != 1)
+      return gv == 0 ? row_in_g<T, NX, row_g_variant<NX>(0), RI_KXTC, false>(u, nunits, Ny, maxcol, tw, st)
+                     : row_in_g<T, NX, row_g_variant<NX>(2), RI_KXTC, false>(u, nunits, Ny, maxcol, tw, st);
+  }
   if constexpr (plan2_a(NX) != 0) {  // two-level register FFT
     constexpr int G = l2_rows(NX), NT = l2_row_threads(NX);
     const size_t sm = (size_t)3 * G * l2_row_lstr<cplx<T>, NX>() * sizeof(cplx<T>);
@@ -65,7 +99,13 @@ static cudaError_t row_in_nx(int mode, const OpUnit<T>* u, int nunits, int Ny, i
 
 template <typename T, int NX>
 static cudaError_t row_out_nx(int mode, const OpUnit<T>* u, int nunits, int Ny, int maxcol,
-                              const cplx<T>* tw, cudaStream_t st) {
+                              const cplx<T>* tw, cudaStream_t st, int gv = 1) {
+  if constexpr (plan2_a(NX) != 0 && sizeof(T) == 4) {
+    // (the dot-product mode keeps the default rows: its partial sums are laid out per row block)
+    if (mode == RO_KXCT && gv != 1)
+      return gv == 0 ? row_out_g<T, NX, row_g_variant<NX>(0), RO_KXCT, true>(u, nunits, Ny, maxcol, tw, st)
+                     : row_out_g<T, NX, row_g_variant<NX>(2), RO_KXCT, true>(u, nunits, Ny, maxcol, tw, st);
+  }
   if constexpr (plan2_a(NX) != 0) {  // two-level register FFT
     constexpr int G = l2_rows(NX), NT = l2_row_threads(NX);
     const size_t sm = (size_t)3 * G * l2_row_lstr<cplx<T>, NX>() * sizeof(cplx<T>);
@@ -96,7 +136,12 @@ enum ColMode : int { CM_M = 0, CM_P = 1, CM_E = 2, CM_FWD = 3, CM_EPSINV = 4, CM
 
 template <typename T, int NY>
 static cudaError_t col_ny(int mode, const OpUnit<T>* u, int nunits, int Nx, int maxcol,
-                          const cplx<T>* tw, cudaStream_t st) {
+                          const cplx<T>* tw, cudaStream_t st, int tv = 1) {
+  if constexpr (plan2_a(NY) != 0 && sizeof(T) == 4) {
+    if (mode == CM_M && tv != 1)
+      return tv == 0 ? col_tx<T, NY, col_tx_variant<NY>(0), CS_FWD, PW_EPS, CS_INV>(u, nunits, Nx, maxcol, tw, st)
+                     : col_tx<T, NY, col_tx_variant<NY>(2), CS_FWD, PW_EPS, CS_INV>(u, nunits, Nx, maxcol, tw, st);
+  }
   if constexpr (plan2_a(NY) != 0) {  // two-level register FFT
     constexpr int TX = l2_tx<T>(NY), NT = l2_col_threads<T>(NY);
     const size_t sm = (size_t)3 * TX * l2_col_lstr<cplx<T>, NY, TX>() * sizeof(cplx<T>);
@@ -132,9 +177,9 @@ template <> const double2* tw_for<double>(const TwTables& t, int L) { return t.f
 
 template <typename T>
 static cudaError_t row_in(int mode, const OpUnit<T>* u, int nunits, int Nx, int Ny, int maxcol,
-                          const TwTables& t, cudaStream_t st) {
+                          const TwTables& t, cudaStream_t st, int gv = 1) {
   switch (Nx) {
-#define OMB_CASE(L) case L: return row_in_nx<T, L>(mode, u, nunits, Ny, maxcol, tw_for<T>(t, L), st);
+#define OMB_CASE(L) case L: return row_in_nx<T, L>(mode, u, nunits, Ny, maxcol, tw_for<T>(t, L), st, gv);
     OMB_FFT_SIZES(OMB_CASE)
 #undef OMB_CASE
     default: return cudaErrorInvalidValue;
@@ -142,9 +187,9 @@ static cudaError_t row_in(int mode, const OpUnit<T>* u, int nunits, int Nx, int 
 }
 template <typename T>
 static cudaError_t row_out(int mode, const OpUnit<T>* u, int nunits, int Nx, int Ny, int maxcol,
-                           const TwTables& t, cudaStream_t st) {
+                           const TwTables& t, cudaStream_t st, int gv = 1) {
   switch (Nx) {
-#define OMB_CASE(L) case L: return row_out_nx<T, L>(mode, u, nunits, Ny, maxcol, tw_for<T>(t, L), st);
+#define OMB_CASE(L) case L: return row_out_nx<T, L>(mode, u, nunits, Ny, maxcol, tw_for<T>(t, L), st, gv);
     OMB_FFT_SIZES(OMB_CASE)
 #undef OMB_CASE
     default: return cudaErrorInvalidValue;
@@ -152,9 +197,9 @@ static cudaError_t row_out(int mode, const OpUnit<T>* u, int nunits, int Nx, int
 }
 template <typename T>
 static cudaError_t col(int mode, const OpUnit<T>* u, int nunits, int Nx, int Ny, int maxcol,
-                       const TwTables& t, cudaStream_t st) {
+                       const TwTables& t, cudaStream_t st, int tv = 1) {
   switch (Ny) {
-#define OMB_CASE(L) case L: return col_ny<T, L>(mode, u, nunits, Nx, maxcol, tw_for<T>(t, L), st);
+#define OMB_CASE(L) case L: return col_ny<T, L>(mode, u, nunits, Nx, maxcol, tw_for<T>(t, L), st, tv);
     OMB_FFT_SIZES(OMB_CASE)
 #undef OMB_CASE
     default: return cudaErrorInvalidValue;
@@ -167,14 +212,15 @@ template <typename T>
 cudaError_t launch_op(OpKind op, const OpUnit<T>* u, int nunits, int Nx, int Ny, int maxcol,
                       const TwTables& t, cudaStream_t st) {
   if (nunits <= 0 || maxcol <= 0) return cudaSuccess;
+  const TileChoice tc = sizeof(T) == 4 ? tiles_for(Nx, Ny) : TileChoice{};
   switch (op) {
     case OP_M:
-      OMB_TRY(row_in<T>(RI_KXTC, u, nunits, Nx, Ny, maxcol, t, st));
-      OMB_TRY(col<T>(CM_M, u, nunits, Nx, Ny, maxcol, t, st));
-      return row_out<T>(RO_KXCT, u, nunits, Nx, Ny, maxcol, t, st);
+      OMB_TRY(row_in<T>(RI_KXTC, u, nunits, Nx, Ny, maxcol, t, st, tc.row));
+      OMB_TRY(col<T>(CM_M, u, nunits, Nx, Ny, maxcol, t, st, tc.col));
+      return row_out<T>(RO_KXCT, u, nunits, Nx, Ny, maxcol, t, st, tc.row);
     case OP_MDOT:
-      OMB_TRY(row_in<T>(RI_KXTC, u, nunits, Nx, Ny, maxcol, t, st));
-      OMB_TRY(col<T>(CM_M, u, nunits, Nx, Ny, maxcol, t, st));
+      OMB_TRY(row_in<T>(RI_KXTC, u, nunits, Nx, Ny, maxcol, t, st, tc.row));
+      OMB_TRY(col<T>(CM_M, u, nunits, Nx, Ny, maxcol, t, st, tc.col));
       return row_out<T>(RO_KXCT_DOT, u, nunits, Nx, Ny, maxcol, t, st);
     case OP_P:
       OMB_TRY(row_in<T>(RI_KXINV, u, nunits, Nx, Ny, maxcol, t, st));

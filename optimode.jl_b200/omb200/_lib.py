@@ -28,6 +28,8 @@ OPS = {"M": 0, "P": 1, "P_diag": 2}
 EXPORTS = (
     "omb_version", "omb_fft_size_supported", "omb_last_error", "omb_ctx_create",
     "omb_ctx_destroy", "omb_apply", "omb_HMkH", "omb_efield", "omb_hfield", "omb_gram_blocks",
+    "omb_autotune", "omb_ctx_set_autotune", "omb_tune_set", "omb_tune_get", "omb_tune_clear", "omb_tune_save",
+    "omb_tune_load",
 )
 
 
@@ -74,6 +76,15 @@ def load():
             "omb_efield": (ctypes.c_int, [vp, ctypes.c_int, gp, ctypes.c_double, _dp, _dp, _dp]),
             "omb_hfield": (ctypes.c_int, [vp, gp, ctypes.c_double, ctypes.c_int, _dp, _dp]),
             "omb_gram_blocks": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int64, ctypes.c_int32, _dp, _dp, _dp, _dp]),
+            "omb_autotune": (ctypes.c_int, [vp, gp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                            ctypes.POINTER(ctypes.c_int32), _dp]),
+            "omb_ctx_set_autotune": (ctypes.c_int, [vp, ctypes.c_int32]),
+            "omb_tune_set": (ctypes.c_int, [ctypes.c_char_p] + [ctypes.c_int32] * 4),
+            "omb_tune_get": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32,
+                                            ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]),
+            "omb_tune_clear": (ctypes.c_int, []),
+            "omb_tune_save": (ctypes.c_int, [ctypes.c_char_p]),
+            "omb_tune_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int32)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(lib, name)

@@ -119,3 +119,41 @@ def gram_blocks(Z, AZ, precision: str = "fp32", device: int = 0):
     _lib.check(lib.omb_gram_blocks(ctx.handle, _lib.PREC[precision], int(n2), int(n), _dptr(Z), _dptr(AZ),
                                    _dptr(G), _dptr(S)))
     return G, S
+
+
+# ---- operator-tile autotuning -------------------------------------------------------------
+
+def autotune(grid, ncol: int = 4, device: int = 0):
+    """Tune the FP32 operator tiles of `grid` now (``omb_autotune``): returns
+    ``(row_variant, col_variant, seconds[3][3])``."""
+    lib = _lib.load()
+    ctx = _lib.context(device)
+    r, c = ctypes.c_int32(), ctypes.c_int32()
+    t = np.zeros(9)
+    _lib.check(lib.omb_autotune(ctx.handle, ctypes.byref(grid.c()), int(ncol), ctypes.byref(r), ctypes.byref(c),
+                                _dptr(t)))
+    return r.value, c.value, t.reshape(3, 3)
+
+
+def tune_set(device_name: str, Nx: int, Ny: int, row: int, col: int) -> None:
+    _lib.check(_lib.load().omb_tune_set(device_name.encode(), Nx, Ny, row, col))
+
+
+def tune_get(device_name: str, Nx: int, Ny: int):
+    r, c = ctypes.c_int32(), ctypes.c_int32()
+    _lib.check(_lib.load().omb_tune_get(device_name.encode(), Nx, Ny, ctypes.byref(r), ctypes.byref(c)))
+    return r.value, c.value
+
+
+def tune_clear() -> None:
+    _lib.check(_lib.load().omb_tune_clear())
+
+
+def tune_save(path: str) -> None:
+    _lib.check(_lib.load().omb_tune_save(path.encode()))
+
+
+def tune_load(path: str) -> int:
+    n = ctypes.c_int32()
+    _lib.check(_lib.load().omb_tune_load(path.encode(), ctypes.byref(n)))
+    return n.value

@@ -151,3 +151,32 @@ def test_gram_blocks_accuracy(n2, n):
         eg = np.max(np.abs(G - Ge) / np.outer(nz, nz))
         es = np.max(np.abs(S - Se) / np.outer(nz, naz))
         assert eg < tol and es < tol, (prec, eg, es)
+
+
+def test_tile_variants_agree_and_autotune_picks_one():
+    """Every tile variant of the FP32 M̂ passes gives the same result as the default tiles (the
+    per-pixel arithmetic does not depend on the tile), and the autotuner times all nine."""
+    import torch
+
+    import omb200
+    from omb200 import ops
+    from omb200.geometry import ln_ridge_shapes
+    from oracle import smoothing as OS
+    name = torch.cuda.get_device_name(0)
+    for (Nx, Ny) in ((256, 256), (192, 128)):
+        g = omb200.Grid(8.0, 5.0, Nx, Ny)
+        shapes, bg = ln_ridge_shapes(g, top_width=1.5)
+        ei = OS.smooth_epsinv_constant(shapes, bg, g)
+        rng = np.random.default_rng(Nx)
+        H = rng.standard_normal((2 * g.N, 3)) + 1j * rng.standard_normal((2 * g.N, 3))
+        ops.tune_set(name, Nx, Ny, 1, 1)
+        ref = omb200.apply_M(1.3, ei, g, H, precision="fp32")
+        for r in range(3):
+            for c in range(3):
+                ops.tune_set(name, Nx, Ny, r, c)
+                got = omb200.apply_M(1.3, ei, g, H, precision="fp32")
+                assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-6, (Nx, Ny, r, c)
+        r, c, t = ops.autotune(g)
+        assert 0 <= r <= 2 and 0 <= c <= 2 and np.all(t > 0)
+        assert t[r, c] == t.min()
+        assert ops.tune_get(name, Nx, Ny) == (r, c)

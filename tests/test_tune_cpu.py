@@ -1,0 +1,38 @@
+"""The autotuner's table and cache file (host logic only, no device work): entries keyed by
+device name and grid, a save/load round trip, malformed lines skipped, bad keys refused."""
+
+from __future__ import annotations
+
+import pytest
+
+from omb200 import ops
+
+
+def test_tune_table_round_trip(tmp_path):
+    ops.tune_clear()
+    ops.tune_set("NVIDIA B200", 256, 256, 2, 0)
+    ops.tune_set("NVIDIA B200", 128, 192, 0, 1)
+    ops.tune_set("Other GPU", 256, 256, 1, 2)
+    assert ops.tune_get("NVIDIA B200", 256, 256) == (2, 0)
+    assert ops.tune_get("Other GPU", 256, 256) == (1, 2)
+    p = tmp_path / "sub" / "tiles.txt"
+    ops.tune_save(str(p))
+    lines = p.read_text().splitlines()
+    assert len(lines) == 3 and all(line.count("|") == 5 for line in lines)
+    ops.tune_clear()
+    with pytest.raises(ops._lib.OmbError):
+        ops.tune_get("NVIDIA B200", 256, 256)
+    # a malformed line and an out-of-range variant are skipped
+    p.write_text(p.read_text() + "garbage line\nNVIDIA B200|64|64|7|0|0.1\n")
+    assert ops.tune_load(str(p)) == 3
+    assert ops.tune_get("NVIDIA B200", 128, 192) == (0, 1)
+    with pytest.raises(ops._lib.OmbError):
+        ops.tune_get("NVIDIA B200", 64, 64)
+    ops.tune_clear()
+
+
+def test_tune_rejects_bad_entries():
+    with pytest.raises(ops._lib.OmbError):
+        ops.tune_set("NVIDIA B200", 256, 256, 3, 0)
+    with pytest.raises(ops._lib.OmbError):
+        ops.tune_set("", 256, 256, 1, 1)
