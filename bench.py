@@ -283,6 +283,109 @@ def cpu_baseline_and_errors(probs, results, infos):
     return base, errs
 
 
+def _solve_bytes(p) -> float:
+    """Device bytes of one problem's tracks (FP64 + FP32 blocks [X W P] and A·[X W P], two
+    parities), to cut large batches into chunks that fit in HBM."""
+    g = p["grid"]
+    n2 = 2 * g.Nx * g.Ny
+    cols = sum(b + 2 for b in range(p["nev"]))
+    return 288.0 * n2 * cols
+
+
+def _chunks(probs, budget: float):
+    """Consecutive chunks under `budget` bytes that keep each shared ε⁻¹ array (a sweep group)
+    in one chunk."""
+    groups, order = {}, []
+    for p in probs:
+        key = id(p["eps_inv"])
+        if key not in groups:
+            groups[key] = []
+            order.append(key)
+        groups[key].append(p)
+    chunks, cur, cur_b = [], [], 0.0
+    for key in order:
+        gb = sum(_solve_bytes(p) for p in groups[key])
+        if cur and cur_b + gb > budget:
+            chunks.append(cur)
+            cur, cur_b = [], 0.0
+        cur += groups[key]
+        cur_b += gb
+    if cur:
+        chunks.append(cur)
+    return chunks
+
+
+def _solve_chunks(chunks, solver):
+    """Device seconds (CUDA events of each omb_batch_run), wall seconds of the whole
+    create/run/results path with host buffers, converged modes, modes and iterations."""
+    import omb200
+    dev, conv, modes, iters = 0.0, 0, 0, []
+    t0 = time.perf_counter()
+    for ch in chunks:
+        b = omb200.Batch(ch, solver)
+        b.run()
+        dev += b.stats()["run_seconds"]
+        _, info = b.results(return_info=True, raise_on_failure=False)
+        b.close()
+        conv += int(sum(int(np.sum(i["status"] == 0)) for i in info))
+        modes += int(sum(len(i["status"]) for i in info))
+        iters += [int(x) for i in info for x in i["iterations"]]
+    wall = time.perf_counter() - t0
+    return {"device_seconds": dev, "e2e_seconds": wall, "converged": conv, "modes": modes,
+            "modes_per_s": conv / dev, "e2e_modes_per_s": conv / wall,
+            "iterations_mean": float(np.mean(iters)), "iterations_max": int(max(iters))}
+
+
+def config3_measure(device: int):
+    """The uneven batch: 512 problems (64 ω in [0.5, 1.0] μm⁻¹ × 8 ridge widths in [0.6, 2.4]
+    μm, grids {128², 192×128, 256×192, 256²}, 2–6 bands, Si₃N₄ / LiNbO₃ / Si cores, seed 3),
+    solved in HBM-sized chunks of whole sweep groups, from random starts and with the sweep
+    warm start, mixed precision, residual 1e-8."""
+    import omb200
+    from omb200 import workloads as W
+    probs = W.sweep_batch(device=device)
+    chunks = _chunks(probs, 40e9)
+    out = {"case": "config3", "problems": len(probs), "modes": sum(p["nev"] for p in probs), "chunks": len(chunks),
+           "grids": sorted({(p["grid"].Nx, p["grid"].Ny) for p in probs})}
+    for warm in ("sweep", "none"):
+        solver = omb200.B200Solver(precision="mixed", warm_start=warm, device=device)
+        _solve_chunks(chunks[:1], solver)  # warm-up (tuning, allocation caches)
+        out[warm] = _solve_chunks(chunks, solver)
+    return out
+
+
+def config5_measure(device: int, n_inst: int = 16, per_chunk: int = 4):
+    """Large instances: 512², 8 bands, seeded slot / coupled-waveguide rows (seeds 0..15),
+    solved in chunks of `per_chunk` with the learned warm start (when trained parameters are
+    present) and the FP32 + FP64 polish, then each instance's full pull-back of a seeded
+    cotangent (k̄ and ē on every band) to ∂ε⁻¹ and ∂ω."""
+    import omb200
+    from omb200 import workloads as W
+    from omb200.warmstart import WEIGHTS_PATH
+    cells = [W.slot_cell(s, 512, device=device) for s in range(n_inst)]
+    probs = [{"omega": 1 / 1.55, "eps_inv": e, "grid": g, "nev": 8} for g, e in cells]
+    warm = "learned" if os.path.exists(WEIGHTS_PATH) else "none"
+    solver = omb200.B200Solver(precision="mixed", warm_start=warm, device=device)
+    chunks = [probs[i:i + per_chunk] for i in range(0, len(probs), per_chunk)]
+    _solve_chunks(chunks[:1], solver)
+    res = _solve_chunks(chunks, solver)
+    # pull-back of every instance (one chunk's results at a time)
+    t_adj, n_adj = 0.0, 0
+    rng = np.random.default_rng(5)
+    for ch in chunks:
+        sols = omb200.solve_k_batch(ch, solver, raise_on_failure=False)
+        for p, (km, kv) in zip(ch, sols):
+            kbar = rng.standard_normal(8)
+            evbar = [rng.standard_normal(kv[0].size) + 1j * rng.standard_normal(kv[0].size) for _ in range(8)]
+            t0 = time.perf_counter()
+            omb200.pullback(p["omega"], p["eps_inv"], p["grid"], km, kv, kbar, evbar, solver=solver)
+            t_adj += time.perf_counter() - t0
+            n_adj += 1
+    return {"case": "config5", "instances": n_inst, "nev": 8, "grid": [512, 512], "warm_start": warm,
+            "solve": res, "pullback_seconds_per_instance": t_adj / max(n_adj, 1),
+            "pullback_what": "seeded cotangent on all 8 k and eigenvectors, host buffers, FP64 MINRES"}
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -329,11 +432,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-smoothing", action="store_true")
-    ap.add_argument("--case", default="full", choices=["full", "apply", "solve1", "batch", "smoothing"],
+    ap.add_argument("--case", default="full",
+                    choices=["full", "apply", "solve1", "batch", "smoothing", "config3", "config5"],
                     help="apply / solve1 / batch / smoothing: one operator-apply timing, one "
                          "single-instance solve, one batched solve of --instances cells, or the "
                          "smoothing measurement with --smoothing-sets frequency sets (small, "
-                         "self-contained runs for profiling)")
+                         "self-contained runs for profiling); config3: the 512-problem uneven "
+                         "batch; config5: sixteen 512x512 8-band slot cells with their pull-backs")
     ap.add_argument("--apply-cells", type=int, default=64)
     ap.add_argument("--smoothing-sets", type=int, default=64)
     args = ap.parse_args()
@@ -342,6 +447,12 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank)
+    if args.case == "config3":
+        print(json.dumps(config3_measure(local)), flush=True)
+        return
+    if args.case == "config5":
+        print(json.dumps(config5_measure(local)), flush=True)
+        return
     if args.case == "smoothing":
         print(json.dumps({"case": "smoothing", **smoothing_measure(local, nsets=args.smoothing_sets,
                                                                     reps=args.steps)}))

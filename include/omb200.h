@@ -126,22 +126,26 @@ int omb_apply_M_noalloc(int32_t Nx, int32_t Ny, double Dx, double Dy, double k, 
 /* ---------------------------------------------------------------------------------
  * Autotuning of the FP32 operator passes (the counterpart of the reference's FFTW PATIENT
  * planning at ModeSolver construction, lib/MaxwellEigenmodes/src/maxwell.jl:940-943).
- * Per (device name, Nx, Ny) the nine combinations of row-pass variant (0, 1, 2: half,
- * default, double the grid rows per CTA) and column-pass variant (0, 1, 2: 4, 8, 16 columns
- * per CTA) of an M̂ application are timed and the fastest is kept in a process-wide table,
+ * Per (device name, Nx, Ny) the 36 combinations of row-pass variant (0, 1, 2: half, default,
+ * double the grid rows per CTA), column-pass variant (0, 1, 2: 4, 8, 16 columns per CTA) and
+ * wave variant (0: all columns in one launch per pass; 1, 2, 3: waves of 32, 64, 128 columns,
+ * each wave's intermediate staying in L2) of an M̂ application are timed and the fastest is
+ * kept in a process-wide table,
  * persisted in a text cache (OMB_TUNE_CACHE, else $XDG_CACHE_HOME/omb200/tiles.txt, else
  * ~/.cache/omb200/tiles.txt).  omb_batch_create tunes every grid it has not seen (unless
  * omb_ctx_set_autotune(ctx, 0)), outside the timed solve.
  * --------------------------------------------------------------------------------- */
 
-/* Tune one grid now for `ncol`-column applications; the chosen variants and, if `seconds` is
- * not NULL, the nine timings (row-major: row variant, then column variant) are returned. */
+/* Tune one grid now for `ncol`-column applications on 64 units; the chosen variants and, if
+ * `seconds` is not NULL, the 36 timings (row-major over row, column, wave variant). */
 int omb_autotune(omb_ctx* ctx, const omb_grid* grid, int32_t ncol, int32_t* row_variant, int32_t* col_variant,
-                 double* seconds);
+                 int32_t* wave_variant, double* seconds);
 int omb_ctx_set_autotune(omb_ctx* ctx, int32_t enabled);
 /* Host-side table access (no device work). */
-int omb_tune_set(const char* device_name, int32_t Nx, int32_t Ny, int32_t row_variant, int32_t col_variant);
-int omb_tune_get(const char* device_name, int32_t Nx, int32_t Ny, int32_t* row_variant, int32_t* col_variant);
+int omb_tune_set(const char* device_name, int32_t Nx, int32_t Ny, int32_t row_variant, int32_t col_variant,
+                 int32_t wave_variant);
+int omb_tune_get(const char* device_name, int32_t Nx, int32_t Ny, int32_t* row_variant, int32_t* col_variant,
+                 int32_t* wave_variant);
 int omb_tune_clear(void);
 /* Write / merge the table to / from a cache file (NULL: the default path); malformed lines
  * are skipped; *entries (may be NULL) receives the number of lines read. */
@@ -170,7 +174,7 @@ int omb_tune_load(const char* path, int32_t* entries);
                             solved first and the others start from its eigenvectors and
                             per-band k — the batched form of the reference's per-cell warm
                             start (lib/EigenmodeExpansion/src/eme.jl:58-72)             */
-#define OMB_WARM_LEARNED 3 /* instances without guesses of their own on 128² or 256² grids start
+#define OMB_WARM_LEARNED 3 /* instances without guesses of their own on 128², 256² or 512² grids start
                             from the learned network attached to the context
                             (omb_ctx_set_warmstart): its (Hx, Hy) fields of bands 0..3 projected
                             on the plane waves at k = n_eff·ω, and those k as Newton starts;
@@ -378,7 +382,7 @@ int omb_smoothing_plan_destroy(omb_smoothing_plan* plan);
  * Learned warm start (no reference counterpart: the reference starts every solve from
  * random blocks or the caller's Hguess, lib/MaxwellEigenmodes/src/solve.jl:201-210).
  * A six-layer BF16 convolutional network on the tensor cores maps the ε⁻¹ map and ω of a
- * 128² or 256² cross-section to initial (Hx, Hy) fields and effective indices of the four
+ * 128², 256² or 512² cross-section to initial (Hx, Hy) fields and effective indices of the four
  * lowest bands.  Device pointers throughout; calls are ordered on the context's stream.
  * --------------------------------------------------------------------------------- */
 
@@ -406,7 +410,8 @@ int64_t omb_warmstart_num_params(void);
 int omb_warmstart_get_params(omb_warmstart* ws, float* host);
 int omb_warmstart_set_params(omb_warmstart* ws, const float* host);
 /* One input image (128×128×8 BF16, NHWC) from a device ε⁻¹ (3, 3, Nx, Ny) Float64 array of a
- * 128² or 256² grid and ω, on `stream` (NULL: the context's stream). */
+ * 128², 256² or 512² grid (pixels averaged down to 128²) and ω, on `stream` (NULL: the
+ * context's stream). */
 int omb_warmstart_features(omb_warmstart* ws, const double* d_epsinv, int32_t Nx, int32_t Ny, double omega,
                            void* d_feat, void* stream);
 /* Network output for `batch` images: d_out [batch·64·64 × 16] FP32, channels 2b, 2b+1 the

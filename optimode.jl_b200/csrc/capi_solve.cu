@@ -202,7 +202,7 @@ int omb_batch_create(omb_ctx* ctx, const omb_instance* inst, int n_inst, const o
     for (const Problem& P : b->probs)
       if (!tune_known(ctx->device, P.Nx, P.Ny)) {
         const omb_grid g{P.Nx, P.Ny, P.Dx, P.Dy};
-        rc = autotune_grid(ctx, &g, 4, 16, nullptr, nullptr);
+        rc = autotune_grid(ctx, &g, 4, 64, nullptr, nullptr);
         if (rc) return rc;
       }
   *out = b.release();
@@ -274,7 +274,7 @@ int omb_batch_run(omb_batch* b) {
       const omb_instance& I = b->inst[i];
       const Problem& P = b->probs[b->pidx[i]];
       if (I.nguess > 0 || !b->kbands[i].empty()) continue;
-      if (!((P.Nx == 128 && P.Ny == 128) || (P.Nx == 256 && P.Ny == 256))) continue;
+      if (!(P.Nx == P.Ny && (P.Nx == 128 || P.Nx == 256 || P.Nx == 512))) continue;
       learned_of[i] = (int)lp.size();
       lp.push_back(&P);
       lw.push_back(I.omega);

@@ -213,6 +213,19 @@ cudaError_t launch_op(OpKind op, const OpUnit<T>* u, int nunits, int Nx, int Ny,
                       const TwTables& t, cudaStream_t st) {
   if (nunits <= 0 || maxcol <= 0) return cudaSuccess;
   const TileChoice tc = sizeof(T) == 4 ? tiles_for(Nx, Ny) : TileChoice{};
+  if (tc.wave > 0 && (op == OP_M || op == OP_MDOT)) {
+    const int per = wave_columns(tc.wave) / maxcol > 0 ? wave_columns(tc.wave) / maxcol : 1;
+    if (per < nunits) {
+      for (int u0 = 0; u0 < nunits; u0 += per) {
+        const int n = nunits - u0 < per ? nunits - u0 : per;
+        OMB_TRY(row_in<T>(RI_KXTC, u + u0, n, Nx, Ny, maxcol, t, st, tc.row));
+        OMB_TRY(col<T>(CM_M, u + u0, n, Nx, Ny, maxcol, t, st, tc.col));
+        OMB_TRY(op == OP_M ? row_out<T>(RO_KXCT, u + u0, n, Nx, Ny, maxcol, t, st, tc.row)
+                           : row_out<T>(RO_KXCT_DOT, u + u0, n, Nx, Ny, maxcol, t, st));
+      }
+      return cudaSuccess;
+    }
+  }
   switch (op) {
     case OP_M:
       OMB_TRY(row_in<T>(RI_KXTC, u, nunits, Nx, Ny, maxcol, t, st, tc.row));

@@ -1,9 +1,10 @@
 // Autotuner for the FP32 operator passes (the analogue of the reference's FFTW PATIENT
 // planning, lib/MaxwellEigenmodes/src/maxwell.jl:940-943): per (device, Nx, Ny) it times
-// the three row-tile × three column-tile variants of an M̂ application on device-resident
-// data and keeps the fastest.  Choices live in a process-wide table keyed by the device name
-// and grid, persisted as text lines "<device>|<Nx>|<Ny>|<row>|<col>|<seconds>" in a cache
-// file (OMB_TUNE_CACHE, else $XDG_CACHE_HOME/omb200/tiles.txt, else ~/.cache/omb200/tiles.txt).
+// the three row-tile × three column-tile × four wave-size variants of an M̂ application on
+// device-resident data and keeps the fastest.  Choices live in a process-wide table keyed by
+// the device name and grid, persisted as text lines
+// "<device>|<Nx>|<Ny>|<row>|<col>|<seconds>|<wave>" in a cache file (OMB_TUNE_CACHE, else
+// $XDG_CACHE_HOME/omb200/tiles.txt, else ~/.cache/omb200/tiles.txt).
 #include <sys/stat.h>
 
 #include <cerrno>
@@ -25,10 +26,13 @@
 
 namespace omb {
 
+constexpr int TUNE_UNITS = 64;  // units of the timed applications (above L2 for ≥ 128² grids)
+
 namespace {
 struct TuneEntry {
   int row = 1, col = 1;
   double seconds = 0;
+  int wave = 0;
 };
 using TuneKey = std::tuple<std::string, int, int>;
 std::mutex g_tune_mu;
@@ -50,13 +54,15 @@ bool parse_line(const std::string& line, TuneKey& k, TuneEntry& e) {
   std::stringstream ss(line);
   std::string item;
   while (std::getline(ss, item, '|')) f.push_back(item);
-  if (f.size() != 6 || f[0].empty()) return false;
+  if ((f.size() != 6 && f.size() != 7) || f[0].empty()) return false;
   try {
     const int nx = std::stoi(f[1]), ny = std::stoi(f[2]), r = std::stoi(f[3]), c = std::stoi(f[4]);
     const double s = std::stod(f[5]);
-    if (nx <= 0 || ny <= 0 || r < 0 || r > 2 || c < 0 || c > 2 || !(s >= 0)) return false;
+    const int w = f.size() == 7 ? std::stoi(f[6]) : 0;
+    if (nx <= 0 || ny <= 0 || r < 0 || r > 2 || c < 0 || c > 2 || w < 0 || w >= WAVE_VARIANTS || !(s >= 0))
+      return false;
     k = TuneKey{f[0], nx, ny};
-    e = TuneEntry{r, c, s};
+    e = TuneEntry{r, c, s, w};
     return true;
   } catch (...) {
     return false;
@@ -87,7 +93,7 @@ int save_locked(const std::string& path) {
     if (!out) return fail(OMB_ERR_INVALID_ARG, "cannot write the tuning cache " + tmp);
     for (const auto& kv : g_tune)
       out << std::get<0>(kv.first) << '|' << std::get<1>(kv.first) << '|' << std::get<2>(kv.first) << '|'
-          << kv.second.row << '|' << kv.second.col << '|' << kv.second.seconds << '\n';
+          << kv.second.row << '|' << kv.second.col << '|' << kv.second.seconds << '|' << kv.second.wave << '\n';
   }
   if (std::rename(tmp.c_str(), path.c_str()) != 0) return fail(OMB_ERR_INVALID_ARG, "cannot replace " + path);
   return OMB_OK;
@@ -123,7 +129,7 @@ TileChoice tiles_for(int Nx, int Ny) {
   ensure_loaded_locked();
   auto it = g_tune.find(TuneKey{current_device_name_locked(), Nx, Ny});
   TileChoice t;
-  if (it != g_tune.end()) { t.row = it->second.row; t.col = it->second.col; }
+  if (it != g_tune.end()) { t.row = it->second.row; t.col = it->second.col; t.wave = it->second.wave; }
   return t;
 }
 
@@ -134,8 +140,8 @@ bool tune_known(int dev, int Nx, int Ny) {
   return g_tune.count(TuneKey{name, Nx, Ny}) > 0;
 }
 
-// Times the nine tile variants of one FP32 M̂ application to `ncol` columns on `units` copies
-// of a uniform cell and records the fastest.
+// Times the 36 tile × wave variants of one FP32 M̂ application to `ncol` columns on `units`
+// copies of a uniform cell and records the fastest.
 int autotune_grid(omb_ctx* ctx, const omb_grid* g, int ncol, int units, TileChoice* best, double* times) {
   int rc = check_grid(g);
   if (rc) return rc;
@@ -177,11 +183,12 @@ int autotune_grid(omb_ctx* ctx, const omb_grid* g, int ncol, int units, TileChoi
   int vi = 0;
   rc = OMB_OK;
   for (int r = 0; r < 3 && !rc; ++r)
-    for (int c = 0; c < 3 && !rc; ++c, ++vi) {
+    for (int c = 0; c < 3 && !rc; ++c)
+      for (int wv = 0; wv < WAVE_VARIANTS && !rc; ++wv, ++vi) {
       {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         ensure_loaded_locked();
-        g_tune[TuneKey{name, g->Nx, g->Ny}] = TuneEntry{r, c, 0.0};
+        g_tune[TuneKey{name, g->Nx, g->Ny}] = TuneEntry{r, c, 0.0, wv};
       }
       cudaError_t e = cudaSuccess;
       for (int w = 0; w < 2 && e == cudaSuccess; ++w) e = launch_op<float>(OP_M, du.p, units, g->Nx, g->Ny, ncol, ctx->tw, st);
@@ -195,7 +202,7 @@ int autotune_grid(omb_ctx* ctx, const omb_grid* g, int ncol, int units, TileChoi
       if (e != cudaSuccess) { rc = cuda_fail(e, "autotune"); break; }
       const double s = ms * 1e-3 / reps;
       if (times) times[vi] = s;
-      if (s < best_s) { best_s = s; bt.row = r; bt.col = c; }
+      if (s < best_s) { best_s = s; bt.row = r; bt.col = c; bt.wave = wv; }
     }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -203,7 +210,7 @@ int autotune_grid(omb_ctx* ctx, const omb_grid* g, int ncol, int units, TileChoi
     std::lock_guard<std::mutex> lk(g_tune_mu);
     if (rc) g_tune.erase(TuneKey{name, g->Nx, g->Ny});
     else {
-      g_tune[TuneKey{name, g->Nx, g->Ny}] = TuneEntry{bt.row, bt.col, best_s};
+      g_tune[TuneKey{name, g->Nx, g->Ny}] = TuneEntry{bt.row, bt.col, best_s, bt.wave};
       const std::string p = default_cache_path();
       if (!p.empty()) save_locked(p);  // best effort: a read-only home only loses persistence
     }
@@ -220,14 +227,15 @@ using namespace omb;
 extern "C" {
 
 int omb_autotune(omb_ctx* ctx, const omb_grid* grid, int32_t ncol, int32_t* row_variant, int32_t* col_variant,
-                 double* seconds) {
+                 int32_t* wave_variant, double* seconds) {
   if (!ctx || !grid) return fail(OMB_ERR_INVALID_ARG, "NULL argument");
   OMB_CU(cudaSetDevice(ctx->device));
   TileChoice t;
-  const int rc = autotune_grid(ctx, grid, ncol, 16, &t, seconds);
+  const int rc = autotune_grid(ctx, grid, ncol, TUNE_UNITS, &t, seconds);
   if (rc) return rc;
   if (row_variant) *row_variant = t.row;
   if (col_variant) *col_variant = t.col;
+  if (wave_variant) *wave_variant = t.wave;
   return OMB_OK;
 }
 
@@ -237,20 +245,22 @@ int omb_ctx_set_autotune(omb_ctx* ctx, int32_t enabled) {
   return OMB_OK;
 }
 
-int omb_tune_set(const char* device_name, int32_t Nx, int32_t Ny, int32_t row_variant, int32_t col_variant) {
+int omb_tune_set(const char* device_name, int32_t Nx, int32_t Ny, int32_t row_variant, int32_t col_variant,
+                 int32_t wave_variant) {
   if (!device_name || !*device_name || Nx <= 0 || Ny <= 0 || row_variant < 0 || row_variant > 2 || col_variant < 0 ||
-      col_variant > 2)
-    return fail(OMB_ERR_INVALID_ARG, "omb_tune_set: bad key or variant (0..2)");
+      col_variant > 2 || wave_variant < 0 || wave_variant >= WAVE_VARIANTS)
+    return fail(OMB_ERR_INVALID_ARG, "omb_tune_set: bad key or variant (rows, columns 0..2; wave 0..3)");
   std::string n = device_name;
   for (char& c : n)
     if (c == '|' || c == '\n') c = '_';
   std::lock_guard<std::mutex> lk(g_tune_mu);
   ensure_loaded_locked();
-  g_tune[TuneKey{n, Nx, Ny}] = TuneEntry{row_variant, col_variant, 0.0};
+  g_tune[TuneKey{n, Nx, Ny}] = TuneEntry{row_variant, col_variant, 0.0, wave_variant};
   return OMB_OK;
 }
 
-int omb_tune_get(const char* device_name, int32_t Nx, int32_t Ny, int32_t* row_variant, int32_t* col_variant) {
+int omb_tune_get(const char* device_name, int32_t Nx, int32_t Ny, int32_t* row_variant, int32_t* col_variant,
+                 int32_t* wave_variant) {
   if (!device_name) return fail(OMB_ERR_INVALID_ARG, "device_name is NULL");
   std::lock_guard<std::mutex> lk(g_tune_mu);
   ensure_loaded_locked();
@@ -258,6 +268,7 @@ int omb_tune_get(const char* device_name, int32_t Nx, int32_t Ny, int32_t* row_v
   if (it == g_tune.end()) return fail(OMB_ERR_INVALID_ARG, "no tuned tiles for this device and grid");
   if (row_variant) *row_variant = it->second.row;
   if (col_variant) *col_variant = it->second.col;
+  if (wave_variant) *wave_variant = it->second.wave;
   return OMB_OK;
 }
 

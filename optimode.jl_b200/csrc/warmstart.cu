@@ -3,7 +3,8 @@
 // (Hx, Hy) and effective indices of the lowest four bands, with its training kernels.
 //
 // Network (activations NHWC, BF16 between layers, FP32 accumulation in TMEM):
-//   input  128×128×8  : ε⁻¹ xx, yy, zz, xy, xz, yz (2×2-averaged from 256² grids), ω, 0
+//   input  128×128×8  : ε⁻¹ xx, yy, zz, xy, xz, yz (averaged over 2×2 / 4×4 pixels of 256² / 512²
+//                       grids), ω, 0
 //   L1 3×3/2   8 →  64, ReLU    64×64
 //   L2 3×3/1  64 → 128, ReLU    64×64
 //   L3 3×3/2 128 → 256, ReLU    32×32
@@ -549,8 +550,8 @@ int ws_guesses(omb_warmstart* W, const std::vector<const Problem*>& probs, const
   size_t tot = 0, maxN = 0;
   for (int i = 0; i < n; ++i) {
     const Problem& P = *probs[i];
-    if (!((P.Nx == 128 && P.Ny == 128) || (P.Nx == 256 && P.Ny == 256)))
-      return fail(OMB_ERR_UNSUPPORTED, "learned warm start: 128x128 or 256x256 grids");
+    if (!(P.Nx == P.Ny && (P.Nx == 128 || P.Nx == 256 || P.Nx == 512)))
+      return fail(OMB_ERR_UNSUPPORTED, "learned warm start: 128x128, 256x256 or 512x512 grids");
     col_off[i] = tot;
     tot += 4 * 2 * P.N();
     maxN = std::max(maxN, P.N());
@@ -724,8 +725,8 @@ int omb_warmstart_set_params(omb_warmstart* W, const float* host) {
 int omb_warmstart_features(omb_warmstart* W, const double* d_epsinv, int32_t Nx, int32_t Ny, double omega,
                            void* d_feat, void* stream) {
   if (!W || !d_epsinv || !d_feat) return fail(OMB_ERR_INVALID_ARG, "NULL argument");
-  if (!((Nx == 128 && Ny == 128) || (Nx == 256 && Ny == 256)))
-    return fail(OMB_ERR_UNSUPPORTED, "warm-start network input: 128x128 or 256x256 grids");
+  if (!(Nx == Ny && (Nx == 128 || Nx == 256 || Nx == 512)))
+    return fail(OMB_ERR_UNSUPPORTED, "warm-start network input: 128x128, 256x256 or 512x512 grids");
   cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : W->ctx->stream;
   k_features<<<64, 256, 0, st>>>(d_epsinv, Nx, Ny, omega, static_cast<bf16*>(d_feat));
   OMB_CU(cudaGetLastError());

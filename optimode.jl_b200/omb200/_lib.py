@@ -76,12 +76,11 @@ def load():
             "omb_efield": (ctypes.c_int, [vp, ctypes.c_int, gp, ctypes.c_double, _dp, _dp, _dp]),
             "omb_hfield": (ctypes.c_int, [vp, gp, ctypes.c_double, ctypes.c_int, _dp, _dp]),
             "omb_gram_blocks": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int64, ctypes.c_int32, _dp, _dp, _dp, _dp]),
-            "omb_autotune": (ctypes.c_int, [vp, gp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
-                                            ctypes.POINTER(ctypes.c_int32), _dp]),
+            "omb_autotune": (ctypes.c_int, [vp, gp, ctypes.c_int32] + [ctypes.POINTER(ctypes.c_int32)] * 3 + [_dp]),
             "omb_ctx_set_autotune": (ctypes.c_int, [vp, ctypes.c_int32]),
-            "omb_tune_set": (ctypes.c_int, [ctypes.c_char_p] + [ctypes.c_int32] * 4),
-            "omb_tune_get": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32,
-                                            ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]),
+            "omb_tune_set": (ctypes.c_int, [ctypes.c_char_p] + [ctypes.c_int32] * 5),
+            "omb_tune_get": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32]
+                             + [ctypes.POINTER(ctypes.c_int32)] * 3),
             "omb_tune_clear": (ctypes.c_int, []),
             "omb_tune_save": (ctypes.c_int, [ctypes.c_char_p]),
             "omb_tune_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int32)]),

@@ -125,24 +125,25 @@ def gram_blocks(Z, AZ, precision: str = "fp32", device: int = 0):
 
 def autotune(grid, ncol: int = 4, device: int = 0):
     """Tune the FP32 operator tiles of `grid` now (``omb_autotune``): returns
-    ``(row_variant, col_variant, seconds[3][3])``."""
+    ``(row_variant, col_variant, wave_variant, seconds[3][3][4])``."""
     lib = _lib.load()
     ctx = _lib.context(device)
-    r, c = ctypes.c_int32(), ctypes.c_int32()
-    t = np.zeros(9)
+    r, c, w = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+    t = np.zeros(36)
     _lib.check(lib.omb_autotune(ctx.handle, ctypes.byref(grid.c()), int(ncol), ctypes.byref(r), ctypes.byref(c),
-                                _dptr(t)))
-    return r.value, c.value, t.reshape(3, 3)
+                                ctypes.byref(w), _dptr(t)))
+    return r.value, c.value, w.value, t.reshape(3, 3, 4)
 
 
-def tune_set(device_name: str, Nx: int, Ny: int, row: int, col: int) -> None:
-    _lib.check(_lib.load().omb_tune_set(device_name.encode(), Nx, Ny, row, col))
+def tune_set(device_name: str, Nx: int, Ny: int, row: int, col: int, wave: int = 0) -> None:
+    _lib.check(_lib.load().omb_tune_set(device_name.encode(), Nx, Ny, row, col, wave))
 
 
 def tune_get(device_name: str, Nx: int, Ny: int):
-    r, c = ctypes.c_int32(), ctypes.c_int32()
-    _lib.check(_lib.load().omb_tune_get(device_name.encode(), Nx, Ny, ctypes.byref(r), ctypes.byref(c)))
-    return r.value, c.value
+    r, c, w = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+    _lib.check(_lib.load().omb_tune_get(device_name.encode(), Nx, Ny, ctypes.byref(r), ctypes.byref(c),
+                                        ctypes.byref(w)))
+    return r.value, c.value, w.value
 
 
 def tune_clear() -> None:

@@ -35,7 +35,7 @@ class B200Solver:
       first-order k per band (``OMB_WARM_SWEEP``); ``"cells"``: problems with the same ω
       and grid form a stack of cross-sections (eigenmode expansion); the middle one is solved
       first and the others start from its eigenvectors and k (``OMB_WARM_CELLS``);
-      ``"learned"``: problems on 128² or 256² grids start from the learned network's fields and
+      ``"learned"``: problems on 128², 256² or 512² grids start from the learned network's fields and
       effective indices (``OMB_WARM_LEARNED``; the trained parameters committed with the
       package, or a ``omb200.warmstart.WarmStartNet`` attached by the caller).
     """

@@ -5,7 +5,7 @@ and ``omb_tc_gemm`` in ``include/omb200.h``).
 the tensor cores) and exposes its forward pass, its training step (forward, loss, backward
 and Adam, all in the library's kernels) and its parameters.  Device buffers are torch
 tensors (plumbing only: every operation on them runs in the library).  The network maps
-the ε⁻¹ map and ω of a 128² or 256² cross-section to initial (Hx, Hy) fields and effective
+the ε⁻¹ map and ω of a 128², 256² or 512² cross-section to initial (Hx, Hy) fields and effective
 indices of the four lowest bands; ``omb200.solver`` feeds them to the eigensolver as its
 starting block (``warm_start="learned"``).
 """

@@ -23,6 +23,10 @@ Configurations (the benchmark's cross-sections):
   config1  6×4 μm, 128², Si₃N₄ 1.7×0.7 μm core (ε 3.98) in SiO₂ (2.09), ω = 1/1.55, 2 bands
   config2  8×5 μm, 256², x-cut LiNbO₃ ridge (diag 4.97, 4.61, 4.97), top width 1.5 μm,
            film 0.6 μm, etch 0.3 μm, 70° sidewalls, SiO₂ below, air above, ω = 1/1.55, 4 bands
+  config3_<i>  problem i of the uneven batch (``omb200.workloads.sweep_spec``, seed 3), for the
+           subset on 128² and 192×128 grids with 2–3 bands
+  config5  8×5 μm, 512², the seed-0 slot / coupled-waveguide row (``omb200.workloads``),
+           ω = 1/1.55, 2 bands (k_tol 1e-11, eig_tol 1e-10)
 """
 
 from __future__ import annotations
@@ -67,11 +71,24 @@ def project(probes: np.ndarray, h: np.ndarray) -> list:
     return [[float(x.real), float(x.imag)] for x in v]
 
 
+CONFIG3_SUBSET = [0, 1, 65, 258]  # uneven-batch problems on 128² / 192×128 grids with 2–3 bands
+
+
 def config_inputs(name: str):
-    """(grid dims, ε⁻¹) of a configuration, smoothed by the oracle."""
+    """(grid, nev, ε⁻¹) of a configuration, smoothed by the oracle; also the ω for the
+    uneven-batch subset ("config3_<index>")."""
     import oracle.smoothing as OS
     from omb200 import geometry as G
+    from omb200 import workloads as W
     from omb200.grid import Grid
+    if name.startswith("config3_"):
+        i = int(name.split("_")[1])
+        s = W.sweep_spec()[i]
+        g = Grid(W.CELL[0], W.CELL[1], *s["grid"])
+        return g, s["nev"], W.ridge_epsinv(s["width"], s["core"], g, smoothing="oracle")
+    if name == "config5":
+        g, ei = W.slot_cell(0, 512, smoothing="oracle")
+        return g, 2, ei
     if name == "config1":
         g = Grid(6.0, 4.0, 128, 128)
         shapes, bg = G.si3n4_rect_shapes()
@@ -83,16 +100,25 @@ def config_inputs(name: str):
     return g, nev, OS.smooth_epsinv_constant(shapes, bg, g)
 
 
+def config_omega(name: str) -> float:
+    if name.startswith("config3_"):
+        from omb200 import workloads as W
+        return W.sweep_spec()[int(name.split("_")[1])]["omega"]
+    return OMEGA
+
+
 def solve_case(name: str) -> dict:
     import oracle as O
     g, nev, ei = config_inputs(name)
     og = O.Grid(g.Dx, g.Dy, g.Nx, g.Ny)
+    omega = config_omega(name)
+    tol = (1e-11, 1e-10) if name == "config5" else (1e-12, 1e-11)
     t0 = time.perf_counter()
-    km, kv = O.solve_k(OMEGA, ei, og, nev=nev, k_tol=1e-12, eig_tol=1e-11)
+    km, kv = O.solve_k(omega, ei, og, nev=nev, k_tol=tol[0], eig_tol=tol[1])
     t_solve = time.perf_counter() - t0
     probes = field_probes(2 * g.N)
     out = {
-        "grid": [g.Dx, g.Dy, g.Nx, g.Ny], "omega": OMEGA, "nev": nev,
+        "grid": [g.Dx, g.Dy, g.Nx, g.Ny], "omega": omega, "nev": nev,
         "epsinv_checksum": epsinv_checksum(ei),
         "kmags": [float(k) for k in km],
         "dw2dk": [], "n_g": [], "residuals": [], "field_probes": [],
@@ -102,8 +128,8 @@ def solve_case(name: str) -> dict:
         op = O.Operator(k, ei, og)
         d = 2.0 * op.HMkH(h)
         out["dw2dk"].append(float(d))
-        out["n_g"].append(float(2.0 * OMEGA / d))
-        out["residuals"].append(float(np.linalg.norm(op.M(h) - OMEGA ** 2 * h)))
+        out["n_g"].append(float(2.0 * omega / d))
+        out["residuals"].append(float(np.linalg.norm(op.M(h) - omega ** 2 * h)))
         out["field_probes"].append(project(probes, h))
     if name == "config1":
         rng = np.random.default_rng(0)
@@ -123,7 +149,7 @@ def solve_case(name: str) -> dict:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--only", choices=["config1", "config2"])
+    ap.add_argument("--only", help="config1, config2, config3 (the uneven-batch subset) or config5")
     args = ap.parse_args()
     import oracle as O
     O.maxwell.FFT_WORKERS = os.cpu_count() or 1
@@ -131,8 +157,9 @@ def main():
     if os.path.exists(OUT):
         with open(OUT) as f:
             data = json.load(f)
-    for name in ("config1", "config2"):
-        if args.only and name != args.only:
+    names = ["config1", "config2"] + [f"config3_{i}" for i in CONFIG3_SUBSET] + ["config5"]
+    for name in names:
+        if args.only and not name.startswith(args.only):
             continue
         data[name] = solve_case(name)
         print(name, data[name]["kmags"], f"{data[name]['oracle_seconds']:.1f} s", flush=True)

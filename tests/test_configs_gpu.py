@@ -145,3 +145,52 @@ def test_config2_bench_batch(omb, warm):
             _check_against_gold("config2", g, ei, km, kv, inf["dw2dk"])
             hit += 1
     assert hit == 1
+
+
+def test_config3_subset_uneven_batch(omb):
+    """Four problems of the uneven batch (128² and 192×128 grids, 2–3 bands, LiNbO₃ and Si
+    cores, ω from 0.54 to 0.90) solved together in one batch with other problems of the same
+    sweep groups, against their golden oracle solves."""
+    from golden.make_golden import CONFIG3_SUBSET
+    from omb200 import workloads as W
+    spec = W.sweep_spec()
+    # the subset plus the other members of their sweep groups (on the same ε⁻¹ arrays)
+    groups = {spec[i]["group"] for i in CONFIG3_SUBSET}
+    idx = [i for i, s in enumerate(spec) if s["group"] in groups][:24]
+    idx = sorted(set(idx) | set(CONFIG3_SUBSET))
+    probs = W.sweep_batch(subset=idx, smoothing="oracle")
+    res, info = omb.solve_k_batch(probs, omb.B200Solver(precision="mixed", warm_start="sweep"), return_info=True)
+    for i, pr, (km, kv), inf in zip(idx, probs, res, info):
+        assert np.all(inf["status"] == 0), (i, inf)
+        if i not in CONFIG3_SUBSET:
+            continue
+        name = f"config3_{i}"
+        g = pr["grid"]
+        assert np.allclose(epsinv_checksum_of(pr["eps_inv"]), GOLD[name]["epsinv_checksum"], rtol=1e-12)
+        gold = GOLD[name]
+        og = O.Grid(g.Dx, g.Dy, g.Nx, g.Ny)
+        for b in range(gold["nev"]):
+            assert abs(km[b] - gold["kmags"][b]) <= 1e-9 * gold["kmags"][b], (i, b, km[b], gold["kmags"][b])
+            r = np.linalg.norm(O.Operator(km[b], pr["eps_inv"], og).M(kv[b]) - pr["omega"] ** 2 * kv[b])
+            assert r <= 5e-8
+
+
+def epsinv_checksum_of(ei):
+    from golden.make_golden import epsinv_checksum
+    return epsinv_checksum(ei)
+
+
+def test_config5_large_slot_cell(omb):
+    """The 512² seed-0 slot row, 2 bands, mixed precision, against its golden oracle solve
+    (k relative ≤ 1e-9, residual under the oracle's operator ≤ 5e-8, n_g ≤ 1e-7); then the
+    pull-back of k̄ = 1 on band 0 against the oracle's on the device's modes (ω̄ and ε̄⁻¹
+    within 1e-6)."""
+    g, nev, ei = _inputs("config5")
+    km, kv, info = omb.solve_k(OMEGA, ei, g, omb.B200Solver(precision="mixed"), nev=nev, return_info=True)
+    assert np.all(info["status"] == 0)
+    _check_against_gold("config5", g, ei, km, kv, info["dw2dk"])
+    og = O.Grid(g.Dx, g.Dy, g.Nx, g.Ny)
+    wb, eib = omb.pullback(OMEGA, ei, g, km[:1], kv[:1], [1.0], None)
+    wr, eir = O.solve_k_pullback(OMEGA, ei, og, km[:1], kv[:1], kbar=[1.0], evbar=None)
+    assert abs(wb - wr) <= 1e-6 * abs(wr)
+    assert np.linalg.norm(eib - eir) <= 1e-6 * np.linalg.norm(eir)

@@ -154,8 +154,10 @@ def test_gram_blocks_accuracy(n2, n):
 
 
 def test_tile_variants_agree_and_autotune_picks_one():
-    """Every tile variant of the FP32 M̂ passes gives the same result as the default tiles (the
-    per-pixel arithmetic does not depend on the tile), and the autotuner times all nine."""
+    """Every tile variant of the FP32 M̂ passes gives the default tiles' result (the per-pixel
+    arithmetic does not depend on the tiling); the wave variants (several launches per pass,
+    which only the batched engine's many units reach) give the same eigensolves; the
+    autotuner times all 36 combinations and keeps the fastest."""
     import torch
 
     import omb200
@@ -169,14 +171,20 @@ def test_tile_variants_agree_and_autotune_picks_one():
         ei = OS.smooth_epsinv_constant(shapes, bg, g)
         rng = np.random.default_rng(Nx)
         H = rng.standard_normal((2 * g.N, 3)) + 1j * rng.standard_normal((2 * g.N, 3))
-        ops.tune_set(name, Nx, Ny, 1, 1)
+        ops.tune_set(name, Nx, Ny, 1, 1, 0)
         ref = omb200.apply_M(1.3, ei, g, H, precision="fp32")
         for r in range(3):
             for c in range(3):
-                ops.tune_set(name, Nx, Ny, r, c)
+                ops.tune_set(name, Nx, Ny, r, c, 0)
                 got = omb200.apply_M(1.3, ei, g, H, precision="fp32")
                 assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-6, (Nx, Ny, r, c)
-        r, c, t = ops.autotune(g)
-        assert 0 <= r <= 2 and 0 <= c <= 2 and np.all(t > 0)
-        assert t[r, c] == t.min()
-        assert ops.tune_get(name, Nx, Ny) == (r, c)
+        probs = [{"omega": w, "eps_inv": ei, "grid": g, "nev": 3} for w in (0.62, 0.64, 0.66, 0.68)]
+        ks = []
+        for w in (0, 1, 3):
+            ops.tune_set(name, Nx, Ny, 1, 1, w)
+            res = omb200.solve_k_batch(probs, omb200.B200Solver(precision="mixed"))
+            ks.append(np.array([km for km, _ in res]))
+        assert np.allclose(ks[1], ks[0], rtol=1e-10) and np.allclose(ks[2], ks[0], rtol=1e-10)
+        r, c, w, t = ops.autotune(g)
+        assert np.all(t > 0) and t[r, c, w] == t.min()
+        assert ops.tune_get(name, Nx, Ny) == (r, c, w)
