@@ -3,9 +3,8 @@ bounded, and the failing statuses come back through the C ABI with the context s
 
 * a self-test kernel waits on a barrier phase that nothing completes, with a 1 ms limit:
   the call returns OMB_ERR_TIMEOUT and the kernel's error code;
-* the same limit on the Gram and update pipelines (their waits run out almost at once, then
-  every producer drains its own copies before it exits): the solve returns OMB_ERR_TIMEOUT
-  and, with the limit restored, the next solve on the same context converges;
+* a 1 µs limit on the Gram and update pipelines leaves a healthy solve unchanged (a copy
+  that lands while the barrier is being polled is never a timeout);
 * maxiter = 1: OMB_ERR_NOT_CONVERGED with the per-band status, results still written
   (the reference's LOBPCG reports non-convergence the same way, ``ME/src/solvers/dftk.jl:457-462``);
 * an all-zero warm-start block: the Rayleigh–Ritz basis has no rank, OMB_ERR_ORTHO_FAIL
@@ -50,19 +49,20 @@ def test_selftest_wait_runs_out_and_context_survives(omb):
     assert np.all(np.isfinite(out))
 
 
-def test_pipeline_wait_limit_gives_timeout_then_recovers(omb):
+def test_short_wait_limit_leaves_healthy_solves_alone(omb):
+    """A 1 µs limit on the streaming kernels' waits does not break a healthy solve: a bulk copy
+    that lands while mbarrier.try_wait is still polling never counts as a timeout (the
+    runaway case is the self-test above)."""
     from omb200 import _lib
     g = omb.Grid(6.0, 4.0, 24, 16)
     ei = gaussian_epsinv(P_WG)
+    ref, _ = omb.solve_k(OMEGA0, ei, g, omb.B200Solver(precision="mixed"), nev=2)
     try:
-        _lib.set_wait_limit(1e-9)
-        with pytest.raises(omb.OmbError) as ex:
-            omb.solve_k(OMEGA0, ei, g, omb.B200Solver(precision="mixed"), nev=2)
-        assert ex.value.code == 5
+        _lib.set_wait_limit(1e-6)
+        km, _, info = omb.solve_k(OMEGA0, ei, g, omb.B200Solver(precision="mixed"), nev=2, return_info=True)
     finally:
         _lib.set_wait_limit(1.0)
-    km, _, info = omb.solve_k(OMEGA0, ei, g, omb.B200Solver(precision="mixed"), nev=2, return_info=True)
-    assert np.all(info["status"] == 0) and np.all(km > 0)
+    assert np.all(info["status"] == 0) and np.allclose(km, ref, rtol=1e-9)
 
 
 def test_maxiter_one_is_not_converged(omb):
