@@ -55,7 +55,7 @@ end
 const _PREC = Dict(:fp32 => Int32(0), :fp64 => Int32(1), :mixed => Int32(2))
 const _PRECOND = Dict(:mpb => Int32(1), :diag => Int32(2))
 const _NEWTON = Dict(:inner => Int32(0), :outer => Int32(1))
-const _WARM = Dict(:none => Int32(0), :sweep => Int32(1), :cells => Int32(2))
+const _WARM = Dict(:none => Int32(0), :sweep => Int32(1), :cells => Int32(2), :learned => Int32(3))
 
 """
     B200Solver(; precision=:mixed, preconditioner=:diag, newton=:inner, device=0,
@@ -65,7 +65,9 @@ NVIDIA B200 (sm_100a) backend: batched device LOBPCG with Newton steps on k insi
 iteration, FP32 iterations polished in FP64 to the requested tolerance.  `warm_start=:sweep`
 makes `solve_k_batch` start the instances that share one ε⁻¹ array from the solved instance
 nearest their mean ω (a frequency sweep); `warm_start=:cells` starts instances that share ω
-from the middle one (the cells of an eigenmode expansion, `eme(...; warmstart=true)`).
+from the middle one (the cells of an eigenmode expansion, `eme(...; warmstart=true)`);
+`warm_start=:learned` starts instances on 128², 256² or 512² grids from the learned network
+attached with `b200_attach_warmstart` (fields and n_eff of bands 0..3; same tolerances).
 """
 struct B200Solver{L<:AbstractLogger} <: AbstractEigensolver{L}
     logger::L
@@ -259,3 +261,45 @@ function b200_smooth_epsinv(plan::B200SmoothingPlan, mat_vals::AbstractMatrix{<:
         plan.h, M, size(M, 2), 1, C_NULL, out))
     return out
 end
+
+
+# ---- learned warm start, autotuning and failure-detection controls ----------------------
+# (new API of this backend; the reference has no counterpart)
+
+"""
+    b200_attach_warmstart(params::Vector{Float32}; device=0, batch_cap=32)
+
+Create the warm-start network on `device`, load its FP32 parameters (the layout of
+`omb_warmstart_get_params`: per layer W as [cout × 9·cin] row-major, then the biases; the
+committed `omb200/data/warmstart_net.npz` holds them under "params", readable with NPZ.jl)
+and attach it to the device's context, so `B200Solver(; warm_start=:learned)` uses it.
+"""
+function b200_attach_warmstart(params::Vector{Float32}; device::Int=0, batch_cap::Int=32)
+    n = ccall((:omb_warmstart_num_params, OMB200_LIB), Int64, ())
+    length(params) == n || error("expected $n warm-start parameters, got $(length(params))")
+    ctx = _omb_ctx(B200Solver(; device=device))
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    _omb_check(ccall((:omb_warmstart_create, OMB200_LIB), Cint, (Ptr{Cvoid}, Int32, UInt64, Ref{Ptr{Cvoid}}),
+        ctx, batch_cap, UInt64(0), h))
+    _omb_check(ccall((:omb_warmstart_set_params, OMB200_LIB), Cint, (Ptr{Cvoid}, Ptr{Float32}), h[], params))
+    _omb_check(ccall((:omb_ctx_set_warmstart, OMB200_LIB), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), ctx, h[]))
+    return h[]
+end
+
+"""
+    b200_autotune(grid::Grid{2}; ncol=4, device=0) -> (row, col, wave)
+
+Tune the FP32 operator tiles of `grid` now (batched solves tune unseen grids by themselves,
+like FFTW planning at `ModeSolver` construction, src/maxwell.jl:940-943).
+"""
+function b200_autotune(grid::Grid{2}; ncol::Int=4, device::Int=0)
+    r, c, w = Ref{Int32}(0), Ref{Int32}(0), Ref{Int32}(0)
+    _omb_check(ccall((:omb_autotune, OMB200_LIB), Cint,
+        (Ptr{Cvoid}, Ref{OmbGrid}, Int32, Ref{Int32}, Ref{Int32}, Ref{Int32}, Ptr{Float64}),
+        _omb_ctx(B200Solver(; device=device)), _omb_grid(grid), ncol, r, c, w, C_NULL))
+    return (r[], c[], w[])
+end
+
+"Limit (seconds) of the device's bounded pipeline waits; a wait that runs out is an error."
+b200_set_wait_limit(seconds::Real; device::Int=0) = _omb_check(ccall((:omb_ctx_set_wait_limit, OMB200_LIB), Cint,
+    (Ptr{Cvoid}, Float64), _omb_ctx(B200Solver(; device=device)), Float64(seconds)))
