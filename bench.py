@@ -577,6 +577,31 @@ def main():
                      "what": "one instance, FP64, reference band-by-band Newton loop, same kernels",
                      "seconds": pst["run_seconds"], "converged": pconv}
             pb.close()
+        # the same batch from the other starts: random (none) and the learned network
+        arms = {}
+        for warm in ("none", "learned"):
+            try:
+                ab = omb200.Batch(probs, omb200.B200Solver(precision="mixed", preconditioner="diag", newton="inner",
+                                                           device=local, warm_start=warm))
+                ab.run()
+                ast = ab.stats()
+                _, ainfo = ab.results(return_info=True, raise_on_failure=False)
+                ab.close()
+                aconv = int(sum(int(np.sum(i["status"] == 0)) for i in ainfo))
+                arms[warm] = {"modes_per_s": aconv / ast["run_seconds"], "device_seconds": ast["run_seconds"],
+                              "converged": aconv,
+                              "iterations_mean": float(np.mean([x for i in ainfo for x in i["iterations"]]))}
+            except Exception as exc:  # e.g. no trained parameters in this checkout
+                arms[warm] = {"unavailable": str(exc)[:200]}
+        arms["sweep"] = {"modes_per_s": value, "device_seconds": max_dev_s / args.steps,
+                         "converged": converged_all / args.steps,
+                         "iterations_mean": float(np.mean([x for i in info for x in i["iterations"]]))}
+        from omb200 import ops as _ops
+        try:
+            tuned = dict(zip(("row", "col", "wave"), _ops.tune_get(torch.cuda.get_device_name(local), NX, NY)))
+        except Exception:
+            tuned = None
+        roofline["tuned_tiles"] = tuned
         cpu, errors = (None, None) if args.no_cpu_baseline or world > 1 else cpu_baseline_and_errors(probs, res, info)
         smoothing = None if args.no_smoothing else smoothing_measure(local, nsets=args.smoothing_sets)
         out = {
@@ -598,6 +623,7 @@ def main():
             "gpu_launches": int(kernels),
             "roofline": roofline,
             "plain_fp64_single": plain,
+            "warm_start_arms": arms,
             "smoothing": smoothing,
             "cpu_baseline": cpu,
             "errors_vs_oracle": errors,
