@@ -57,6 +57,14 @@ typedef struct {
   double Dx, Dy;
 } omb_grid;
 
+/* A 3D cell periodic along z (reference `Grid{3}`, grid.jl:46-76): Dx × Dy μm on Nx × Ny
+ * pixels in the cross-section and Nz slabs over the period Dz = Λ (Nz a supported length, at
+ * least 8). */
+typedef struct {
+  int32_t Nx, Ny, Nz;
+  double Dx, Dy, Dz;
+} omb_grid3;
+
 /* Library version (major*10000 + minor*100 + patch). */
 int omb_version(void);
 /* 1 when n is a supported grid length, else 0. */
@@ -92,6 +100,14 @@ int omb_apply(omb_ctx* ctx, int op, int precision, const omb_grid* grid, double 
  * Replaces HMₖH (maxwell.jl:267-275) / _gpu_HMkH (gpu.jl:171-180). */
 int omb_HMkH(omb_ctx* ctx, int precision, const omb_grid* grid, double k,
              const double* epsinv, int ncol, const double* H, double* out);
+
+/* The same on a z-periodic cell: epsinv (3, 3, Nx, Ny, Nz) Float64, columns ComplexF64
+ * (2, Nx, Ny, Nz); w = k ẑ − G with G = (gx, gy, m/Λ) (the 3D forms of maxwell.jl's
+ * kx_tc/kx_ct/mag_mn, 3D FFTs).  op: OMB_OP_M or OMB_OP_P. */
+int omb_apply3(omb_ctx* ctx, int op, int precision, const omb_grid3* grid, double k, const double* epsinv, int ncol,
+               const double* H_in, double* H_out);
+int omb_HMkH3(omb_ctx* ctx, int precision, const omb_grid3* grid, double k, const double* epsinv, int ncol,
+              const double* H, double* out);
 
 /* Un-normalised, un-canonicalised E = ε⁻¹·fft(kx_tc H) for one column.
  * Replaces E⃗(k, evec, ε⁻¹, ∂ε_∂ω, grid; canonicalize=false, normalized=false)
@@ -240,6 +256,17 @@ int omb_solve_omega2(omb_ctx* ctx, const omb_grid* grid, double k, const double*
                      const double* Hguess, int nguess, const omb_options* opt, double* evals,
                      double* evecs, double* residuals, int32_t* status);
 
+/* Propagation constants and Bloch modes of the lowest `nev` bands of a cell periodic along z
+ * with period Λ = grid->Dz, at frequency ω.  Replaces solve_k_periodic(ω, ε⁻¹, Λ, grid,
+ * solver; nev) (lib/MaxwellEigenmodes/src/grads/period.jl:108-112): solve_k on the grid whose
+ * z-extent is Λ, here with the same device iteration as omb_solve_k (inner Newton, mixed /
+ * FP64 precision, phase-canonicalised unit eigenvectors).  epsinv (3, 3, Nx, Ny, Nz), evecs
+ * nev columns ComplexF64 (2, Nx, Ny, Nz); kguess ≤ 0 → ω/√(min diag ε⁻¹); any output but
+ * kmags may be NULL. */
+int omb_solve_k_periodic(omb_ctx* ctx, const omb_grid3* grid, double omega, const double* epsinv, int nev,
+                         double kguess, const omb_options* opt, double* kmags, double* evecs, double* residuals,
+                         double* dw2dk, int32_t* status, int32_t* iterations);
+
 /* Adjoint pull-back of one solve_k result: cotangents (k̄, ē) of (kmags, evecs) → ω̄ and
  * ε̄⁻¹ (and optionally ε̄ = ∂/∂ε).  Replaces the pullback closure of
  * rrule(solve_k, ω, ε⁻¹, grid, solver) (lib/MaxwellEigenmodes/src/solve.jl:213-289; GPU
@@ -255,6 +282,17 @@ int omb_pullback(omb_ctx* ctx, const omb_grid* grid, double omega, const double*
                  const double* kmags, const double* evecs, const double* kbar, const double* evbar,
                  const omb_options* opt, double* omega_bar, double* epsinv_bar, double* eps_bar,
                  int32_t* iterations);
+
+/* The same pull-back for omb_solve_k_periodic's outputs on a z-periodic cell (Nz ≥ 8):
+ * cotangents (k̄, ē) → ω̄, ε̄⁻¹ (3, 3, Nx, Ny, Nz) and the period cotangent Λ̄ (L_bar, may be
+ * NULL).  Replaces _solve_k_period_grads (lib/MaxwellEigenmodes/src/grads/period.jl:136-200):
+ * Λ̄ = Σ_bands [Λ̄ₕ + (k̄ + k̄ₕ)·(−∂ω²/∂Λ ÷ ∂ω²/∂k)], ∂ω²/∂Λ = 2⟨h|∂M̂/∂Λ|h⟩ with the ẑ× action
+ * weighted by g_z/Λ per plane wave (HMₖH_weighted, period.jl:69-74), and Λ̄ₕ the same
+ * per-plane-wave terms as the eigenvector channel's k̄ₕ weighted by g_z/Λ (period.jl:171-175). */
+int omb_pullback_periodic(omb_ctx* ctx, const omb_grid3* grid, double omega, const double* epsinv, int nev,
+                          const double* kmags, const double* evecs, const double* kbar, const double* evbar,
+                          const omb_options* opt, double* omega_bar, double* epsinv_bar, double* L_bar,
+                          int32_t* iterations);
 
 /* ---------------------------------------------------------------------------------
  * Staged batches: the same solve as omb_solve_k split into its host→device, device and

@@ -70,28 +70,33 @@ __device__ __forceinline__ void block_reduce4(double a, double b, double c, doub
   }
 }
 
-__device__ __forceinline__ double prec_scale(long long row, int Nx, int Ny, double inv_dx, double inv_dy, double k,
-                                             double eps_mean) {
-  const long long p = row >> 1;
-  const int ix = (int)(p % Nx), iy = (int)(p / Nx);
-  const double gx = freq_index(ix, Nx) * inv_dx, gy = freq_index(iy, Ny) * inv_dy;
-  return eps_mean / (gx * gx + gy * gy + k * k);
-}
-
 struct AdjVecs {
   double2 *x, *v, *w, *w2, *r1, *r2, *y, *Av;
   const double2* e;  // unit eigenvector (deflation direction)
   long long n2;
   int Nx, Ny;
   double inv_dx, inv_dy, k, eps_mean;
+  int Nz;            // z-periodic cells (1 for a 2D cell)
+  double inv_dz;
 };
+
+// Diagonal preconditioner ⟨ε⟩/|w|² at row `row` (w = k ẑ − G; g_z of the row's slab)
+__device__ __forceinline__ double prec_scale(long long row, const AdjVecs& V) {
+  const long long p = row >> 1;
+  const int ix = (int)(p % V.Nx);
+  const long long rest = p / V.Nx;
+  const int iy = (int)(rest % V.Ny), iz = (int)(rest / V.Ny);
+  const double gx = freq_index(ix, V.Nx) * V.inv_dx, gy = freq_index(iy, V.Ny) * V.inv_dy;
+  const double wz = V.k - freq_index(iz, V.Nz) * V.inv_dz;
+  return V.eps_mean / (gx * gx + gy * gy + wz * wz);
+}
 
 // init: r1 = r2 = b, z = P b, partials ⟨e,z⟩, ⟨b,z⟩ (y holds z)
 __global__ void __launch_bounds__(ADJ_NT) k_minres_init(AdjVecs V, const double2* __restrict__ b, double* part) {
   double er = 0, ei = 0, br = 0, bi = 0;
   for (long long i = blockIdx.x * (long long)ADJ_NT + threadIdx.x; i < V.n2; i += (long long)gridDim.x * ADJ_NT) {
     const double2 bb = b[i];
-    const double s = prec_scale(i, V.Nx, V.Ny, V.inv_dx, V.inv_dy, V.k, V.eps_mean);
+    const double s = prec_scale(i, V);
     const double2 z = make_double2(bb.x * s, bb.y * s);
     V.r1[i] = bb; V.r2[i] = bb; V.y[i] = z;
     V.x[i] = make_double2(0, 0); V.w[i] = make_double2(0, 0); V.w2[i] = make_double2(0, 0);
@@ -164,7 +169,7 @@ __global__ void __launch_bounds__(ADJ_NT) k_minres_b(AdjVecs V, const MinresStat
     const double2 yn = make_double2(y.x - (er0 * e.x - ei0 * e.y) - c2 * r2.x, y.y - (er0 * e.y + ei0 * e.x) - c2 * r2.y);
     V.r1[i] = r2;
     V.r2[i] = yn;
-    const double s = prec_scale(i, V.Nx, V.Ny, V.inv_dx, V.inv_dy, V.k, V.eps_mean);
+    const double s = prec_scale(i, V);
     const double2 z = make_double2(yn.x * s, yn.y * s);
     V.y[i] = z;
     er += e.x * z.x + e.y * z.y; ei += e.x * z.y - e.y * z.x;
@@ -262,16 +267,22 @@ __global__ void __launch_bounds__(ADJ_NT) k_sub_proj(const double2* __restrict__
 }
 
 // k̄ₕ partials from ẽ = EC/N, λ̃e = ED/N (planar), h and λ (interleaved), basis at k
+// (z-periodic cells: the basis at k − g_z, and beside k̄ₕ's sum the same per-plane-wave terms
+// weighted by g_z/Λ, whose negative is the eigenvector channel's period cotangent Λ̄_H,
+// lib/MaxwellEigenmodes/src/grads/period.jl:113-117, 171-175)
 __global__ void __launch_bounds__(ADJ_NT) k_adj_kbar(const double2* __restrict__ EC, const double2* __restrict__ ED,
                                                      const double2* __restrict__ h, const double2* __restrict__ lam,
-                                                     int Nx, int Ny, double inv_dx, double inv_dy, double k,
-                                                     double* part) {
-  const long long N = (long long)Nx * Ny;
+                                                     int Nx, int Ny, int Nz, double inv_dx, double inv_dy,
+                                                     double inv_dz, double k, double* part) {
+  const long long N = (long long)Nx * Ny * Nz;
   const double sN = 1.0 / (double)N;
-  double acc = 0;
+  double acc = 0, accL = 0;
   for (long long p = blockIdx.x * (long long)ADJ_NT + threadIdx.x; p < N; p += (long long)gridDim.x * ADJ_NT) {
-    const int ix = (int)(p % Nx), iy = (int)(p / Nx);
-    const Basis<double> B = basis_at<double>(k, freq_index(ix, Nx) * inv_dx, freq_index(iy, Ny) * inv_dy);
+    const int ix = (int)(p % Nx);
+    const long long rest = p / Nx;
+    const int iy = (int)(rest % Ny), iz = (int)(rest / Ny);
+    const double gz = freq_index(iz, Nz) * inv_dz;
+    const Basis<double> B = basis_at<double>(k - gz, freq_index(ix, Nx) * inv_dx, freq_index(iy, Ny) * inv_dy);
     const double m[3] = {B.mx, B.my, B.mz}, n[3] = {B.nx, B.ny, 0.0};
     const double2 h1 = h[2 * p], h2 = h[2 * p + 1], l1 = lam[2 * p], l2 = lam[2 * p + 1];
     double km[3], kn[3];
@@ -292,8 +303,9 @@ __global__ void __launch_bounds__(ADJ_NT) k_adj_kbar(const double2* __restrict__
     const double kmm = -(km[0] * mq[0] + km[1] * mq[1] + km[2] * mq[2]) * B.mag;  // m̄ = kx̄_m·mag
     const double knn = -(kn[0] * nq[0] + kn[1] * nq[1] + kn[2] * nq[2]) * B.mag;
     acc += kmag + kmm + knn;
+    accL += (kmag + kmm + knn) * gz * inv_dz;
   }
-  block_reduce4(acc, 0, 0, 0, part);
+  block_reduce4(acc, accL, 0, 0, part);
 }
 
 // ε̄⁻¹ (6 unique entries) += ε⁻¹_bar(d, lt), d = D0/N, lt = Λd + s·D0
@@ -344,23 +356,14 @@ __global__ void __launch_bounds__(ADJ_NT) k_adj_expand(const double* __restrict_
 
 using namespace omb;
 
-extern "C" int omb_pullback(omb_ctx* ctx, const omb_grid* grid, double omega, const double* epsinv, int nev,
-                            const double* kmags, const double* evecs, const double* kbar, const double* evbar,
-                            const omb_options* opt, double* omega_bar, double* epsinv_bar, double* eps_bar,
-                            int32_t* iterations) {
-  if (!ctx) return fail(OMB_ERR_INVALID_ARG, "ctx is NULL");
-  if (nev <= 0 || !kmags || !evecs || !omega_bar || !epsinv_bar)
-    return fail(OMB_ERR_INVALID_ARG, "need nev > 0 and non-NULL kmags, evecs, omega_bar, epsinv_bar");
-  if (!(omega > 0) || !std::isfinite(omega)) return fail(OMB_ERR_INVALID_ARG, "omega must be finite and positive");
-  omb_options dflt;
-  omb_options_default(&dflt);
-  const omb_options& O = opt ? *opt : dflt;
-  OMB_CU(cudaSetDevice(ctx->device));
-  Problem P;
-  int rc = upload_problem(ctx, grid, epsinv, P);
-  if (rc) return rc;
+// The pull-back on an uploaded problem; Nz > 1 is a z-periodic cell, for which L_bar (when
+// non-NULL) receives the period cotangent Λ̄ (lib/MaxwellEigenmodes/src/grads/period.jl:136-200).
+static int pullback_impl(omb_ctx* ctx, Problem& P, double omega, int nev, const double* kmags, const double* evecs,
+                         const double* kbar, const double* evbar, const omb_options& O, double* omega_bar,
+                         double* epsinv_bar, double* eps_bar, double* L_bar, int32_t* iterations) {
   cudaStream_t st = ctx->stream;
   const long long N = (long long)P.N(), n2 = 2 * N;
+  const bool periodic = P.Nz > 1;
   // device buffers
   DevBuf<double2> vecs, scr, ev, eb, lamv;
   OMB_CU(vecs.alloc(8 * n2, st));   // x v w w2 r1 r2 y Av
@@ -373,14 +376,14 @@ extern "C" int omb_pullback(omb_ctx* ctx, const omb_grid* grid, double omega, co
   OMB_CU(eib.alloc(6 * N, st));
   OMB_CU(eib.zero());
   OMB_CU(kd.alloc(1, st));
-  const int rb = row_blocks(P.Nx, P.Ny);
+  const int rb = row_blocks(P.Nx, P.Ny) * P.Nz;  // HMₖH partials: row blocks of every slab
   OMB_CU(hpart.alloc(2 * rb, st));
   OMB_CU(hred.alloc(2, st));
   DevBuf<MinresState> S;
   OMB_CU(S.alloc(1, st));
   double2* vb = vecs.p;
   AdjVecs V{vb, vb + n2, vb + 2 * n2, vb + 3 * n2, vb + 4 * n2, vb + 5 * n2, vb + 6 * n2, vb + 7 * n2, ev.p,
-            n2, P.Nx, P.Ny, 1.0 / P.Dx, 1.0 / P.Dy, 0.0, P.eps_mean};
+            n2, P.Nx, P.Ny, 1.0 / P.Dx, 1.0 / P.Dy, 0.0, P.eps_mean, P.Nz, 1.0 / P.Dz};
   double2* SA = scr.p;              // D0 = fft(kx_tc h)
   double2* SB = SA + 3 * N;         // Λd = fft(kx_tc λ)
   double2* SC = SB + 3 * N;         // copies consumed by the D2E passes
@@ -394,30 +397,49 @@ extern "C" int omb_pullback(omb_ctx* ctx, const omb_grid* grid, double omega, co
     u.in_cs = n2; u.out_cs = n2; u.scr_cs = 3 * N; u.ncol = 1;
     return u;
   };
-  OpUnit<double> hu[7] = {unit(V.v, V.Av, SC), unit(ev.p, nullptr, SC), unit(ev.p, nullptr, SA),
-                          unit(V.x, nullptr, SB), unit(nullptr, EC, SC), unit(nullptr, ED, SD), {}};
+  // (unit 6: HMₖH with the ẑ× action weighted by g_z/Λ, for ∂ω²/∂Λ)
+  OpUnit<double> hu[7] = {unit(V.v, V.Av, SC),   unit(ev.p, nullptr, SC), unit(ev.p, nullptr, SA),
+                          unit(V.x, nullptr, SB), unit(nullptr, EC, SC),   unit(nullptr, ED, SD),
+                          unit(ev.p, nullptr, SC)};
   hu[4].out_cs = 3 * N;
   hu[5].out_cs = 3 * N;
-  DevBuf<OpUnit<double>> du;
-  OMB_CU(du.alloc(6, st));
-  OMB_CU(cudaMemcpyAsync(du.p, hu, 6 * sizeof(OpUnit<double>), cudaMemcpyHostToDevice, st));
+  hu[6].zx_weight_gz = 1;
+  DevBuf<OpUnit<double>> du, dexp;
+  OMB_CU(du.alloc(7, st));
+  OMB_CU(cudaMemcpyAsync(du.p, hu, 7 * sizeof(OpUnit<double>), cudaMemcpyHostToDevice, st));
+  if (periodic) OMB_CU(dexp.alloc(P.Nz + 1, st));
   const TwTables& tw = ctx->tw;
-  double wbar = 0.0;
+  auto run = [&](OpKind kind, int u) -> cudaError_t {
+    return periodic ? launch_op3d<double>(kind, du.p + u, 1, P.Nx, P.Ny, P.Nz, 1, tw, dexp.p, st)
+                    : launch_op<double>(kind, du.p + u, 1, P.Nx, P.Ny, 1, tw, st);
+  };
+  // ⟨h|∂M̂|h⟩ with unit u (the device partials hold Re⟨h|kx_ct(…)⟩ = −HMₖH)
+  auto hmkh = [&](int u, double& out) -> cudaError_t {
+    cudaError_t e = run(OP_HMKH, u);
+    if (e != cudaSuccess) return e;
+    k_reduce_partials<<<1, 256, 0, st>>>(hpart.p, rb, 1, hred.p);
+    e = cudaGetLastError();
+    double hh[2];
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hh, hred.p, sizeof(hh), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    out = -hh[0];
+    return e;
+  };
+  double wbar = 0.0, Lbar = 0.0;
   for (int b = 0; b < nev; ++b) {
     const double kb = kmags[b];
     if (!(kb > 0) || !std::isfinite(kb)) return fail(OMB_ERR_INVALID_ARG, "kmags must be finite and positive");
     V.k = kb;
     OMB_CU(cudaMemcpyAsync(kd.p, &kb, sizeof(double), cudaMemcpyHostToDevice, st));
     OMB_CU(cudaMemcpyAsync(ev.p, evecs + 4 * N * (size_t)b, n2 * sizeof(double2), cudaMemcpyHostToDevice, st));
-    // ∂ω²/∂k = 2⟨h|∂M̂/∂k|h⟩
-    OMB_CU(launch_op<double>(OP_HMKH, du.p + 1, 1, P.Nx, P.Ny, 1, tw, st));
-    k_reduce_partials<<<1, 256, 0, st>>>(hpart.p, rb, 1, hred.p);
-    OMB_CU(cudaGetLastError());
-    double hh[2];
-    OMB_CU(cudaMemcpyAsync(hh, hred.p, sizeof(hh), cudaMemcpyDeviceToHost, st));
-    OMB_CU(cudaStreamSynchronize(st));
-    const double dw2dk = 2.0 * (-hh[0]);
+    // ∂ω²/∂k = 2⟨h|∂M̂/∂k|h⟩ and, on a periodic cell, ∂ω²/∂Λ = 2⟨h|∂M̂/∂Λ|h⟩ (period.jl:150-151)
+    double hk = 0, hL = 0;
+    OMB_CU(hmkh(1, hk));
+    const double dw2dk = 2.0 * hk;
     if (!(dw2dk > 0) || !std::isfinite(dw2dk)) return fail(OMB_ERR_NAN, "non-positive ∂ω²/∂k in the pull-back");
+    if (periodic && L_bar) OMB_CU(hmkh(6, hL));
+    const double dw2dL = 2.0 * hL;
+    double Lbar_h = 0.0;
     const double kb_bar = kbar ? kbar[b] : 0.0;
     double kbar_h = 0.0;
     const double* eb_host = evbar ? evbar + 4 * N * (size_t)b : nullptr;
@@ -425,7 +447,7 @@ extern "C" int omb_pullback(omb_ctx* ctx, const omb_grid* grid, double omega, co
     if (eb_host)
       for (long long i = 0; i < 2 * n2 && !have_eb; ++i) have_eb = eb_host[i] != 0.0;
     // D0 = fft(kx_tc h) into SA
-    OMB_CU(launch_op<double>(OP_H2D, du.p + 2, 1, P.Nx, P.Ny, 1, tw, st));
+    OMB_CU(run(OP_H2D, 2));
     if (have_eb) {
       // b = ē − h⟨h,ē⟩
       OMB_CU(cudaMemcpyAsync(eb.p, eb_host, n2 * sizeof(double2), cudaMemcpyHostToDevice, st));
@@ -443,7 +465,7 @@ extern "C" int omb_pullback(omb_ctx* ctx, const omb_grid* grid, double omega, co
       OMB_CU(cudaGetLastError());
       // one MINRES iteration; 8 per graph replay, host checks the flag between replays
       auto iter = [&]() -> cudaError_t {
-        cudaError_t e = launch_op<double>(OP_M, du.p + 0, 1, P.Nx, P.Ny, 1, tw, st);
+        cudaError_t e = run(OP_M, 0);
         if (e != cudaSuccess) return e;
         k_minres_a<<<nb, ADJ_NT, 0, st>>>(V, S.p, part.p);
         k_minres_a_scalar<<<1, 32, 0, st>>>(S.p, part.p, nb);
@@ -481,20 +503,25 @@ extern "C" int omb_pullback(omb_ctx* ctx, const omb_grid* grid, double omega, co
       k_dot_e<<<nb, ADJ_NT, 0, st>>>(ev.p, V.x, n2, part.p);
       k_sub_proj<<<nb, ADJ_NT, 0, st>>>(ev.p, V.x, n2, part.p, nb);
       OMB_CU(cudaGetLastError());
-      OMB_CU(launch_op<double>(OP_H2D, du.p + 3, 1, P.Nx, P.Ny, 1, tw, st));
+      OMB_CU(run(OP_H2D, 3));
       // ẽ·N and λ̃e·N through the D2E passes on copies (the passes work in place)
       OMB_CU(cudaMemcpyAsync(SC, SA, 3 * N * sizeof(double2), cudaMemcpyDeviceToDevice, st));
       OMB_CU(cudaMemcpyAsync(SD, SB, 3 * N * sizeof(double2), cudaMemcpyDeviceToDevice, st));
-      OMB_CU(launch_op<double>(OP_D2E, du.p + 4, 1, P.Nx, P.Ny, 1, tw, st));
-      OMB_CU(launch_op<double>(OP_D2E, du.p + 5, 1, P.Nx, P.Ny, 1, tw, st));
-      k_adj_kbar<<<nb, ADJ_NT, 0, st>>>(EC, ED, ev.p, V.x, P.Nx, P.Ny, 1.0 / P.Dx, 1.0 / P.Dy, kb, part.p);
+      OMB_CU(run(OP_D2E, 4));
+      OMB_CU(run(OP_D2E, 5));
+      k_adj_kbar<<<nb, ADJ_NT, 0, st>>>(EC, ED, ev.p, V.x, P.Nx, P.Ny, P.Nz, 1.0 / P.Dx, 1.0 / P.Dy, 1.0 / P.Dz, kb,
+                                        part.p);
       OMB_CU(cudaGetLastError());
       std::vector<double> hp(4 * nb);
       OMB_CU(cudaMemcpyAsync(hp.data(), part.p, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
       OMB_CU(cudaStreamSynchronize(st));
-      double acc = 0;
-      for (int i = 0; i < nb; ++i) acc += hp[4 * i];
+      double acc = 0, accL = 0;
+      for (int i = 0; i < nb; ++i) {
+        acc += hp[4 * i];
+        accL += hp[4 * i + 1];
+      }
       kbar_h = -acc;
+      Lbar_h = -accL;
     } else {
       if (iterations) iterations[b] = 0;
       OMB_CU(cudaMemsetAsync(SB, 0, 3 * N * sizeof(double2), st));
@@ -503,6 +530,7 @@ extern "C" int omb_pullback(omb_ctx* ctx, const omb_grid* grid, double omega, co
     k_adj_eibar<<<nb, ADJ_NT, 0, st>>>(SA, SB, N, s, eib.p);
     OMB_CU(cudaGetLastError());
     wbar += 2.0 * omega * s;
+    Lbar += Lbar_h + (kb_bar + kbar_h) * (-dw2dL / dw2dk);
   }
   DevBuf<double> oei, oe;
   OMB_CU(oei.alloc(9 * N, st));
@@ -513,5 +541,50 @@ extern "C" int omb_pullback(omb_ctx* ctx, const omb_grid* grid, double omega, co
   if (eps_bar) OMB_CU(cudaMemcpyAsync(eps_bar, oe.p, 9 * N * sizeof(double), cudaMemcpyDeviceToHost, st));
   OMB_CU(cudaStreamSynchronize(st));
   *omega_bar = wbar;
+  if (L_bar) *L_bar = Lbar;
   return OMB_OK;
+}
+
+static int pullback_args(omb_ctx* ctx, double omega, int nev, const double* kmags, const double* evecs,
+                         double* omega_bar, double* epsinv_bar) {
+  if (!ctx) return fail(OMB_ERR_INVALID_ARG, "ctx is NULL");
+  if (nev <= 0 || !kmags || !evecs || !omega_bar || !epsinv_bar)
+    return fail(OMB_ERR_INVALID_ARG, "need nev > 0 and non-NULL kmags, evecs, omega_bar, epsinv_bar");
+  if (!(omega > 0) || !std::isfinite(omega)) return fail(OMB_ERR_INVALID_ARG, "omega must be finite and positive");
+  return OMB_OK;
+}
+
+extern "C" int omb_pullback(omb_ctx* ctx, const omb_grid* grid, double omega, const double* epsinv, int nev,
+                            const double* kmags, const double* evecs, const double* kbar, const double* evbar,
+                            const omb_options* opt, double* omega_bar, double* epsinv_bar, double* eps_bar,
+                            int32_t* iterations) {
+  int rc = pullback_args(ctx, omega, nev, kmags, evecs, omega_bar, epsinv_bar);
+  if (rc) return rc;
+  omb_options dflt;
+  omb_options_default(&dflt);
+  OMB_CU(cudaSetDevice(ctx->device));
+  Problem P;
+  rc = upload_problem(ctx, grid, epsinv, P);
+  if (rc) return rc;
+  return pullback_impl(ctx, P, omega, nev, kmags, evecs, kbar, evbar, opt ? *opt : dflt, omega_bar, epsinv_bar,
+                       eps_bar, nullptr, iterations);
+}
+
+extern "C" int omb_pullback_periodic(omb_ctx* ctx, const omb_grid3* grid, double omega, const double* epsinv,
+                                     int nev, const double* kmags, const double* evecs, const double* kbar,
+                                     const double* evbar, const omb_options* opt, double* omega_bar,
+                                     double* epsinv_bar, double* L_bar, int32_t* iterations) {
+  int rc = pullback_args(ctx, omega, nev, kmags, evecs, omega_bar, epsinv_bar);
+  if (rc) return rc;
+  if (!grid) return fail(OMB_ERR_INVALID_ARG, "grid is NULL");
+  if (grid->Nz < 8) return fail(OMB_ERR_UNSUPPORTED, "a z-periodic cell needs Nz >= 8 slabs (a supported length)");
+  omb_options dflt;
+  omb_options_default(&dflt);
+  OMB_CU(cudaSetDevice(ctx->device));
+  Problem P;
+  const omb_grid g2{grid->Nx, grid->Ny, grid->Dx, grid->Dy};
+  rc = upload_problem(ctx, &g2, epsinv, P, grid->Nz, grid->Dz);
+  if (rc) return rc;
+  return pullback_impl(ctx, P, omega, nev, kmags, evecs, kbar, evbar, opt ? *opt : dflt, omega_bar, epsinv_bar,
+                       nullptr, L_bar, iterations);
 }

@@ -45,6 +45,20 @@ static int to_host(omb_ctx* ctx, const cplx<T>* d, size_t n, double* h) {
   return OMB_OK;
 }
 
+// One unit through a pipeline on a 2D or z-periodic cell.
+template <typename T>
+static int launch_cell(OpKind op, const OpUnit<T>* du, const Problem& P, int ncol, omb_ctx* ctx, cudaStream_t st) {
+  if (P.Nz > 1) {
+    DevBuf<OpUnit<T>> ex;
+    OMB_CU(ex.alloc((size_t)P.Nz + 1, st));
+    OMB_CU(launch_op3d<T>(op, du, 1, P.Nx, P.Ny, P.Nz, ncol, ctx->tw, ex.p, st));
+    OMB_CU(cudaStreamSynchronize(st));  // ex is released at return
+    return OMB_OK;
+  }
+  OMB_CU(launch_op<T>(op, du, 1, P.Nx, P.Ny, ncol, ctx->tw, st));
+  return OMB_OK;
+}
+
 template <typename T>
 static int run_apply(omb_ctx* ctx, int op, const Problem& P, double k, int ncol, const double* Hin, double* Hout) {
   const size_t N = P.N(), n = 2 * N * (size_t)ncol;
@@ -69,7 +83,8 @@ static int run_apply(omb_ctx* ctx, int op, const Problem& P, double k, int ncol,
     DevBuf<OpUnit<T>> du;
     OMB_CU(du.alloc(1, st));
     OMB_CU(cudaMemcpyAsync(du.p, &u, sizeof(u), cudaMemcpyHostToDevice, st));
-    OMB_CU(launch_op<T>(op == OMB_OP_M ? OP_M : OP_P, du.p, 1, P.Nx, P.Ny, ncol, ctx->tw, st));
+    rc = launch_cell<T>(op == OMB_OP_M ? OP_M : OP_P, du.p, P, ncol, ctx, st);
+    if (rc) return rc;
   }
   return to_host<T>(ctx, hout.p, n, Hout);
 }
@@ -84,7 +99,7 @@ static int run_hmkh(omb_ctx* ctx, const Problem& P, double k, int ncol, const do
   if (rc) return rc;
   OMB_CU(scr.alloc(3 * N * (size_t)ncol, st));
   DevBuf<double> kd, part, red;
-  const int nb = row_blocks(P.Nx, P.Ny);
+  const int nb = row_blocks(P.Nx, P.Ny) * P.Nz;
   OMB_CU(kd.alloc(1, st));
   OMB_CU(part.alloc(2 * (size_t)nb * ncol, st));
   OMB_CU(red.alloc(2 * (size_t)ncol, st));
@@ -95,7 +110,8 @@ static int run_hmkh(omb_ctx* ctx, const Problem& P, double k, int ncol, const do
   DevBuf<OpUnit<T>> du;
   OMB_CU(du.alloc(1, st));
   OMB_CU(cudaMemcpyAsync(du.p, &u, sizeof(u), cudaMemcpyHostToDevice, st));
-  OMB_CU(launch_op<T>(OP_HMKH, du.p, 1, P.Nx, P.Ny, ncol, ctx->tw, st));
+  rc = launch_cell<T>(OP_HMKH, du.p, P, ncol, ctx, st);
+  if (rc) return rc;
   k_reduce_partials<<<ncol, 256, 0, st>>>(part.p, nb, ncol, red.p);
   OMB_CU(cudaGetLastError());
   std::vector<double> h(2 * (size_t)ncol);
@@ -231,6 +247,35 @@ int omb_apply(omb_ctx* ctx, int op, int precision, const omb_grid* grid, double 
   if (rc) return rc;
   return precision == OMB_PREC_FP64 ? run_apply<double>(ctx, op, P, k, ncol, H_in, H_out)
                                     : run_apply<float>(ctx, op, P, k, ncol, H_in, H_out);
+}
+
+int omb_apply3(omb_ctx* ctx, int op, int precision, const omb_grid3* grid, double k, const double* epsinv, int ncol,
+               const double* H_in, double* H_out) {
+  int rc = check_common(ctx, precision, k);
+  if (rc) return rc;
+  if (!grid) return fail(OMB_ERR_INVALID_ARG, "grid is NULL");
+  if (op != OMB_OP_M && op != OMB_OP_P) return fail(OMB_ERR_INVALID_ARG, "op must be OMB_OP_M or OMB_OP_P");
+  if (ncol <= 0 || !H_in || !H_out) return fail(OMB_ERR_INVALID_ARG, "need ncol > 0 and non-NULL H_in, H_out");
+  const omb_grid g2{grid->Nx, grid->Ny, grid->Dx, grid->Dy};
+  Problem P;
+  rc = upload_problem(ctx, &g2, epsinv, P, grid->Nz, grid->Dz);
+  if (rc) return rc;
+  return precision == OMB_PREC_FP64 ? run_apply<double>(ctx, op, P, k, ncol, H_in, H_out)
+                                    : run_apply<float>(ctx, op, P, k, ncol, H_in, H_out);
+}
+
+int omb_HMkH3(omb_ctx* ctx, int precision, const omb_grid3* grid, double k, const double* epsinv, int ncol,
+              const double* H, double* out) {
+  int rc = check_common(ctx, precision, k);
+  if (rc) return rc;
+  if (!grid) return fail(OMB_ERR_INVALID_ARG, "grid is NULL");
+  if (ncol <= 0 || !H || !out) return fail(OMB_ERR_INVALID_ARG, "need ncol > 0 and non-NULL H, out");
+  const omb_grid g2{grid->Nx, grid->Ny, grid->Dx, grid->Dy};
+  Problem P;
+  rc = upload_problem(ctx, &g2, epsinv, P, grid->Nz, grid->Dz);
+  if (rc) return rc;
+  return precision == OMB_PREC_FP64 ? run_hmkh<double>(ctx, P, k, ncol, H, out)
+                                    : run_hmkh<float>(ctx, P, k, ncol, H, out);
 }
 
 int omb_HMkH(omb_ctx* ctx, int precision, const omb_grid* grid, double k, const double* epsinv,

@@ -438,6 +438,58 @@ int omb_solve_k(omb_ctx* ctx, const omb_instance* inst, int n_inst, const omb_op
   return rc;
 }
 
+int omb_solve_k_periodic(omb_ctx* ctx, const omb_grid3* grid, double omega, const double* epsinv, int nev,
+                         double kguess, const omb_options* opt, double* kmags, double* evecs, double* residuals,
+                         double* dw2dk, int32_t* status, int32_t* iterations) {
+  if (!ctx || !grid) return fail(OMB_ERR_INVALID_ARG, "ctx and grid must be non-NULL");
+  if (!kmags) return fail(OMB_ERR_INVALID_ARG, "kmags is NULL");
+  if (!(omega > 0) || !std::isfinite(omega)) return fail(OMB_ERR_INVALID_ARG, "omega must be finite and positive");
+  if (grid->Nz < 8) return fail(OMB_ERR_UNSUPPORTED, "a z-periodic cell needs Nz >= 8 slabs (a supported length)");
+  SolveOptions so;
+  int rc = options_from(opt, so);
+  if (rc) return rc;
+  if (so.newton_mode != MODE_NEWTON_INNER)
+    return fail(OMB_ERR_UNSUPPORTED, "z-periodic cells use the inner Newton iteration (OMB_NEWTON_INNER)");
+  if (nev <= 0 || nev + so.guard > MMAX) return fail(OMB_ERR_INVALID_ARG, "nev + guard_bands must be in 2..12");
+  OMB_CU(cudaSetDevice(ctx->device));
+  std::vector<Problem> probs(1);
+  const omb_grid g2{grid->Nx, grid->Ny, grid->Dx, grid->Dy};
+  rc = upload_problem(ctx, &g2, epsinv, probs[0], grid->Nz, grid->Dz);
+  if (rc) return rc;
+  const double k0 = kguess > 0 ? kguess : omega * std::sqrt(1.0 / probs[0].min_diag);
+  std::vector<TrackSpec> tracks;
+  for (int band = 0; band < nev; ++band) {
+    TrackSpec ts;
+    ts.prob = 0; ts.band = band; ts.nbands = 1; ts.M = band + 1 + so.guard; ts.need = band + 1;
+    ts.mode = MODE_NEWTON_INNER; ts.k0 = k0; ts.omega2 = omega * omega;
+    tracks.push_back(ts);
+  }
+  Engine E(ctx, &probs, tracks, so);
+  rc = E.run();
+  if (rc) return rc;
+  if (!opt || opt->canonicalize) {
+    rc = E.canonicalize_results();
+    if (rc) return rc;
+  }
+  const size_t n2 = 2 * probs[0].N();
+  bool all_ok = true;
+  for (int b = 0; b < nev; ++b) {
+    const TrackState& s = E.result_state(b, 0);
+    kmags[b] = s.k;
+    if (residuals) residuals[b] = s.resid[b];
+    if (dw2dk) dw2dk[b] = 2.0 * s.hmkh;
+    if (status) status[b] = status_code(s.status);
+    if (iterations) iterations[b] = s.iter;
+    all_ok = all_ok && s.status == TS_CONVERGED;
+    if (evecs)
+      OMB_CU(cudaMemcpyAsync(evecs + 2 * n2 * b, E.result_dev(b, 0), n2 * sizeof(double2), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+  }
+  OMB_CU(cudaStreamSynchronize(ctx->stream));
+  if (!all_ok) return fail(OMB_ERR_NOT_CONVERGED, "one or more bands did not converge (see the per-band status)");
+  return OMB_OK;
+}
+
 int omb_solve_omega2(omb_ctx* ctx, const omb_grid* grid, double k, const double* epsinv, int nev,
                      const double* Hguess, int nguess, const omb_options* opt, double* evals,
                      double* evecs, double* residuals, int32_t* status) {

@@ -216,11 +216,20 @@ int gather_to_host(omb_ctx* ctx, const D2HPiece* pieces, size_t n) {
   return OMB_OK;
 }
 
-int upload_problem(omb_ctx* ctx, const omb_grid* g, const double* epsinv, Problem& P) {
+int upload_problem(omb_ctx* ctx, const omb_grid* g, const double* epsinv, Problem& P, int Nz, double Dz) {
   int rc = check_grid(g);
   if (rc) return rc;
   if (!epsinv) return fail(OMB_ERR_INVALID_ARG, "epsinv is NULL");
+  if (Nz > 1) {
+    if (!fft_size_supported(Nz)) return fail(OMB_ERR_UNSUPPORTED, "unsupported Nz " + std::to_string(Nz));
+    if (!(Dz > 0) || !std::isfinite(Dz)) return fail(OMB_ERR_INVALID_ARG, "the period Dz must be finite and positive");
+    if ((long long)Nz * row_blocks(g->Nx, g->Ny) > 512)
+      return fail(OMB_ERR_UNSUPPORTED, "Nz x row blocks of a slab above 512 (use fewer z slabs or rows)");
+  } else if (Nz != 1) {
+    return fail(OMB_ERR_INVALID_ARG, "Nz must be >= 1");
+  }
   P.Nx = g->Nx; P.Ny = g->Ny; P.Dx = g->Dx; P.Dy = g->Dy;
+  P.Nz = Nz; P.Dz = Nz > 1 ? Dz : 0;
   const size_t N = P.N();
   std::vector<float4> a32(N);
   std::vector<float2> b32(N);
@@ -279,7 +288,8 @@ template <> OpUnit<float> make_unit<float>(const Problem& P) {
   u.e32a = P.e32a.p; u.e32b = P.e32b.p; u.e64 = P.e64.p; u.eave = P.eave32.p;
   u.Nx = P.Nx; u.Ny = P.Ny;
   u.inv_dx = (float)(1.0 / P.Dx); u.inv_dy = (float)(1.0 / P.Dy);
-  u.part_stride = row_blocks(P.Nx, P.Ny);
+  u.part_stride = row_blocks(P.Nx, P.Ny) * P.Nz;
+  u.inv_dz = P.Nz > 1 ? 1.0 / P.Dz : 0.0;
   return u;
 }
 template <> OpUnit<double> make_unit<double>(const Problem& P) {
@@ -287,7 +297,8 @@ template <> OpUnit<double> make_unit<double>(const Problem& P) {
   u.e32a = P.e32a.p; u.e32b = P.e32b.p; u.e64 = P.e64.p; u.eave = P.eave64.p;
   u.Nx = P.Nx; u.Ny = P.Ny;
   u.inv_dx = 1.0 / P.Dx; u.inv_dy = 1.0 / P.Dy;
-  u.part_stride = row_blocks(P.Nx, P.Ny);
+  u.part_stride = row_blocks(P.Nx, P.Ny) * P.Nz;
+  u.inv_dz = P.Nz > 1 ? 1.0 / P.Dz : 0.0;
   return u;
 }
 

@@ -96,7 +96,8 @@ template <typename T> struct DevBuf {
 // plus ε_ave = 3/tr(ε⁻¹) for the MPB-style preconditioner.
 struct Problem {
   int Nx = 0, Ny = 0;
-  double Dx = 0, Dy = 0;
+  int Nz = 1;       // z-periodic cells: Nz > 1 slabs over the period Dz
+  double Dx = 0, Dy = 0, Dz = 0;
   double eps_mean = 0;  // cell mean of ε_ave (diagonal preconditioner scale)
   double min_diag = 0;  // min over pixels and a of ε⁻¹[a,a] (k_guess)
   double max_trace = 0; // max over pixels of tr ε⁻¹ (bounds the largest eigenvalue of ε⁻¹)
@@ -105,12 +106,13 @@ struct Problem {
   DevBuf<double2> e64;
   DevBuf<float> eave32;
   DevBuf<double> eave64;
-  size_t N() const { return (size_t)Nx * Ny; }
+  size_t N() const { return (size_t)Nx * Ny * Nz; }
 };
 
 // Validate the grid and ε⁻¹ and upload them.  Returns OMB_OK or an error code.
 int check_grid(const omb_grid* g);
-int upload_problem(omb_ctx* ctx, const omb_grid* g, const double* epsinv, Problem& P);
+// Nz > 1: a z-periodic cell, ε⁻¹ (3, 3, Nx, Ny, Nz) over the period Dz.
+int upload_problem(omb_ctx* ctx, const omb_grid* g, const double* epsinv, Problem& P, int Nz = 1, double Dz = 0);
 
 // Fill an OpUnit for one problem (pointers to block buffers set by the caller).
 template <typename T> OpUnit<T> make_unit(const Problem& P);

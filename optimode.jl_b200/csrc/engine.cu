@@ -4,6 +4,7 @@
 #include <cstring>
 
 #include <map>
+#include <tuple>
 
 #include "engine.h"
 #include "vec.cuh"
@@ -30,14 +31,14 @@ Engine::Engine(omb_ctx* ctx, std::vector<Problem>* problems, std::vector<TrackSp
   std::stable_sort(order_.begin(), order_.end(), [&](int a, int b) {
     const Problem& pa = (*probs_)[tracks_[a].prob];
     const Problem& pb = (*probs_)[tracks_[b].prob];
-    return std::make_pair(pa.Nx, pa.Ny) < std::make_pair(pb.Nx, pb.Ny);
+    return std::make_tuple(pa.Nx, pa.Ny, pa.Nz) < std::make_tuple(pb.Nx, pb.Ny, pb.Nz);
   });
   for (int i = 0; i < nt_;) {
     const Problem& p = (*probs_)[tracks_[order_[i]].prob];
-    Group g{i, 0, p.Nx, p.Ny, 0};
+    Group g{i, 0, p.Nx, p.Ny, 0, p.Nz};
     while (i < nt_) {
       const Problem& q = (*probs_)[tracks_[order_[i]].prob];
-      if (q.Nx != p.Nx || q.Ny != p.Ny) break;
+      if (q.Nx != p.Nx || q.Ny != p.Ny || q.Nz != p.Nz) break;
       g.Mmax = std::max(g.Mmax, tracks_[order_[i]].M);
       ++g.n;
       ++i;
@@ -187,8 +188,9 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
     d.res_acc = res_acc_.p + (size_t)t * MMAX;
     d.hmkh_part = hmkh_part_.p + (size_t)t * 2 * 512;
     d.n2 = n2; d.Nx = P.Nx; d.Ny = P.Ny; d.M = M;
-    d.hmkh_nb = row_blocks(P.Nx, P.Ny);
+    d.hmkh_nb = row_blocks(P.Nx, P.Ny) * P.Nz;
     d.inv_dx = 1.0 / P.Dx; d.inv_dy = 1.0 / P.Dy; d.eps_mean = P.eps_mean;
+    d.Nz = P.Nz; d.inv_dz = P.Nz > 1 ? 1.0 / P.Dz : 0.0;
   }
   for (int gi = 0; gi < nt_; ++gi) {
     const int t = order_[gi];
@@ -302,6 +304,12 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
     }
   }
   OMB_CU(d_pre_.alloc(2 * (size_t)LANES * ((size_t)nt_ + 1), st));
+  // z-periodic groups: per-lane room for the slab and line units of launch_op3d
+  int maxNz = 1;
+  for (const Group& g : groups_) maxNz = std::max(maxNz, g.Nz);
+  DevBuf<OpUnit<T>> d_exp[LANES];
+  if (maxNz > 1)
+    for (int L = 0; L < LANES; ++L) OMB_CU(d_exp[L].alloc((size_t)(maxNz + 1) * nt_, st));
 
   const char* step = "";
   auto iteration = [&](int par, int L, cudaStream_t s) -> cudaError_t {
@@ -311,6 +319,10 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
     if (n <= 0) return e;
     int* preg = d_pre_.p + (size_t)L * 2 * (nt_ + 1);
     int* preu = preg + nt_ + 1;
+    auto op = [&](OpKind kind, const OpUnit<T>* u, int cnt, const Group& g, int maxcol) -> cudaError_t {
+      return g.Nz > 1 ? launch_op3d<T>(kind, u, cnt, g.Nx, g.Ny, g.Nz, maxcol, ctx_->tw, d_exp[L].p, s)
+                      : launch_op<T>(kind, u, cnt, g.Nx, g.Ny, maxcol, ctx_->tw, s);
+    };
     // the lane's part of every grid group
     auto for_groups = [&](auto&& f) -> bool {
       for (const Group& g : groups_) {
@@ -321,17 +333,17 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
     };
     if (!opt_.prec_diag &&
         !for_groups([&](const Group& g, int off, int cnt) {
-          return ok("preconditioner pass", launch_op<T>(OP_P, d_uP[par].p + off, cnt, g.Nx, g.Ny, g.Mmax, ctx_->tw, s));
+          return ok("preconditioner pass", op(OP_P, d_uP[par].p + off, cnt, g, g.Mmax));
         }))
       return e;
     if (!for_groups([&](const Group& g, int off, int cnt) {
-          return ok("HMkH pass", launch_op<T>(OP_HMKH, d_uH[par].p + off, cnt, g.Nx, g.Ny, 1, ctx_->tw, s));
+          return ok("HMkH pass", op(OP_HMKH, d_uH[par].p + off, cnt, g, 1));
         }))
       return e;
     k_newton<<<(n + 127) / 128, 128, 0, s>>>(d_state_ptrs_.p + a, d_hmkh_ptrs_.p + a, d_hmkh_nb_.p + a, n, prm);
     if (!ok("k_newton", cudaGetLastError())) return e;
     if (!for_groups([&](const Group& g, int off, int cnt) {
-          return ok("operator pass", launch_op<T>(OP_M, d_uA[par].p + off, cnt, g.Nx, g.Ny, 3 * g.Mmax, ctx_->tw, s));
+          return ok("operator pass", op(OP_M, d_uA[par].p + off, cnt, g, 3 * g.Mmax));
         }))
       return e;
     k_live_prefix<<<1, 1024, 0, s>>>(d_state_ptrs_.p + a, d_n2_.p + a, n, rg, UpdCfg<T>::R, preg, preu);
@@ -446,7 +458,8 @@ int Engine::run() {
     s.M = ts.M; s.band = ts.band; s.need = ts.need; s.mode = ts.mode;
     s.dk_last = 1e300;
     const double gx = 0.5 * P.Nx / P.Dx, gy = 0.5 * P.Ny / P.Dy;
-    normA = std::max(normA, (gx * gx + gy * gy + ts.k0 * ts.k0) * P.max_trace);
+    const double kz = std::fabs(ts.k0) + (P.Nz > 1 ? 0.5 * P.Nz / P.Dz : 0.0);
+    normA = std::max(normA, (gx * gx + gy * gy + kz * kz) * P.max_trace);
   }
   OMB_CU(d_states_.alloc(nt_, st));
   OMB_CU(coef_.alloc((size_t)nt_ * 2 * NMAX * MMAX, st));
@@ -473,7 +486,7 @@ int Engine::run() {
     cp32[gi] = coef32_.p + (size_t)t * 2 * NMAX * MMAX;
     rp[gi] = res_acc_.p + (size_t)t * MMAX;
     hp[gi] = hmkh_part_.p + (size_t)t * 2 * 512;
-    hnb[gi] = row_blocks(P.Nx, P.Ny);
+    hnb[gi] = row_blocks(P.Nx, P.Ny) * P.Nz;
     n2s[gi] = 2 * (long long)P.N();
   }
   OMB_CU(d_state_ptrs_.alloc(nt_, st));
@@ -599,15 +612,15 @@ int Engine::fetch_block_column(int t, int col, double* out) {
 int Engine::canonicalize_results() {
   cudaStream_t st = ctx_->stream;
   // finished results (track, band), grouped by grid
-  std::map<std::pair<int, int>, std::vector<std::pair<int, int>>> groups;
+  std::map<std::tuple<int, int, int>, std::vector<std::pair<int, int>>> groups;
   for (int t = 0; t < nt_; ++t) {
     const Problem& P = (*probs_)[tracks_[t].prob];
-    for (int b = 0; b < (int)snaps_[t].size(); ++b) groups[{P.Nx, P.Ny}].push_back({t, b});
+    for (int b = 0; b < (int)snaps_[t].size(); ++b) groups[{P.Nx, P.Ny, P.Nz}].push_back({t, b});
   }
   constexpr int CHUNK = 64;
   for (const auto& kv : groups) {
-    const int Nx = kv.first.first, Ny = kv.first.second;
-    const size_t N = (size_t)Nx * Ny, n2 = 2 * N;
+    const int Nx = std::get<0>(kv.first), Ny = std::get<1>(kv.first), Nz = std::get<2>(kv.first);
+    const size_t N = (size_t)Nx * Ny * Nz, n2 = 2 * N;
     const auto& all = kv.second;
     for (size_t c0 = 0; c0 < all.size(); c0 += CHUNK) {
       const int cnt = (int)std::min<size_t>(CHUNK, all.size() - c0);
@@ -632,7 +645,13 @@ int Engine::canonicalize_results() {
       }
       OMB_CU(cudaMemcpyAsync(kd.p, kh.data(), cnt * sizeof(double), cudaMemcpyHostToDevice, st));
       OMB_CU(cudaMemcpyAsync(du.p, uh.data(), cnt * sizeof(OpUnit<double>), cudaMemcpyHostToDevice, st));
-      OMB_CU(launch_op<double>(OP_EFIELD, du.p, cnt, Nx, Ny, 1, ctx_->tw, st));
+      DevBuf<OpUnit<double>> ex;
+      if (Nz > 1) {
+        OMB_CU(ex.alloc((size_t)(Nz + 1) * cnt, st));
+        OMB_CU(launch_op3d<double>(OP_EFIELD, du.p, cnt, Nx, Ny, Nz, 1, ctx_->tw, ex.p, st));
+      } else {
+        OMB_CU(launch_op<double>(OP_EFIELD, du.p, cnt, Nx, Ny, 1, ctx_->tw, st));
+      }
       k_argmax_abs2<double><<<cnt, 1024, 0, st>>>(scr.p, (long long)N, 3 * (long long)N, cnt, red.p);
       OMB_CU(cudaGetLastError());
       std::vector<double> h(3 * (size_t)cnt);
@@ -677,7 +696,13 @@ int Engine::result_efield_argmax(int t, int b, long long* idx, double* re, doubl
   DevBuf<OpUnit<double>> du;
   OMB_CU(du.alloc(1, st));
   OMB_CU(cudaMemcpyAsync(du.p, &u, sizeof(u), cudaMemcpyHostToDevice, st));
-  OMB_CU(launch_op<double>(OP_EFIELD, du.p, 1, P.Nx, P.Ny, 1, ctx_->tw, st));
+  DevBuf<OpUnit<double>> ex;
+  if (P.Nz > 1) {
+    OMB_CU(ex.alloc((size_t)(P.Nz + 1), st));
+    OMB_CU(launch_op3d<double>(OP_EFIELD, du.p, 1, P.Nx, P.Ny, P.Nz, 1, ctx_->tw, ex.p, st));
+  } else {
+    OMB_CU(launch_op<double>(OP_EFIELD, du.p, 1, P.Nx, P.Ny, 1, ctx_->tw, st));
+  }
   k_argmax_abs2<double><<<1, 1024, 0, st>>>(scr.p, (long long)N, 3 * (long long)N, 1, red.p);
   OMB_CU(cudaGetLastError());
   double h[3];

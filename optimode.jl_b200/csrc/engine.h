@@ -80,7 +80,7 @@ class Engine {
   int last_prec_ = 1;  // precision of the buffers holding the final block (0 fp32, 1 fp64)
   int64_t launches_ = 0, kernels_ = 0;
 
-  struct Group { int off, n, Nx, Ny, Mmax; };
+  struct Group { int off, n, Nx, Ny, Mmax, Nz; };
   std::vector<Group> groups_;
   std::vector<int> order_;  // tracks sorted by grid size
 

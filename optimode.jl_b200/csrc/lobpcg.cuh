@@ -71,6 +71,8 @@ template <typename T> struct TrackDesc {
   long long n2;         // vector length (2·Nx·Ny complex)
   int Nx, Ny, M, hmkh_nb;
   double inv_dx, inv_dy, eps_mean;
+  int Nz;                // z-periodic cells: slabs (1 for a 2D cell)
+  double inv_dz;
 };
 
 struct IterParams {
@@ -446,8 +448,10 @@ __device__ __forceinline__ void update_tile(const TrackDesc<T>& d, const TrackSt
     T pscale = T(1);
     if (prec_diag) {
       const long long pix = row >> 1;
-      const int ix = (int)(pix % d.Nx), iy = (int)(pix / d.Nx);
-      const T k = (T)s.k;
+      const int ix = (int)(pix % d.Nx);
+      const long long rest = pix / d.Nx;
+      const int iy = (int)(rest % d.Ny), iz = (int)(rest / d.Ny);
+      const T k = (T)(s.k - freq_index(iz, d.Nz) * d.inv_dz);  // w_z = k − g_z
       const T gx = T(freq_index(ix, d.Nx)) * (T)d.inv_dx, gy = T(freq_index(iy, d.Ny)) * (T)d.inv_dy;
       pscale = T(d.eps_mean) / (gx * gx + gy * gy + k * k);
     }

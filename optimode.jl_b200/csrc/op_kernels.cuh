@@ -42,6 +42,11 @@ template <typename T> struct OpUnit {
   int Nx, Ny, ncol;
   int part_stride;        // partial sums per column (≥ gridDim.x of row_out)
   T inv_dx, inv_dy;
+  // z-periodic cells: one unit per z-slab (or per z-line set) of a 3D field
+  long long comp_stride;  // component stride of planar 3-component fields (0: Nx·Ny of the pass)
+  double kz_shift;        // g_z of the slab: the passes see k − g_z (w = k ẑ − G)
+  double inv_dz;          // 1/Λ of a z-periodic cell (0 for a 2D cell)
+  int zx_weight_gz;       // RI_ZXTC only: weight ẑ×H by g_z/Λ (⟨H|∂M̂/∂Λ|H⟩, the period derivative)
 };
 
 enum RowIn : int { RI_KXTC = 0, RI_KXINV = 1, RI_ZXTC = 2, RI_LOAD3 = 3, RI_HCART = 4 };
@@ -87,9 +92,9 @@ __global__ void __launch_bounds__(NT) k_row_in(const OpUnit<T>* __restrict__ uni
   const int Ny = U.Ny;
   const int row0 = blockIdx.x * ROWS;
   if (row0 >= Ny) return;
-  const size_t N = (size_t)NX * Ny;
+  const size_t N = U.comp_stride ? (size_t)U.comp_stride : (size_t)NX * Ny;
   load_tw(tw, tw_g, NX);
-  const T k = (T)(*U.k_dev);
+  const T k = (T)(*U.k_dev - U.kz_shift);
   const C* __restrict__ H = U.in + (size_t)(col + unit_col0(U)) * U.in_cs;
 #pragma unroll
   for (int q = threadIdx.x; q < ROWS * NX; q += NT) {
@@ -119,6 +124,11 @@ __global__ void __launch_bounds__(NT) k_row_in(const OpUnit<T>* __restrict__ uni
         } else {  // RI_ZXTC: ẑ × (h1 m̂ + h2 n̂)
           d0 = (h1 * b.my + h2 * b.ny) * T(-1);
           d1 = h1 * b.mx + h2 * b.nx;
+          if (U.zx_weight_gz) {
+            const T wz = (T)(U.kz_shift * U.inv_dz);
+            d0 = d0 * wz;
+            d1 = d1 * wz;
+          }
         }
       }
     }
@@ -157,7 +167,7 @@ __global__ void __launch_bounds__(NT) k_col(const OpUnit<T>* __restrict__ units,
   const int Nx = U.Nx;
   const int ix0 = blockIdx.x * TX;
   if (ix0 >= Nx) return;
-  const size_t N = (size_t)Nx * NY;
+  const size_t N = U.comp_stride ? (size_t)U.comp_stride : (size_t)Nx * NY;
   load_tw(tw, tw_g, NY);
   C* __restrict__ D = U.scr + (size_t)col * U.scr_cs;
 #pragma unroll
@@ -223,7 +233,7 @@ __global__ void __launch_bounds__(NT) k_row_out(const OpUnit<T>* __restrict__ un
   const int Ny = U.Ny;
   const int row0 = blockIdx.x * ROWS;
   if (row0 >= Ny) return;
-  const size_t N = (size_t)NX * Ny;
+  const size_t N = U.comp_stride ? (size_t)U.comp_stride : (size_t)NX * Ny;
   load_tw(tw, tw_g, NX);
   const C* __restrict__ D = U.scr + (size_t)col * U.scr_cs;
 #pragma unroll
@@ -236,7 +246,7 @@ __global__ void __launch_bounds__(NT) k_row_out(const OpUnit<T>* __restrict__ un
   }
   __syncthreads();
   fft_lines<C, NX, INV, 3 * ROWS, NT>(s, LS, tw);
-  const T k = (T)(*U.k_dev);
+  const T k = (T)(*U.k_dev - U.kz_shift);
   const T sN = T(1) / T(N);
   const int c0 = unit_col0(U);
   C* __restrict__ O = U.out + (size_t)(col + c0) * U.out_cs;

@@ -99,6 +99,11 @@ __device__ __forceinline__ void prologue_at(const OpUnit<T>& U, const cplx<T>* _
       d0 = (h1 * b.my + h2 * b.ny) * T(-1);
       d1 = h1 * b.mx + h2 * b.nx;
       d2 = mk<C>(0, 0);
+      if (U.zx_weight_gz) {  // the period derivative: each plane wave weighted by g_z/Λ
+        const T wz = (T)(U.kz_shift * U.inv_dz);
+        d0 = d0 * wz;
+        d1 = d1 * wz;
+      }
     }
   }
 }
@@ -120,8 +125,8 @@ __global__ void __launch_bounds__(l2_row_threads(NX, G)) k_row_in2(const OpUnit<
   const int Ny = U.Ny;
   const int row0 = blockIdx.x * G;
   if (row0 >= Ny) return;
-  const size_t N = (size_t)NX * Ny;
-  const T k = (T)(*U.k_dev);
+  const size_t N = U.comp_stride ? (size_t)U.comp_stride : (size_t)NX * Ny;
+  const T k = (T)(*U.k_dev - U.kz_shift);
   const C* __restrict__ H = U.in + (size_t)(col + unit_col0(U)) * U.in_cs;
   const C* tw1 = tw_g + NX;
   for (int q = threadIdx.x; q < G * B; q += NT) {
@@ -219,7 +224,7 @@ __global__ void __launch_bounds__(l2_col_threads_tx(NY, TX),
   const int Nx = U.Nx;
   const int ix0 = blockIdx.x * TX;
   if (ix0 >= Nx) return;
-  const size_t N = (size_t)Nx * NY;
+  const size_t N = U.comp_stride ? (size_t)U.comp_stride : (size_t)Nx * NY;
   const C* tw1 = tw_g + NY;
   const C* tw3 = tw_g + 2 * NY;
   C* __restrict__ D = U.scr + (size_t)col * U.scr_cs;
@@ -351,7 +356,7 @@ __global__ void __launch_bounds__(l2_row_threads(NX, G)) k_row_out2(const OpUnit
   const int Ny = U.Ny;
   const int row0 = blockIdx.x * G;
   if (row0 >= Ny) return;
-  const size_t N = (size_t)NX * Ny;
+  const size_t N = U.comp_stride ? (size_t)U.comp_stride : (size_t)NX * Ny;
   const C* tw3 = tw_g + 2 * NX;
   const C* __restrict__ D = U.scr + (size_t)col * U.scr_cs;
   for (int q = threadIdx.x; q < G * A; q += NT) {
@@ -366,7 +371,7 @@ __global__ void __launch_bounds__(l2_row_threads(NX, G)) k_row_out2(const OpUnit
     }
   }
   __syncthreads();
-  const T k = (T)(*U.k_dev);
+  const T k = (T)(*U.k_dev - U.kz_shift);
   const T sN = T(1) / T(N);
   const int c0 = unit_col0(U);
   C* __restrict__ O = U.out + (size_t)(col + c0) * U.out_cs;

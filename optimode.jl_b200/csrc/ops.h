@@ -47,5 +47,10 @@ int row_blocks(int Nx, int Ny);
 template <typename T>
 cudaError_t launch_op(OpKind op, const OpUnit<T>* d_units, int nunits, int Nx, int Ny, int maxcol,
                       const TwTables& tw, cudaStream_t st);
+// The same pipelines on z-periodic cells (Nz slabs; ops3d.cuh); `expand` is device memory for
+// (Nz + 1)·nunits units.
+template <typename T>
+cudaError_t launch_op3d(OpKind op, const OpUnit<T>* d_units, int nunits, int Nx, int Ny, int Nz, int maxcol,
+                        const TwTables& tw, OpUnit<T>* expand, cudaStream_t st);
 
 }  // namespace omb

@@ -13,6 +13,9 @@ from .solver import B200Solver, Batch, solve_k, solve_k_batch, solve_omega2  # n
 from .adjoint import pullback, solve_k_rrule  # noqa: F401
 from .analysis import group_index, ng_gvd  # noqa: F401
 from . import warmstart  # noqa: F401  (declares the warm-start symbols before the library loads)
+from .periodic import (  # noqa: F401
+    Grid3, apply3, HMkH3, solve_k_periodic, solve_k_periodic_pullback, solve_k_periodic_rrule,
+)
 from .geometry import (  # noqa: F401
     Polygon, SmoothingPlan, smoothing_plan, smooth_eps, smooth_epsinv, material_column,
 )

@@ -139,6 +139,15 @@ class Operator3:
         e = bfft3(self._eid(d))
         return kx_ct(e, self.mag, self.m, self.n, 1.0 / self.grid.N).reshape(-1)
 
+    def P(self, Hv):
+        """MPB-style preconditioner (``_P!``, ``ME/src/maxwell.jl:430-469``) on 3D fields:
+        e = (H₁n − H₂m)/mag → bfft → ε_ave·e → fft → H₁ = (d·n)/(mag N), H₂ = −(d·m)/(mag N)."""
+        H = _field(Hv, self.grid, 2)
+        e = (H[..., 0:1] * self.n - H[..., 1:2] * self.m) / self.mag[..., None]
+        d = fft3(bfft3(e) * self.eps_ave[..., None])
+        s = 1.0 / (self.mag * self.grid.N)
+        return np.stack([np.sum(d * self.n, axis=-1) * s, -np.sum(d * self.m, axis=-1) * s], axis=-1).reshape(-1)
+
     def P_diag(self, Hv):
         H = _field(Hv, self.grid, 2)
         scale = float(np.mean(self.eps_ave)) / self.mag ** 2

@@ -49,6 +49,9 @@ def test_hermitian_and_uniform_medium():
     # (the period keeps k = ω√ε inside the first Brillouin zone, |k| < 1/(2Λ) = 2 μm⁻¹)
     km, _ = P.solve_k_periodic(OMEGA, u, 0.25, g, nev=1, k_tol=1e-12, eig_tol=1e-11)
     assert np.isclose(km[0], OMEGA * np.sqrt(2.5), rtol=1e-10)
+    # the MPB-style P̂ inverts M̂ exactly in a uniform medium
+    opu = P.Operator3(1.3, u, g)
+    assert np.allclose(opu.P(opu.M(a)), a, rtol=0, atol=1e-12 * np.linalg.norm(a))
 
 
 def test_z_invariant_cell_matches_2d_oracle():
