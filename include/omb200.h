@@ -73,7 +73,9 @@ int omb_fft_size_supported(int n);
 const char* omb_last_error(void);
 
 /* Create / destroy a context on CUDA device `device`.  The context owns a stream,
- * device-resident twiddle tables and a stream-ordered memory pool. */
+ * device-resident twiddle tables and a stream-ordered memory pool.  Destroy the batches and
+ * smoothing plans made on a context before the context; a warm-start network still alive
+ * then is released with it (its handle then only goes to omb_warmstart_destroy). */
 int omb_ctx_create(int device, omb_ctx** out);
 int omb_ctx_destroy(omb_ctx* ctx);
 
@@ -142,8 +144,10 @@ int omb_apply_M_noalloc(int32_t Nx, int32_t Ny, double Dx, double Dy, double k, 
 /* ---------------------------------------------------------------------------------
  * Autotuning of the FP32 operator passes (the counterpart of the reference's FFTW PATIENT
  * planning at ModeSolver construction, lib/MaxwellEigenmodes/src/maxwell.jl:940-943).
- * Per (device name, Nx, Ny) the 36 combinations of row-pass variant (0, 1, 2: half, default,
- * double the grid rows per CTA), column-pass variant (0, 1, 2: 4, 8, 16 columns per CTA) and
+ * Per (device name, Nx, Ny) the 80 combinations of row-pass variant (0, 1, 2: half, default,
+ * double the grid rows per CTA; 3: default rows, one thread per line slot and field component),
+ * column-pass variant (0, 1, 2: 4, 8, 16 columns per CTA; 3, 4: 8 columns, one thread per slot
+ * and component, with a register budget for three or two CTAs per SM) and
  * wave variant (0: all columns in one launch per pass; 1, 2, 3: waves of 32, 64, 128 columns,
  * each wave's intermediate staying in L2) of an M̂ application are timed and the fastest is
  * kept in a process-wide table,
@@ -153,7 +157,7 @@ int omb_apply_M_noalloc(int32_t Nx, int32_t Ny, double Dx, double Dy, double k, 
  * --------------------------------------------------------------------------------- */
 
 /* Tune one grid now for `ncol`-column applications on 64 units; the chosen variants and, if
- * `seconds` is not NULL, the 36 timings (row-major over row, column, wave variant). */
+ * `seconds` is not NULL, the 80 timings (row-major over row, column, wave variant). */
 int omb_autotune(omb_ctx* ctx, const omb_grid* grid, int32_t ncol, int32_t* row_variant, int32_t* col_variant,
                  int32_t* wave_variant, double* seconds);
 int omb_ctx_set_autotune(omb_ctx* ctx, int32_t enabled);

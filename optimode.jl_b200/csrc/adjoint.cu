@@ -364,6 +364,7 @@ static int pullback_impl(omb_ctx* ctx, Problem& P, double omega, int nev, const 
   cudaStream_t st = ctx->stream;
   const long long N = (long long)P.N(), n2 = 2 * N;
   const bool periodic = P.Nz > 1;
+  const double inv_dz = periodic ? 1.0 / P.Dz : 0.0;  // (a 2D cell has Dz = 0)
   // device buffers
   DevBuf<double2> vecs, scr, ev, eb, lamv;
   OMB_CU(vecs.alloc(8 * n2, st));   // x v w w2 r1 r2 y Av
@@ -383,7 +384,7 @@ static int pullback_impl(omb_ctx* ctx, Problem& P, double omega, int nev, const 
   OMB_CU(S.alloc(1, st));
   double2* vb = vecs.p;
   AdjVecs V{vb, vb + n2, vb + 2 * n2, vb + 3 * n2, vb + 4 * n2, vb + 5 * n2, vb + 6 * n2, vb + 7 * n2, ev.p,
-            n2, P.Nx, P.Ny, 1.0 / P.Dx, 1.0 / P.Dy, 0.0, P.eps_mean, P.Nz, 1.0 / P.Dz};
+            n2, P.Nx, P.Ny, 1.0 / P.Dx, 1.0 / P.Dy, 0.0, P.eps_mean, P.Nz, inv_dz};
   double2* SA = scr.p;              // D0 = fft(kx_tc h)
   double2* SB = SA + 3 * N;         // Λd = fft(kx_tc λ)
   double2* SC = SB + 3 * N;         // copies consumed by the D2E passes
@@ -509,7 +510,7 @@ static int pullback_impl(omb_ctx* ctx, Problem& P, double omega, int nev, const 
       OMB_CU(cudaMemcpyAsync(SD, SB, 3 * N * sizeof(double2), cudaMemcpyDeviceToDevice, st));
       OMB_CU(run(OP_D2E, 4));
       OMB_CU(run(OP_D2E, 5));
-      k_adj_kbar<<<nb, ADJ_NT, 0, st>>>(EC, ED, ev.p, V.x, P.Nx, P.Ny, P.Nz, 1.0 / P.Dx, 1.0 / P.Dy, 1.0 / P.Dz, kb,
+      k_adj_kbar<<<nb, ADJ_NT, 0, st>>>(EC, ED, ev.p, V.x, P.Nx, P.Ny, P.Nz, 1.0 / P.Dx, 1.0 / P.Dy, inv_dz, kb,
                                         part.p);
       OMB_CU(cudaGetLastError());
       std::vector<double> hp(4 * nb);

@@ -394,6 +394,7 @@ int omb_ctx_destroy(omb_ctx* ctx) {
   if (!ctx) return OMB_OK;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  ws_release_all(ctx);
   if (ctx->tw_mem) cudaFree(ctx->tw_mem);
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   cudaStreamDestroy(ctx->stream);

@@ -5,6 +5,7 @@
 
 #include <string>
 #include <utility>
+#include <vector>
 
 #include "omb200.h"
 #include "ops.h"
@@ -22,6 +23,8 @@ struct omb_ctx {
   uint64_t wait_ns = 1000000000ull;
   // learned warm-start network used by OMB_WARM_LEARNED (not owned)
   struct omb_warmstart* ws = nullptr;
+  // every network created on this context: omb_ctx_destroy releases their device memory
+  std::vector<struct omb_warmstart*> nets;
   // tune the FP32 operator tiles of a grid on its first batched solve (omb_ctx_set_autotune)
   int autotune = 1;
 };
@@ -119,5 +122,9 @@ template <typename T> OpUnit<T> make_unit(const Problem& P);
 // Autotuner (tune.cu): has (device, Nx, Ny) been tuned; tune it now (9 timed variants).
 bool tune_known(int dev, int Nx, int Ny);
 int autotune_grid(omb_ctx* ctx, const omb_grid* g, int ncol, int units, struct TileChoice* best, double* times);
+
+// Release the device memory of every warm-start network created on `ctx` and detach them
+// (warmstart.cu); omb_ctx_destroy calls it before the context's stream goes away.
+void ws_release_all(omb_ctx* ctx);
 
 }  // namespace omb

@@ -27,13 +27,17 @@ struct TwTables {
 bool fft_size_supported(int L);
 
 // Tile variants of the FP32 M̂ passes (0, 1, 2: half, default, double the rows per CTA of the
-// row passes / columns per CTA of the column pass) and the wave size (0: every column in one
+// row passes / columns per CTA of the column pass; 3: the default tile with one thread per
+// line slot and field component; column variant 4: as 3 with two CTAs' register budget per
+// SM) and the wave size (0: every column in one
 // launch of each pass; w > 0: the units are cut into waves of about wave_columns(w) columns,
 // each wave running its three passes while its intermediate stays in L2), chosen per grid by
 // the autotuner (tune.cu); grids never tuned use the defaults.
 struct TileChoice {
   int row = 1, col = 1, wave = 0;
 };
+constexpr int ROW_VARIANTS = 4;
+constexpr int COL_VARIANTS = 5;
 constexpr int WAVE_VARIANTS = 4;
 __host__ __device__ constexpr int wave_columns(int w) { return w == 1 ? 32 : w == 2 ? 64 : w == 3 ? 128 : 0; }
 TileChoice tiles_for(int Nx, int Ny);  // for the calling thread's current device

@@ -2,6 +2,7 @@
 #pragma once
 
 #include "op_kernels_2l.cuh"
+#include "op_kernels_split.cuh"
 #include "ops.h"
 
 namespace omb {
@@ -34,7 +35,9 @@ static cudaError_t launch_pass(PassKernel<T> kern, dim3 g, int nt, size_t smem, 
 }
 
 // Tunable tiles (FP32, the eigensolver's M̂ passes): row passes with G/2, G or 2G rows per CTA,
-// the column pass with TX/2, TX or 2·TX columns (variant 0, 1, 2; 1 is the default).
+// the column pass with TX/2, TX or 2·TX columns (variant 0, 1, 2; 1 is the default); variant 3
+// is the component-parallel form of the default tile (op_kernels_split.cuh), and column
+// variant 4 the same with a register budget for two CTAs per SM instead of three.
 template <int NX> __host__ __device__ constexpr int row_g_variant(int v) {
   return v == 0 ? (l2_rows(NX) / 2 > 0 ? l2_rows(NX) / 2 : 1) : (v == 2 ? 2 * l2_rows(NX) : l2_rows(NX));
 }
@@ -62,10 +65,35 @@ static cudaError_t col_tx(const OpUnit<T>* u, int nunits, int Nx, int maxcol, co
   return launch_pass<T>(k_col2<T, NY, S1, PW, S2, TX>, g, NT, sm, st, u, tw);
 }
 
+template <int NX, int MODE, bool INV>
+static cudaError_t row_in_sp(const OpUnit<float>* u, int nunits, int Ny, int maxcol, const float2* tw, cudaStream_t st) {
+  constexpr int G = l2_rows(NX), NT = sp_row_threads(NX, G);
+  const size_t sm = (size_t)3 * G * l2_row_lstr<float2, NX>() * sizeof(float2);
+  const dim3 g((Ny + G - 1) / G, maxcol, nunits);
+  return launch_pass<float>(k_row_in_sp<NX, MODE, INV, G>, g, NT, sm, st, u, tw);
+}
+template <int NX, int MODE, bool INV>
+static cudaError_t row_out_sp(const OpUnit<float>* u, int nunits, int Ny, int maxcol, const float2* tw, cudaStream_t st) {
+  constexpr int G = l2_rows(NX), NT = sp_row_threads(NX, G);
+  const size_t sm = (size_t)3 * G * l2_row_lstr<float2, NX>() * sizeof(float2);
+  const dim3 g((Ny + G - 1) / G, maxcol, nunits);
+  return launch_pass<float>(k_row_out_sp<NX, MODE, INV, G>, g, NT, sm, st, u, tw);
+}
+template <int NY, int S1, int PW, int S2, int MINB>
+static cudaError_t col_sp(const OpUnit<float>* u, int nunits, int Nx, int maxcol, const float2* tw, cudaStream_t st) {
+  constexpr int TX = l2_tx<float>(NY), NT = sp_col_threads(NY, TX);
+  const size_t sm = (size_t)3 * TX * l2_col_lstr<float2, NY, TX>() * sizeof(float2);
+  const dim3 g((Nx + TX - 1) / TX, maxcol, nunits);
+  return launch_pass<float>(k_col_sp<NY, S1, PW, S2, TX, MINB>, g, NT, sm, st, u, tw);
+}
+
 template <typename T, int NX>
 static cudaError_t row_in_nx(int mode, const OpUnit<T>* u, int nunits, int Ny, int maxcol,
                              const cplx<T>* tw, cudaStream_t st, int gv = 1) {
   if constexpr (plan2_a(NX) != 0 && sizeof(T) == 4) {
+    if (mode == RI_KXTC && gv == 3)
+      return row_in_sp<NX, RI_KXTC, false>(reinterpret_cast<const OpUnit<float>*>(u), nunits, Ny, maxcol,
+                                           reinterpret_cast<const float2*>(tw), st);
     if (mode == RI_KXTC && gv != 1)
       return gv == 0 ? row_in_g<T, NX, row_g_variant<NX>(0), RI_KXTC, false>(u, nunits, Ny, maxcol, tw, st)
                      : row_in_g<T, NX, row_g_variant<NX>(2), RI_KXTC, false>(u, nunits, Ny, maxcol, tw, st);
@@ -102,6 +130,12 @@ static cudaError_t row_out_nx(int mode, const OpUnit<T>* u, int nunits, int Ny, 
                               const cplx<T>* tw, cudaStream_t st, int gv = 1) {
   if constexpr (plan2_a(NX) != 0 && sizeof(T) == 4) {
     // (the dot-product mode keeps the default rows: its partial sums are laid out per row block)
+    if (mode == RO_KXCT && gv == 3)
+      return row_out_sp<NX, RO_KXCT, true>(reinterpret_cast<const OpUnit<float>*>(u), nunits, Ny, maxcol,
+                                           reinterpret_cast<const float2*>(tw), st);
+    if (mode == RO_KXCT_DOT && gv == 3)
+      return row_out_sp<NX, RO_KXCT_DOT, true>(reinterpret_cast<const OpUnit<float>*>(u), nunits, Ny, maxcol,
+                                               reinterpret_cast<const float2*>(tw), st);
     if (mode == RO_KXCT && gv != 1)
       return gv == 0 ? row_out_g<T, NX, row_g_variant<NX>(0), RO_KXCT, true>(u, nunits, Ny, maxcol, tw, st)
                      : row_out_g<T, NX, row_g_variant<NX>(2), RO_KXCT, true>(u, nunits, Ny, maxcol, tw, st);
@@ -138,6 +172,12 @@ template <typename T, int NY>
 static cudaError_t col_ny(int mode, const OpUnit<T>* u, int nunits, int Nx, int maxcol,
                           const cplx<T>* tw, cudaStream_t st, int tv = 1) {
   if constexpr (plan2_a(NY) != 0 && sizeof(T) == 4) {
+    if (mode == CM_M && (tv == 3 || tv == 4)) {
+      const auto* uf = reinterpret_cast<const OpUnit<float>*>(u);
+      const auto* tf = reinterpret_cast<const float2*>(tw);
+      return tv == 3 ? col_sp<NY, CS_FWD, PW_EPS, CS_INV, 3>(uf, nunits, Nx, maxcol, tf, st)
+                     : col_sp<NY, CS_FWD, PW_EPS, CS_INV, 2>(uf, nunits, Nx, maxcol, tf, st);
+    }
     if (mode == CM_M && tv != 1)
       return tv == 0 ? col_tx<T, NY, col_tx_variant<NY>(0), CS_FWD, PW_EPS, CS_INV>(u, nunits, Nx, maxcol, tw, st)
                      : col_tx<T, NY, col_tx_variant<NY>(2), CS_FWD, PW_EPS, CS_INV>(u, nunits, Nx, maxcol, tw, st);
@@ -221,7 +261,7 @@ cudaError_t launch_op(OpKind op, const OpUnit<T>* u, int nunits, int Nx, int Ny,
         OMB_TRY(row_in<T>(RI_KXTC, u + u0, n, Nx, Ny, maxcol, t, st, tc.row));
         OMB_TRY(col<T>(CM_M, u + u0, n, Nx, Ny, maxcol, t, st, tc.col));
         OMB_TRY(op == OP_M ? row_out<T>(RO_KXCT, u + u0, n, Nx, Ny, maxcol, t, st, tc.row)
-                           : row_out<T>(RO_KXCT_DOT, u + u0, n, Nx, Ny, maxcol, t, st));
+                           : row_out<T>(RO_KXCT_DOT, u + u0, n, Nx, Ny, maxcol, t, st, tc.row == 3 ? 3 : 1));
       }
       return cudaSuccess;
     }
@@ -234,7 +274,7 @@ cudaError_t launch_op(OpKind op, const OpUnit<T>* u, int nunits, int Nx, int Ny,
     case OP_MDOT:
       OMB_TRY(row_in<T>(RI_KXTC, u, nunits, Nx, Ny, maxcol, t, st, tc.row));
       OMB_TRY(col<T>(CM_M, u, nunits, Nx, Ny, maxcol, t, st, tc.col));
-      return row_out<T>(RO_KXCT_DOT, u, nunits, Nx, Ny, maxcol, t, st);
+      return row_out<T>(RO_KXCT_DOT, u, nunits, Nx, Ny, maxcol, t, st, tc.row == 3 ? 3 : 1);
     case OP_P:
       OMB_TRY(row_in<T>(RI_KXINV, u, nunits, Nx, Ny, maxcol, t, st));
       OMB_TRY(col<T>(CM_P, u, nunits, Nx, Ny, maxcol, t, st));

@@ -59,7 +59,8 @@ bool parse_line(const std::string& line, TuneKey& k, TuneEntry& e) {
     const int nx = std::stoi(f[1]), ny = std::stoi(f[2]), r = std::stoi(f[3]), c = std::stoi(f[4]);
     const double s = std::stod(f[5]);
     const int w = f.size() == 7 ? std::stoi(f[6]) : 0;
-    if (nx <= 0 || ny <= 0 || r < 0 || r > 2 || c < 0 || c > 2 || w < 0 || w >= WAVE_VARIANTS || !(s >= 0))
+    if (nx <= 0 || ny <= 0 || r < 0 || r >= ROW_VARIANTS || c < 0 || c >= COL_VARIANTS || w < 0 ||
+        w >= WAVE_VARIANTS || !(s >= 0))
       return false;
     k = TuneKey{f[0], nx, ny};
     e = TuneEntry{r, c, s, w};
@@ -140,7 +141,7 @@ bool tune_known(int dev, int Nx, int Ny) {
   return g_tune.count(TuneKey{name, Nx, Ny}) > 0;
 }
 
-// Times the 36 tile × wave variants of one FP32 M̂ application to `ncol` columns on `units`
+// Times the 80 tile × wave variants of one FP32 M̂ application to `ncol` columns on `units`
 // copies of a uniform cell and records the fastest.
 int autotune_grid(omb_ctx* ctx, const omb_grid* g, int ncol, int units, TileChoice* best, double* times) {
   int rc = check_grid(g);
@@ -182,8 +183,8 @@ int autotune_grid(omb_ctx* ctx, const omb_grid* g, int ncol, int units, TileChoi
   TileChoice bt;
   int vi = 0;
   rc = OMB_OK;
-  for (int r = 0; r < 3 && !rc; ++r)
-    for (int c = 0; c < 3 && !rc; ++c)
+  for (int r = 0; r < ROW_VARIANTS && !rc; ++r)
+    for (int c = 0; c < COL_VARIANTS && !rc; ++c)
       for (int wv = 0; wv < WAVE_VARIANTS && !rc; ++wv, ++vi) {
       {
         std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -247,9 +248,9 @@ int omb_ctx_set_autotune(omb_ctx* ctx, int32_t enabled) {
 
 int omb_tune_set(const char* device_name, int32_t Nx, int32_t Ny, int32_t row_variant, int32_t col_variant,
                  int32_t wave_variant) {
-  if (!device_name || !*device_name || Nx <= 0 || Ny <= 0 || row_variant < 0 || row_variant > 2 || col_variant < 0 ||
-      col_variant > 2 || wave_variant < 0 || wave_variant >= WAVE_VARIANTS)
-    return fail(OMB_ERR_INVALID_ARG, "omb_tune_set: bad key or variant (rows, columns 0..2; wave 0..3)");
+  if (!device_name || !*device_name || Nx <= 0 || Ny <= 0 || row_variant < 0 || row_variant >= ROW_VARIANTS ||
+      col_variant < 0 || col_variant >= COL_VARIANTS || wave_variant < 0 || wave_variant >= WAVE_VARIANTS)
+    return fail(OMB_ERR_INVALID_ARG, "omb_tune_set: bad key or variant (rows 0..3, columns 0..4, wave 0..3)");
   std::string n = device_name;
   for (char& c : n)
     if (c == '|' || c == '\n') c = '_';

@@ -42,7 +42,6 @@ namespace {
 constexpr int WS_IN = 128;     // input image side
 constexpr int WS_CIN = 8;      // input channels
 constexpr int WS_OUT = 64;     // output image side
-constexpr int WS_NOUT = 12;    // output channels
 constexpr int WS_OUT_LD = 16;  // output row pitch (floats)
 constexpr float WS_LAMBDA_N = 100.f;
 
@@ -367,7 +366,8 @@ struct WsLayer {
 }  // namespace omb
 
 struct omb_warmstart {
-  omb_ctx* ctx = nullptr;
+  omb_ctx* ctx = nullptr;  // null once the context was destroyed (device memory released)
+  int device = 0;
   int cap = 0;
   omb::WsLayer L[omb::WS_LAYERS];
   omb::DevBuf<omb::bf16> up;          // L5 output upsampled [B·64·64 × 128]
@@ -619,6 +619,28 @@ int ws_guesses(omb_warmstart* W, const std::vector<const Problem*>& probs, const
   return OMB_OK;
 }
 
+void ws_release_all(omb_ctx* ctx) {
+  for (omb_warmstart* W : ctx->nets) {
+    for (WsLayer& L : W->L) L = WsLayer{};
+    W->up = DevBuf<bf16>{};
+    W->out = DevBuf<float>{};
+    W->dout = DevBuf<float>{};
+    W->dy = DevBuf<float>{};
+    W->dx = DevBuf<float>{};
+    W->dym = DevBuf<float>{};
+    W->dz = DevBuf<bf16>{};
+    W->dzt = DevBuf<bf16>{};
+    W->at = DevBuf<bf16>{};
+    W->da = DevBuf<float>{};
+    W->loss = DevBuf<float>{};
+    W->err = DevBuf<int>{};
+    W->ctx = nullptr;
+  }
+  ctx->nets.clear();
+  ctx->ws = nullptr;
+  cudaStreamSynchronize(ctx->stream);
+}
+
 }  // namespace omb
 
 using namespace omb;
@@ -631,6 +653,7 @@ int omb_warmstart_create(omb_ctx* ctx, int32_t batch_cap, uint64_t seed, omb_war
   OMB_CU(cudaSetDevice(ctx->device));
   auto W = std::make_unique<omb_warmstart>();
   W->ctx = ctx;
+  W->device = ctx->device;
   W->cap = batch_cap;
   cudaStream_t st = ctx->stream;
   std::mt19937_64 rng(seed);
@@ -664,6 +687,7 @@ int omb_warmstart_create(omb_ctx* ctx, int32_t batch_cap, uint64_t seed, omb_war
   int rc = ws_alloc(W.get(), batch_cap);
   if (rc) return rc;
   OMB_CU(cudaStreamSynchronize(st));
+  ctx->nets.push_back(W.get());
   *out = W.release();
   return OMB_OK;
 }
@@ -677,10 +701,14 @@ int omb_ctx_set_warmstart(omb_ctx* ctx, omb_warmstart* W) {
 
 int omb_warmstart_destroy(omb_warmstart* W) {
   if (!W) return OMB_OK;
-  if (W->ctx->ws == W) W->ctx->ws = nullptr;
-  cudaSetDevice(W->ctx->device);
-  cudaStreamSynchronize(W->ctx->stream);
-  delete W;
+  cudaSetDevice(W->device);
+  if (omb_ctx* ctx = W->ctx) {
+    if (ctx->ws == W) ctx->ws = nullptr;
+    auto& v = ctx->nets;
+    v.erase(std::remove(v.begin(), v.end(), W), v.end());
+    cudaStreamSynchronize(ctx->stream);
+  }
+  delete W;  // (an orphaned network holds no device memory any more)
   return OMB_OK;
 }
 

@@ -207,6 +207,70 @@ function ChainRulesCore.rrule(::typeof(solve_k), ω::T0, ε⁻¹::AbstractArray{
     return ((kmags, evecs), b200_solve_k_pullback)
 end
 
+# ---- 3D cells periodic along ẑ (src/grads/period.jl) ----------------------------------------
+# solve_k_periodic(ω, ε⁻¹, Λ, grid::Grid{3}, ::B200Solver; nev) and its rrule, whose pullback
+# returns (NoTangent(), ω̄, ε̄⁻¹, Λ̄, NoTangent(), NoTangent()) like period.jl:227-240.
+
+struct OmbGrid3
+    Nx::Int32
+    Ny::Int32
+    Nz::Int32
+    Dx::Float64
+    Dy::Float64
+    Dz::Float64
+end
+
+_omb_grid3(g::Grid{3}, Λ) = OmbGrid3(g.Nx, g.Ny, g.Nz, g.Δx, g.Δy, Float64(Λ))
+
+function solve_k_periodic(ω::T, ε⁻¹::AbstractArray{T,5}, Λ::Real, grid::Grid{3,T}, s::B200Solver; nev=1,
+    max_eigsolves=60, maxiter=s.maxiter, k_tol=1e-8, eig_tol=1e-8, kguess=nothing, kwargs...) where {T<:Real}
+    eps = convert(Array{Float64,5}, ε⁻¹)
+    kmags = zeros(Float64, nev)
+    evecs = zeros(ComplexF64, 2 * grid.Nx * grid.Ny * grid.Nz, nev)
+    opt = Ref(_omb_options(s; k_tol, eig_tol, max_eigsolves, maxiter))
+    GC.@preserve eps kmags evecs begin
+        rc = ccall((:omb_solve_k_periodic, OMB200_LIB), Cint,
+            (Ptr{Cvoid}, Ref{OmbGrid3}, Cdouble, Ptr{Float64}, Cint, Cdouble, Ref{OmbOptions}, Ptr{Float64},
+             Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Int32}, Ptr{Int32}),
+            _omb_ctx(s), Ref(_omb_grid3(grid, Λ)), Float64(ω), eps, nev,
+            kguess === nothing ? 0.0 : Float64(first(kguess)), opt, kmags, Ptr{Float64}(pointer(evecs)),
+            C_NULL, C_NULL, C_NULL, C_NULL)
+        _omb_check(rc)
+    end
+    return kmags, [evecs[:, j] for j in 1:nev]
+end
+
+function ChainRulesCore.rrule(::typeof(solve_k_periodic), ω::T, ε⁻¹::AbstractArray{T,5}, Λ::Real,
+    grid::Grid{3,T}, s::B200Solver; nev=1, max_eigsolves=60, maxiter=s.maxiter, k_tol=1e-8, eig_tol=1e-8,
+    kwargs...) where {T<:Real}
+    kmags, evecs = solve_k_periodic(ω, ε⁻¹, Λ, grid, s; nev, max_eigsolves, maxiter, k_tol, eig_tol, kwargs...)
+    eps = convert(Array{Float64,5}, ε⁻¹)
+    function b200_solve_k_periodic_pullback(ΔΩ)
+        ΔΩ isa AbstractZero && return (NoTangent(), 0.0, zero(eps), 0.0, NoTangent(), NoTangent())
+        k̄mags, ēvecs = ΔΩ
+        kbar = k̄mags isa AbstractZero ? nothing : [k isa AbstractZero ? 0.0 : Float64(k) for k in k̄mags]
+        n2 = length(first(evecs))
+        ebar = ēvecs isa AbstractZero ? nothing :
+               reduce(hcat, [e isa AbstractZero ? zeros(ComplexF64, n2) : ComplexF64.(e) for e in ēvecs])
+        V = reduce(hcat, evecs)
+        ω̄, Λ̄ = Ref(0.0), Ref(0.0)
+        ε̄⁻¹ = zeros(Float64, size(eps))
+        opt = Ref(_omb_options(s; k_tol, eig_tol, max_eigsolves, maxiter))
+        GC.@preserve eps kmags V kbar ebar ε̄⁻¹ begin
+            rc = ccall((:omb_pullback_periodic, OMB200_LIB), Cint,
+                (Ptr{Cvoid}, Ref{OmbGrid3}, Cdouble, Ptr{Float64}, Cint, Ptr{Float64}, Ptr{Float64},
+                 Ptr{Float64}, Ptr{Float64}, Ref{OmbOptions}, Ref{Float64}, Ptr{Float64}, Ref{Float64}, Ptr{Int32}),
+                _omb_ctx(s), Ref(_omb_grid3(grid, Λ)), Float64(ω), eps, nev, kmags, Ptr{Float64}(pointer(V)),
+                kbar === nothing ? Ptr{Float64}(C_NULL) : pointer(kbar),
+                ebar === nothing ? Ptr{Float64}(C_NULL) : Ptr{Float64}(pointer(ebar)),
+                opt, ω̄, ε̄⁻¹, Λ̄, C_NULL)
+            _omb_check(rc)
+        end
+        return (NoTangent(), ω̄[], ε̄⁻¹, Λ̄[], NoTangent(), NoTangent())
+    end
+    return ((kmags, evecs), b200_solve_k_periodic_pullback)
+end
+
 # ---- Kottke smoothing on the device -------------------------------------------------------
 # `SmoothingPlan` / `smooth_ε(plan, mat_vals)` of lib/DielectricSmoothing/src/smoothing_plan.jl
 # computed by libomb200.  Shapes are passed as convex polygons: one (n, 2) vertex matrix per

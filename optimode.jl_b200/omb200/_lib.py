@@ -7,6 +7,7 @@ device is missing, every entry point raises.
 
 from __future__ import annotations
 
+import atexit
 import ctypes
 import os
 import threading
@@ -49,6 +50,25 @@ class c_grid(ctypes.Structure):
 _lib = None
 _lock = threading.Lock()
 _dp = ctypes.POINTER(ctypes.c_double)
+_exiting = False
+
+
+def _mark_exiting():
+    global _exiting
+    _exiting = True
+
+
+# At interpreter exit the library's handles (contexts, batches, plans, networks) are left to
+# the process teardown: Python finalises the objects of reference cycles, module globals
+# among them, in no particular order, so a context could be destroyed before a network or
+# batch that still uses its stream.  ``finalizing()`` makes every ``__del__`` a no-op then;
+# explicit ``close()`` calls before exit free resources in the caller's order.
+atexit.register(_mark_exiting)
+
+
+def finalizing() -> bool:
+    """True once the interpreter has begun to exit (``__del__`` must not call the library)."""
+    return _exiting
 
 
 def load():
@@ -122,7 +142,8 @@ class Context:
 
     def __del__(self):  # pragma: no cover - interpreter shutdown order
         try:
-            self.close()
+            if not finalizing():
+                self.close()
         except Exception:
             pass
 

@@ -125,7 +125,8 @@ class SmoothingPlan:
 
     def __del__(self):  # pragma: no cover - interpreter shutdown order
         try:
-            self.close()
+            if not _lib.finalizing():
+                self.close()
         except Exception:
             pass
 

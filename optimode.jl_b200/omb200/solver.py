@@ -123,7 +123,8 @@ class Batch:
 
     def __del__(self):  # pragma: no cover
         try:
-            self.close()
+            if not _lib.finalizing():
+                self.close()
         except Exception:
             pass
 

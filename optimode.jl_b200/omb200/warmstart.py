@@ -134,7 +134,8 @@ class WarmStartNet:
 
     def __del__(self):  # pragma: no cover
         try:
-            self.close()
+            if not _lib.finalizing():
+                self.close()
         except Exception:
             pass
 

@@ -156,11 +156,34 @@ def test_gram_blocks_accuracy(n2, n):
         assert eg < tol and es < tol, (prec, eg, es)
 
 
+@pytest.mark.parametrize("Nx,Ny", [(24, 16), (40, 24), (12, 8), (128, 128), (192, 128), (256, 192)])
+def test_component_parallel_passes_match_oracle(omb, Nx, Ny):
+    """The component-parallel FP32 passes (row variant 3, column variants 3 and 4) against the
+    FP64 oracle at the FP32 tolerance, on radix-2/3/5 and non-square grids."""
+    import torch
+
+    from omb200 import ops
+    name = torch.cuda.get_device_name(0)
+    g = omb.Grid(6.0, 4.0, Nx, Ny)
+    og = O.Grid(6.0, 4.0, Nx, Ny)
+    ei = random_epsinv(Nx, Ny, seed=3)
+    H = rand_block(2 * g.N, 3, seed=Nx + Ny)
+    op = O.Operator(1.3, ei, og)
+    ref = np.stack([op.M(H[:, j]) for j in range(3)], axis=1)
+    try:
+        for r, c in ((3, 3), (3, 4), (3, 1), (1, 3)):
+            ops.tune_set(name, Nx, Ny, r, c, 0)
+            got = omb.apply_M(1.3, ei, g, H, precision="fp32")
+            assert rel(got, ref) <= TOL["fp32"], (r, c)
+    finally:
+        ops.tune_set(name, Nx, Ny, 1, 1, 0)
+
+
 def test_tile_variants_agree_and_autotune_picks_one():
     """Every tile variant of the FP32 M̂ passes gives the default tiles' result (the per-pixel
     arithmetic does not depend on the tiling); the wave variants (several launches per pass,
     which only the batched engine's many units reach) give the same eigensolves; the
-    autotuner times all 36 combinations and keeps the fastest."""
+    autotuner times all 80 combinations and keeps the fastest."""
     import torch
 
     import omb200
@@ -176,18 +199,19 @@ def test_tile_variants_agree_and_autotune_picks_one():
         H = rng.standard_normal((2 * g.N, 3)) + 1j * rng.standard_normal((2 * g.N, 3))
         ops.tune_set(name, Nx, Ny, 1, 1, 0)
         ref = omb200.apply_M(1.3, ei, g, H, precision="fp32")
-        for r in range(3):
-            for c in range(3):
+        for r in range(4):
+            for c in range(5):
                 ops.tune_set(name, Nx, Ny, r, c, 0)
                 got = omb200.apply_M(1.3, ei, g, H, precision="fp32")
                 assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-6, (Nx, Ny, r, c)
         probs = [{"omega": w, "eps_inv": ei, "grid": g, "nev": 3} for w in (0.62, 0.64, 0.66, 0.68)]
         ks = []
-        for w in (0, 1, 3):
-            ops.tune_set(name, Nx, Ny, 1, 1, w)
+        for r, c, w in ((1, 1, 0), (1, 1, 1), (1, 1, 3), (3, 3, 0), (3, 4, 2)):
+            ops.tune_set(name, Nx, Ny, r, c, w)
             res = omb200.solve_k_batch(probs, omb200.B200Solver(precision="mixed"))
             ks.append(np.array([km for km, _ in res]))
-        assert np.allclose(ks[1], ks[0], rtol=1e-10) and np.allclose(ks[2], ks[0], rtol=1e-10)
+        for kv in ks[1:]:
+            assert np.allclose(kv, ks[0], rtol=1e-10)
         r, c, w, t = ops.autotune(g)
         assert np.all(t > 0) and t[r, c, w] == t.min()
         assert ops.tune_get(name, Nx, Ny) == (r, c, w)
