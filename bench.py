@@ -579,7 +579,7 @@ def main():
             pb.close()
         # the same batch from the other starts: random (none) and the learned network
         arms = {}
-        for warm in ("none", "learned"):
+        for warm in ("none", "learned", "sweep_learned"):
             try:
                 ab = omb200.Batch(probs, omb200.B200Solver(precision="mixed", preconditioner="diag", newton="inner",
                                                            device=local, warm_start=warm))

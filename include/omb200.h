@@ -199,6 +199,9 @@ int omb_tune_load(const char* path, int32_t* entries);
                             (omb_ctx_set_warmstart): its (Hx, Hy) fields of bands 0..3 projected
                             on the plane waves at k = n_eff·ω, and those k as Newton starts;
                             the solve itself is unchanged (same tolerances)            */
+#define OMB_WARM_SWEEP_LEARNED 4 /* OMB_WARM_SWEEP whose first-solved instances (each sweep's
+                            anchor, and instances in no sweep) start from the learned network
+                            as with OMB_WARM_LEARNED                                    */
 
 typedef struct {
   double k_tol;           /* Newton tolerance on |Δk|                       (1e-8) */
@@ -213,7 +216,8 @@ typedef struct {
   uint64_t seed;          /* random start blocks                              (0)    */
   int32_t guard_bands;    /* extra block columns beyond the wanted bands of a
                              Newton track (OMB_NEWTON_INNER)                  (1)    */
-  int32_t warm_start;     /* OMB_WARM_NONE / OMB_WARM_SWEEP / OMB_WARM_CELLS  (NONE) */
+  int32_t warm_start;     /* OMB_WARM_NONE / _SWEEP / _CELLS / _LEARNED /
+                             _SWEEP_LEARNED                                   (NONE) */
 } omb_options;
 
 /* One solve_k problem: the lowest `nev` guided modes of one cell at frequency ω. */

@@ -54,10 +54,9 @@ static int options_from(const omb_options* o, SolveOptions& so) {
   so.seed = o->seed;
   if (o->guard_bands < 0 || o->guard_bands > 4) return fail(OMB_ERR_INVALID_ARG, "guard_bands must be in 0..4");
   so.guard = o->guard_bands;
-  if (o->warm_start != OMB_WARM_NONE && o->warm_start != OMB_WARM_SWEEP && o->warm_start != OMB_WARM_CELLS &&
-      o->warm_start != OMB_WARM_LEARNED)
+  if (o->warm_start < OMB_WARM_NONE || o->warm_start > OMB_WARM_SWEEP_LEARNED)
     return fail(OMB_ERR_INVALID_ARG,
-                "warm_start must be OMB_WARM_NONE, OMB_WARM_SWEEP, OMB_WARM_CELLS or OMB_WARM_LEARNED");
+                "warm_start must be OMB_WARM_NONE, _SWEEP, _CELLS, _LEARNED or _SWEEP_LEARNED");
   return OMB_OK;
 }
 
@@ -219,7 +218,8 @@ int omb_batch_run(omb_batch* b) {
   // warm-start groups (no warm start of their own, same grid and band count): a frequency
   // sweep shares one ε⁻¹ pointer; a stack of cells shares one ω
   std::vector<int> anchor(n_inst, -1);  // stage-2 instance → its stage-1 neighbour
-  if (b->warm == OMB_WARM_SWEEP || b->warm == OMB_WARM_CELLS) {
+  const bool learned = b->warm == OMB_WARM_LEARNED || b->warm == OMB_WARM_SWEEP_LEARNED;
+  if (b->warm == OMB_WARM_SWEEP || b->warm == OMB_WARM_CELLS || b->warm == OMB_WARM_SWEEP_LEARNED) {
     const bool cells = b->warm == OMB_WARM_CELLS;
     std::vector<std::vector<int>> groups;
     std::vector<int> gid(n_inst, -1);
@@ -256,24 +256,24 @@ int omb_batch_run(omb_batch* b) {
   OMB_CU(cudaEventCreate(&e0));
   OMB_CU(cudaEventCreate(&e1));
   OMB_CU(cudaEventRecord(e0, ctx->stream));
-  // learned warm start: the network's starting block and per-band k for every instance
-  // without guesses of its own on a grid the network reads
+  // learned warm start: the network's starting block and per-band k for every first-stage
+  // instance without guesses of its own on a grid the network reads
   std::vector<int> learned_of(n_inst, -1);
   std::vector<size_t> loff;
   std::vector<std::array<double, 4>> lk;
   b->learned_instances = 0;
-  if (b->warm == OMB_WARM_LEARNED) {
+  if (learned) {
     if (!ctx->ws) {
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
-      return fail(OMB_ERR_INVALID_ARG, "OMB_WARM_LEARNED needs a network attached with omb_ctx_set_warmstart");
+      return fail(OMB_ERR_INVALID_ARG, "a learned warm start needs a network attached with omb_ctx_set_warmstart");
     }
     std::vector<const Problem*> lp;
     std::vector<double> lw;
     for (int i = 0; i < n_inst; ++i) {
       const omb_instance& I = b->inst[i];
       const Problem& P = b->probs[b->pidx[i]];
-      if (I.nguess > 0 || !b->kbands[i].empty()) continue;
+      if (I.nguess > 0 || !b->kbands[i].empty() || anchor[i] >= 0) continue;
       if (!(P.Nx == P.Ny && (P.Nx == 128 || P.Nx == 256 || P.Nx == 512))) continue;
       learned_of[i] = (int)lp.size();
       lp.push_back(&P);

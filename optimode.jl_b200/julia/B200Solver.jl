@@ -55,7 +55,8 @@ end
 const _PREC = Dict(:fp32 => Int32(0), :fp64 => Int32(1), :mixed => Int32(2))
 const _PRECOND = Dict(:mpb => Int32(1), :diag => Int32(2))
 const _NEWTON = Dict(:inner => Int32(0), :outer => Int32(1))
-const _WARM = Dict(:none => Int32(0), :sweep => Int32(1), :cells => Int32(2), :learned => Int32(3))
+const _WARM = Dict(:none => Int32(0), :sweep => Int32(1), :cells => Int32(2), :learned => Int32(3),
+                   :sweep_learned => Int32(4))
 
 """
     B200Solver(; precision=:mixed, preconditioner=:diag, newton=:inner, device=0,
@@ -67,7 +68,8 @@ makes `solve_k_batch` start the instances that share one ε⁻¹ array from the 
 nearest their mean ω (a frequency sweep); `warm_start=:cells` starts instances that share ω
 from the middle one (the cells of an eigenmode expansion, `eme(...; warmstart=true)`);
 `warm_start=:learned` starts instances on 128², 256² or 512² grids from the learned network
-attached with `b200_attach_warmstart` (fields and n_eff of bands 0..3; same tolerances).
+attached with `b200_attach_warmstart` (fields and n_eff of bands 0..3; same tolerances);
+`warm_start=:sweep_learned` is `:sweep` with the first-solved instances started from the network.
 """
 struct B200Solver{L<:AbstractLogger} <: AbstractEigensolver{L}
     logger::L

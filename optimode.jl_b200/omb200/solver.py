@@ -16,7 +16,7 @@ from .ops import epsinv_host
 
 _PRECOND = {"mpb": 1, "diag": 2}
 _NEWTON = {"inner": 0, "outer": 1}
-_WARM = {"none": 0, "sweep": 1, "cells": 2, "learned": 3}
+_WARM = {"none": 0, "sweep": 1, "cells": 2, "learned": 3, "sweep_learned": 4}
 
 
 @dataclasses.dataclass(frozen=True)
@@ -37,7 +37,9 @@ class B200Solver:
       first and the others start from its eigenvectors and k (``OMB_WARM_CELLS``);
       ``"learned"``: problems on 128², 256² or 512² grids start from the learned network's fields and
       effective indices (``OMB_WARM_LEARNED``; the trained parameters committed with the
-      package, or a ``omb200.warmstart.WarmStartNet`` attached by the caller).
+      package, or a ``omb200.warmstart.WarmStartNet`` attached by the caller);
+      ``"sweep_learned"``: ``"sweep"`` whose first-solved instances (each sweep's anchor and
+      the instances in no sweep) start from the learned network (``OMB_WARM_SWEEP_LEARNED``).
     """
 
     precision: str = "mixed"
@@ -91,7 +93,7 @@ class Batch:
         self.solver = solver or B200Solver()
         self._lib = _lib.load()
         self._ctx = _lib.context(self.solver.device)
-        if self.solver.warm_start == "learned":
+        if self.solver.warm_start in ("learned", "sweep_learned"):
             from .warmstart import ensure_attached
             ensure_attached(self.solver.device)
         insts, results, keep, outs = _marshal(problems)
@@ -199,7 +201,7 @@ def solve_k_batch(problems, solver: B200Solver | None = None, k_tol=1e-8, eig_to
     solver = solver or B200Solver()
     lib = _lib.load()
     ctx = _lib.context(solver.device)
-    if solver.warm_start == "learned":
+    if solver.warm_start in ("learned", "sweep_learned"):
         from .warmstart import ensure_attached
         ensure_attached(solver.device)
     insts, results, keep, outs = _marshal(problems)

@@ -158,34 +158,39 @@ def heldout_problems(n: int, seed: int, ngrid: int = NGRID, device: int = 0):
     return probs
 
 
-def evaluate(probs, device: int = 0, d_omega: float = 0.01):
-    """Iterations to the 1e-8 tolerance and device seconds of one batched solve of `probs` from
-    three starts: random (``none``), the learned network (``learned``), and the previous
-    frequency's converged modes (``previous_omega``: each problem solved first at ω − d_omega,
-    untimed, then at ω from those eigenvectors and k·ω/ω_prev).  Every arm is checked to
-    converge every band, and the arms' k to agree."""
+def evaluate(probs, device: int = 0, d_omega: float = 0.01, chunk: int = 64):
+    """Iterations to the 1e-8 tolerance and device seconds of batched solves of `probs` (in
+    batches of `chunk` instances) from three starts: random (``none``), the learned network
+    (``learned``), and the previous frequency's converged modes (``previous_omega``: each
+    problem solved first at ω − d_omega, untimed, then at ω from those eigenvectors and
+    k·ω/ω_prev).  Every arm is checked to converge every band, and the arms' k to agree."""
     import omb200
     out = {}
     ks = {}
 
     def run(arm, problems, solver):
-        b = omb200.Batch(problems, solver)
-        b.run()
-        st = b.stats()
-        res, info = b.results(return_info=True, raise_on_failure=False)
-        b.close()
-        conv = int(sum(int(np.sum(i["status"] == 0)) for i in info))
-        its = [int(x) for i in info for x in i["iterations"]]
-        out[arm] = {"device_seconds": st["run_seconds"], "converged": conv, "modes": 4 * len(problems),
+        secs, conv, its, kk = 0.0, 0, [], []
+        for i in range(0, len(problems), chunk):
+            b = omb200.Batch(problems[i:i + chunk], solver)
+            b.run()
+            secs += b.stats()["run_seconds"]
+            res, info = b.results(return_info=True, raise_on_failure=False)
+            b.close()
+            conv += int(sum(int(np.sum(x["status"] == 0)) for x in info))
+            its += [int(x) for r in info for x in r["iterations"]]
+            kk += [r[0] for r in res]
+        out[arm] = {"device_seconds": secs, "converged": conv, "modes": 4 * len(problems),
                     "iterations_total": int(sum(its)), "iterations_mean": float(np.mean(its)),
                     "iterations_max": int(max(its))}
-        ks[arm] = np.array([r[0] for r in res])
-        return res
+        ks[arm] = np.array(kk)
 
     run("none", probs, omb200.B200Solver(precision="mixed", warm_start="none", device=device))
     run("learned", probs, omb200.B200Solver(precision="mixed", warm_start="learned", device=device))
     prev = [{**p, "omega": p["omega"] - d_omega} for p in probs]
-    pres = omb200.solve_k_batch(prev, omb200.B200Solver(precision="mixed", device=device), raise_on_failure=False)
+    pres = []
+    for i in range(0, len(prev), chunk):
+        pres += omb200.solve_k_batch(prev[i:i + chunk], omb200.B200Solver(precision="mixed", device=device),
+                                     raise_on_failure=False)
     warm = [{**p, "Hguess": np.stack(kv, axis=1), "kguess_bands": km * p["omega"] / q["omega"]}
             for p, q, (km, kv) in zip(probs, prev, pres)]
     run("previous_omega", warm, omb200.B200Solver(precision="mixed", warm_start="none", device=device))
@@ -206,6 +211,8 @@ def main():
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--out", default=WEIGHTS_PATH)
     ap.add_argument("--heldout", type=int, default=64, help="held-out cross-sections evaluated after training")
+    ap.add_argument("--heldout-256", type=int, default=None,
+                    help="held-out cross-sections on 256² grids (default: as --heldout)")
     args = ap.parse_args()
     print(f"generating {args.samples} samples (seed {args.seed})", flush=True)
     F, TF, TN, recs, t_gen = generate(args.samples, args.seed, device=args.device,
@@ -222,9 +229,10 @@ def main():
     print(f"final val loss {hist[-1]['val_loss']:.4f}; wrote {args.out}", flush=True)
     if args.heldout > 0:
         net.attach()
-        for ngrid in (128, 256):
-            ev = evaluate(heldout_problems(args.heldout, args.seed + 1000, ngrid, args.device), args.device)
-            print("heldout", json.dumps(ev), flush=True)
+        for ngrid, n in ((128, args.heldout), (256, args.heldout if args.heldout_256 is None else args.heldout_256)):
+            if n > 0:
+                ev = evaluate(heldout_problems(n, args.seed + 1000, ngrid, args.device), args.device)
+                print("heldout", json.dumps(ev), flush=True)
 
 
 if __name__ == "__main__":
