@@ -558,11 +558,19 @@ def main():
         peak, peak_kind = measured_peak_hbm()
         achieved = alg / t_apply / 1e9
         traffic = APPLY_TRAFFIC_BYTES
+        # the same launch against FP32 issue: nominal flops 5·N·log2(N) per complex 2D transform
+        # (six per column: three components, forward and inverse) + ≈60·N for the basis, curls
+        # and the ε⁻¹ contraction; FP32 peak from the SM count and the maximum SM clock
+        flops = (30.0 * N * np.log2(N) + 60.0 * N) * ncol * nbatch
+        fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "traffic": traffic,
                     "kernel": "operator apply M(k) (row_in + col + row_out, FP32), 4 columns x 64 cells",
                     "algorithmic_bytes_per_launch": alg, "seconds_per_launch": t_apply,
-                    "peak_source": peak_kind}
+                    "peak_source": peak_kind,
+                    "fp32": {"flops_per_launch": flops, "achieved_tflops": flops / t_apply / 1e12,
+                             "peak_tflops": fp32_peak, "frac": flops / t_apply / 1e12 / fp32_peak,
+                             "peak_source": "nominal: 148 SMs x 128 FP32 lanes x 2 x 1965 MHz"}}
         plain = None
         if not args.no_plain:
             # the reference loop's per-eigensolve budget is raised so that it converges

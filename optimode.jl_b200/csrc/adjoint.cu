@@ -20,6 +20,7 @@
 // eigenvalue ω² of the operator.  All recurrence scalars live in device memory; one
 // iteration is a fixed launch sequence replayed from a CUDA graph.
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <vector>
 
@@ -37,7 +38,8 @@ struct MinresState {
   double dot_ey_r, dot_ey_i, dot_ez_r, dot_ez_i;
   double rtol;
   double phibar_mark;  // phibar at itn_mark (stagnation test)
-  int itn, maxit, done, status;  // status: 0 running, 1 converged, 2 maxiter, 3 breakdown
+  int itn, maxit, done, status;  // status: 0 running, 1 converged, 2 maxiter, 3 breakdown,
+                                 // 4 maxiter with the residual below LOOSE_TOL
   int itn_mark;
 };
 
@@ -47,6 +49,11 @@ struct MinresState {
 // phibar ≤ STALL_TOL·β₁ and did not halve over the last STALL_WINDOW iterations.
 constexpr double STALL_TOL = 1e-10;
 constexpr int STALL_WINDOW = 50;
+// A solve that reaches its iteration cap is still accepted when its relative residual is
+// below √ε₆₄ ≈ 1.5e-8, the default relative tolerance of the reference's GMRES
+// (IterativeSolvers `gmres`, lib/MaxwellEigenmodes/src/grads/solve.jl:56-66, which returns
+// whatever it reached after maxiter = 1000).
+constexpr double LOOSE_TOL = 1.4901161193847656e-08;
 
 // block-reduce two complex partial sums (4 doubles) into part[blockIdx.x*4 + 0..3]
 __device__ __forceinline__ void block_reduce4(double a, double b, double c, double d, double* part) {
@@ -211,7 +218,7 @@ __global__ void k_minres_b_scalar(MinresState* S, const double* part, int nb) {
     S->itn_mark = S->itn;
   }
   if (S->beta == 0.0) { S->done = 2; S->status = 1; return; }                   // invariant subspace
-  if (S->itn >= S->maxit) { S->done = 2; S->status = 2; }
+  if (S->itn >= S->maxit) { S->done = 2; S->status = S->phibar <= LOOSE_TOL * S->beta1 ? 4 : 2; }
 }
 
 // w_k = (v − oldeps·w_{k−2} − delta·w_{k−1})/gamma ; x += phi·w_k ; v ← (z − ⟨e,z⟩e)/β_{k+1}
@@ -458,7 +465,7 @@ static int pullback_impl(omb_ctx* ctx, Problem& P, double omega, int nev, const 
       MinresState s0{};
       s0.shift = omega * omega;
       s0.rtol = 1e-12;
-      s0.maxit = 4 * std::max(O.maxiter, 300);
+      s0.maxit = std::max(4 * O.maxiter, 3000);
       OMB_CU(cudaMemcpyAsync(S.p, &s0, sizeof(s0), cudaMemcpyHostToDevice, st));
       k_minres_init<<<nb, ADJ_NT, 0, st>>>(V, eb.p, part.p);
       k_minres_init_scalar<<<1, 32, 0, st>>>(S.p, part.p, nb);
@@ -499,7 +506,12 @@ static int pullback_impl(omb_ctx* ctx, Problem& P, double omega, int nev, const 
       cudaGraphDestroy(graph);
       if (iterations) iterations[b] = sh.itn;
       if (sh.status == 3) return fail(OMB_ERR_NAN, "MINRES breakdown in the adjoint solve");
-      if (sh.status != 1) return fail(OMB_ERR_NOT_CONVERGED, "adjoint MINRES did not converge");
+      if (sh.status != 1 && sh.status != 4) {
+        char msg[160];
+        snprintf(msg, sizeof msg, "adjoint MINRES did not converge (band %d: relative residual %.3g after %d iterations)",
+                 b, sh.beta1 > 0 ? sh.phibar / sh.beta1 : 0.0, sh.itn);
+        return fail(OMB_ERR_NOT_CONVERGED, msg);
+      }
       // λ ⟂ h (re-projection against round-off), then Λd = fft(kx_tc λ) into SB
       k_dot_e<<<nb, ADJ_NT, 0, st>>>(ev.p, V.x, n2, part.p);
       k_sub_proj<<<nb, ADJ_NT, 0, st>>>(ev.p, V.x, n2, part.p, nb);
