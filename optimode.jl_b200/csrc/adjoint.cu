@@ -41,6 +41,7 @@ struct MinresState {
   int itn, maxit, done, status;  // status: 0 running, 1 converged, 2 maxiter, 3 breakdown,
                                  // 4 maxiter with the residual below LOOSE_TOL
   int itn_mark;
+  int flat_windows;  // consecutive windows in which phibar did not halve
 };
 
 // Below rtol the recurrence residual phibar can flatten at the rounding floor of the FP64
@@ -54,6 +55,12 @@ constexpr int STALL_WINDOW = 50;
 // (IterativeSolvers `gmres`, lib/MaxwellEigenmodes/src/grads/solve.jl:56-66, which returns
 // whatever it reached after maxiter = 1000).
 constexpr double LOOSE_TOL = 1.4901161193847656e-08;
+// Near-degenerate bands make (M̂ − ω²) ill-conditioned on the complement of the deflated
+// eigenvector, and the FP64 recurrence then flattens at ≈ε₆₄·cond above LOOSE_TOL.  A solve
+// whose phibar has not halved over FLAT_WINDOWS consecutive windows while below FLAT_TOL·β₁
+// ends there, accepted (status 4): more iterations would not lower it.
+constexpr double FLAT_TOL = 1e-6;
+constexpr int FLAT_WINDOWS = 4;
 
 // block-reduce two complex partial sums (4 doubles) into part[blockIdx.x*4 + 0..3]
 __device__ __forceinline__ void block_reduce4(double a, double b, double c, double d, double* part) {
@@ -130,6 +137,7 @@ __global__ void k_minres_init_scalar(MinresState* S, const double* part, int nb)
   S->phibar = S->beta1;
   S->phibar_mark = S->beta1;
   S->itn_mark = 0;
+  S->flat_windows = 0;
 }
 
 // v = (z − ⟨e,z⟩e)/beta  (start of the first iteration)
@@ -211,8 +219,13 @@ __global__ void k_minres_b_scalar(MinresState* S, const double* part, int nb) {
   if (!isfinite(S->phibar) || !isfinite(S->phi)) { S->done = 1; S->status = 3; return; }
   if (S->phibar <= S->rtol * S->beta1) { S->done = 2; S->status = 1; return; }  // finish this update
   if (S->itn - S->itn_mark >= STALL_WINDOW) {
-    if (S->phibar <= STALL_TOL * S->beta1 && S->phibar > 0.5 * S->phibar_mark) {
+    const bool flat = S->phibar > 0.5 * S->phibar_mark;
+    if (S->phibar <= STALL_TOL * S->beta1 && flat) {
       S->done = 2; S->status = 1; return;
+    }
+    S->flat_windows = flat ? S->flat_windows + 1 : 0;
+    if (S->flat_windows >= FLAT_WINDOWS && S->phibar <= FLAT_TOL * S->beta1) {
+      S->done = 2; S->status = 4; return;
     }
     S->phibar_mark = S->phibar;
     S->itn_mark = S->itn;

@@ -34,16 +34,18 @@ bool fft_size_supported(int L) {
   }
 }
 
-cudaError_t ensure_smem(const void* func, size_t bytes) {
+cudaError_t ensure_smem(const void* func, size_t bytes, bool max_shared) {
   static std::mutex mu;
   static std::map<std::pair<const void*, int>, size_t> done;
   int dev = 0;
   cudaGetDevice(&dev);
   std::lock_guard<std::mutex> lk(mu);
   size_t& have = done[{func, dev}];
-  if (have >= bytes) return cudaSuccess;
+  if (have >= bytes && have > 0) return cudaSuccess;
   cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  if (e == cudaSuccess) have = bytes;
+  if (e == cudaSuccess && max_shared)
+    e = cudaFuncSetAttribute(func, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+  if (e == cudaSuccess) have = bytes > 0 ? bytes : 1;
   return e;
 }
 

@@ -206,9 +206,10 @@ __device__ __forceinline__ void pointwise_at(const OpUnit<T>& U, size_t p, cplx<
 
 // ------------------------------------------------------------------------------------
 // col.  Grid: (ceil(Nx/TX), max columns, units); l2_col_threads(NY) threads.
-template <typename T, int NY, int S1, int PW, int S2, int TX = l2_tx<T>(NY)>
-__global__ void __launch_bounds__(l2_col_threads_tx(NY, TX),
-                                  sizeof(T) == 4 ? (384 / l2_col_threads_tx(NY, TX) > 1 ? 384 / l2_col_threads_tx(NY, TX) : 1) : 1)
+// (MINB: CTAs per SM the register budget is set for)
+template <typename T, int NY, int S1, int PW, int S2, int TX = l2_tx<T>(NY),
+          int MINB = sizeof(T) == 4 ? (384 / l2_col_threads_tx(NY, TX) > 1 ? 384 / l2_col_threads_tx(NY, TX) : 1) : 1>
+__global__ void __launch_bounds__(l2_col_threads_tx(NY, TX), MINB)
     k_col2(const OpUnit<T>* __restrict__ units, const cplx<T>* __restrict__ tw_g) {
   using C = cplx<T>;
   constexpr int A = plan2_a(NY), B = NY / A, NT = l2_col_threads_tx(NY, TX);

@@ -27,24 +27,26 @@ struct TwTables {
 bool fft_size_supported(int L);
 
 // Tile variants of the FP32 M̂ passes (0, 1, 2: half, default, double the rows per CTA of the
-// row passes / columns per CTA of the column pass; 3: the default tile with one thread per
-// line slot and field component; column variant 4: as 3 with two CTAs' register budget per
-// SM) and the wave size (0: every column in one
+// row passes / columns per CTA of the column pass; row 3: row_in with one thread per line
+// slot and field component, row 4: both row passes so; column 3 and 4: the column pass so,
+// with a register budget for three or two CTAs per SM; column 5: the default tile with a
+// budget for four) and the wave size (0: every column in one
 // launch of each pass; w > 0: the units are cut into waves of about wave_columns(w) columns,
 // each wave running its three passes while its intermediate stays in L2), chosen per grid by
 // the autotuner (tune.cu); grids never tuned use the defaults.
 struct TileChoice {
   int row = 1, col = 1, wave = 0;
 };
-constexpr int ROW_VARIANTS = 4;
-constexpr int COL_VARIANTS = 5;
+constexpr int ROW_VARIANTS = 5;
+constexpr int COL_VARIANTS = 6;
 constexpr int WAVE_VARIANTS = 4;
 __host__ __device__ constexpr int wave_columns(int w) { return w == 1 ? 32 : w == 2 ? 64 : w == 3 ? 128 : 0; }
 TileChoice tiles_for(int Nx, int Ny);  // for the calling thread's current device
-// Raise a kernel's dynamic shared-memory limit once per (kernel, device); later calls for
-// the same or a smaller size return without touching the driver (so they are safe inside
-// a stream capture after a warm-up launch).
-cudaError_t ensure_smem(const void* func, size_t bytes);
+// Raise a kernel's dynamic shared-memory limit once per (kernel, device), and with
+// `max_shared` ask for the whole L1/shared carve-out; later calls for the same or a smaller
+// size return without touching the driver (so they are safe inside a stream capture after a
+// warm-up launch).
+cudaError_t ensure_smem(const void* func, size_t bytes, bool max_shared = false);
 // Number of row blocks row_out uses for a grid with Ny rows (partial sums per column).
 int row_blocks(int Nx, int Ny);
 

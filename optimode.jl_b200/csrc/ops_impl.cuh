@@ -25,9 +25,9 @@ using PassKernel = void (*)(const OpUnit<T>*, const cplx<T>*);
 
 template <typename T>
 static cudaError_t launch_pass(PassKernel<T> kern, dim3 g, int nt, size_t smem, cudaStream_t st,
-                               const OpUnit<T>* units, const cplx<T>* tw) {
-  if (smem > 32 * 1024) {  // the default limit counts static shared memory too
-    cudaError_t e = ensure_smem(reinterpret_cast<const void*>(kern), smem);
+                               const OpUnit<T>* units, const cplx<T>* tw, bool max_shared = false) {
+  if (smem > 32 * 1024 || max_shared) {  // the default limit counts static shared memory too
+    cudaError_t e = ensure_smem(reinterpret_cast<const void*>(kern), smem, max_shared);
     if (e != cudaSuccess) return e;
   }
   kern<<<g, nt, smem, st>>>(units, tw);
@@ -35,9 +35,12 @@ static cudaError_t launch_pass(PassKernel<T> kern, dim3 g, int nt, size_t smem, 
 }
 
 // Tunable tiles (FP32, the eigensolver's M̂ passes): row passes with G/2, G or 2G rows per CTA,
-// the column pass with TX/2, TX or 2·TX columns (variant 0, 1, 2; 1 is the default); variant 3
-// is the component-parallel form of the default tile (op_kernels_split.cuh), and column
-// variant 4 the same with a register budget for two CTAs per SM instead of three.
+// the column pass with TX/2, TX or 2·TX columns (variant 0, 1, 2; 1 is the default); row
+// variant 3 runs row_in in the component-parallel form (op_kernels_split.cuh) and row_out in the
+// default one, row variant 4 both passes in the component-parallel form; column variants 3 and
+// 4 are the component-parallel column pass with a register budget for three or two CTAs per
+// SM, and column variant 5 the default tile with a budget for four (and the whole
+// shared-memory carve-out).
 template <int NX> __host__ __device__ constexpr int row_g_variant(int v) {
   return v == 0 ? (l2_rows(NX) / 2 > 0 ? l2_rows(NX) / 2 : 1) : (v == 2 ? 2 * l2_rows(NX) : l2_rows(NX));
 }
@@ -56,6 +59,15 @@ static cudaError_t row_out_g(const OpUnit<T>* u, int nunits, int Ny, int maxcol,
   const size_t sm = (size_t)3 * G * l2_row_lstr<cplx<T>, NX>() * sizeof(cplx<T>);
   const dim3 g((Ny + G - 1) / G, maxcol, nunits);
   return launch_pass<T>(k_row_out2<T, NX, MODE, INV, G>, g, NT, sm, st, u, tw);
+}
+// the default tile with a register budget for four CTAs per SM and the whole shared-memory
+// carve-out (four 53 KB blocks)
+template <int NY, int S1, int PW, int S2>
+static cudaError_t col_b4(const OpUnit<float>* u, int nunits, int Nx, int maxcol, const float2* tw, cudaStream_t st) {
+  constexpr int TX = l2_tx<float>(NY), NT = l2_col_threads_tx(NY, TX);
+  const size_t sm = (size_t)3 * TX * l2_col_lstr<float2, NY, TX>() * sizeof(float2);
+  const dim3 g((Nx + TX - 1) / TX, maxcol, nunits);
+  return launch_pass<float>(k_col2<float, NY, S1, PW, S2, TX, 4>, g, NT, sm, st, u, tw, true);
 }
 template <typename T, int NY, int TX, int S1, int PW, int S2>
 static cudaError_t col_tx(const OpUnit<T>* u, int nunits, int Nx, int maxcol, const cplx<T>* tw, cudaStream_t st) {
@@ -91,7 +103,7 @@ template <typename T, int NX>
 static cudaError_t row_in_nx(int mode, const OpUnit<T>* u, int nunits, int Ny, int maxcol,
                              const cplx<T>* tw, cudaStream_t st, int gv = 1) {
   if constexpr (plan2_a(NX) != 0 && sizeof(T) == 4) {
-    if (mode == RI_KXTC && gv == 3)
+    if (mode == RI_KXTC && (gv == 3 || gv == 4))
       return row_in_sp<NX, RI_KXTC, false>(reinterpret_cast<const OpUnit<float>*>(u), nunits, Ny, maxcol,
                                            reinterpret_cast<const float2*>(tw), st);
     if (mode == RI_KXTC && gv != 1)
@@ -131,9 +143,11 @@ static cudaError_t row_out_nx(int mode, const OpUnit<T>* u, int nunits, int Ny, 
   if constexpr (plan2_a(NX) != 0 && sizeof(T) == 4) {
     // (the dot-product mode keeps the default rows: its partial sums are laid out per row block)
     if (mode == RO_KXCT && gv == 3)
+      return row_out_nx<T, NX>(mode, u, nunits, Ny, maxcol, tw, st, 1);
+    if (mode == RO_KXCT && gv == 4)
       return row_out_sp<NX, RO_KXCT, true>(reinterpret_cast<const OpUnit<float>*>(u), nunits, Ny, maxcol,
                                            reinterpret_cast<const float2*>(tw), st);
-    if (mode == RO_KXCT_DOT && gv == 3)
+    if (mode == RO_KXCT_DOT && gv == 4)
       return row_out_sp<NX, RO_KXCT_DOT, true>(reinterpret_cast<const OpUnit<float>*>(u), nunits, Ny, maxcol,
                                                reinterpret_cast<const float2*>(tw), st);
     if (mode == RO_KXCT && gv != 1)
@@ -172,6 +186,9 @@ template <typename T, int NY>
 static cudaError_t col_ny(int mode, const OpUnit<T>* u, int nunits, int Nx, int maxcol,
                           const cplx<T>* tw, cudaStream_t st, int tv = 1) {
   if constexpr (plan2_a(NY) != 0 && sizeof(T) == 4) {
+    if (mode == CM_M && tv == 5)
+      return col_b4<NY, CS_FWD, PW_EPS, CS_INV>(reinterpret_cast<const OpUnit<float>*>(u), nunits, Nx, maxcol,
+                                                reinterpret_cast<const float2*>(tw), st);
     if (mode == CM_M && (tv == 3 || tv == 4)) {
       const auto* uf = reinterpret_cast<const OpUnit<float>*>(u);
       const auto* tf = reinterpret_cast<const float2*>(tw);
@@ -261,7 +278,7 @@ cudaError_t launch_op(OpKind op, const OpUnit<T>* u, int nunits, int Nx, int Ny,
         OMB_TRY(row_in<T>(RI_KXTC, u + u0, n, Nx, Ny, maxcol, t, st, tc.row));
         OMB_TRY(col<T>(CM_M, u + u0, n, Nx, Ny, maxcol, t, st, tc.col));
         OMB_TRY(op == OP_M ? row_out<T>(RO_KXCT, u + u0, n, Nx, Ny, maxcol, t, st, tc.row)
-                           : row_out<T>(RO_KXCT_DOT, u + u0, n, Nx, Ny, maxcol, t, st, tc.row == 3 ? 3 : 1));
+                           : row_out<T>(RO_KXCT_DOT, u + u0, n, Nx, Ny, maxcol, t, st, tc.row == 4 ? 4 : 1));
       }
       return cudaSuccess;
     }
@@ -274,7 +291,7 @@ cudaError_t launch_op(OpKind op, const OpUnit<T>* u, int nunits, int Nx, int Ny,
     case OP_MDOT:
       OMB_TRY(row_in<T>(RI_KXTC, u, nunits, Nx, Ny, maxcol, t, st, tc.row));
       OMB_TRY(col<T>(CM_M, u, nunits, Nx, Ny, maxcol, t, st, tc.col));
-      return row_out<T>(RO_KXCT_DOT, u, nunits, Nx, Ny, maxcol, t, st, tc.row == 3 ? 3 : 1);
+      return row_out<T>(RO_KXCT_DOT, u, nunits, Nx, Ny, maxcol, t, st, tc.row == 4 ? 4 : 1);
     case OP_P:
       OMB_TRY(row_in<T>(RI_KXINV, u, nunits, Nx, Ny, maxcol, t, st));
       OMB_TRY(col<T>(CM_P, u, nunits, Nx, Ny, maxcol, t, st));

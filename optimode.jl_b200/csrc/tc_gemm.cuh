@@ -186,19 +186,58 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     float v[16];
     tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);  // warp-collective
     if (failed || row >= g.M) continue;
+    const int nb = n0 + c0;
+    if (nb >= g.N) continue;
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
-      const int n = n0 + c0 + j;
-      if (n >= g.N) break;
       float x = v[j];
-      if (g.bias) x += g.bias[n];
+      if (g.bias && nb + j < g.N) x += g.bias[nb + j];
       if (g.relu) x = fmaxf(x, 0.f);
-      if (g.epi == TC_STORE_F32) {
-        static_cast<float*>(g.D)[(size_t)row * g.ldd + n] = x;
-      } else if (g.epi == TC_STORE_BF16) {
-        static_cast<__nv_bfloat16*>(g.D)[(size_t)row * g.ldd + n] = __float2bfloat16_rn(x);
+      v[j] = x;
+    }
+    // a thread's 16 consecutive outputs of its row: whole 16-byte vectors when they are all in
+    // range and aligned (full 32-byte sectors per thread instead of 16 scattered scalars)
+    const size_t off = (size_t)row * g.ldd + nb;
+    if (g.epi == TC_STORE_BF16) {
+      __nv_bfloat16* dst = static_cast<__nv_bfloat16*>(g.D) + off;
+      if (nb + 16 <= g.N && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+        uint4 q[2];
+        uint32_t* w = reinterpret_cast<uint32_t*>(q);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * j], v[2 * j + 1]);
+          w[j] = *reinterpret_cast<const uint32_t*>(&h);
+        }
+        reinterpret_cast<uint4*>(dst)[0] = q[0];
+        reinterpret_cast<uint4*>(dst)[1] = q[1];
       } else {
-        atomicAdd(static_cast<float*>(g.D) + (size_t)row * g.ldd + n, x);
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+          if (nb + j < g.N) dst[j] = __float2bfloat16_rn(v[j]);
+      }
+    } else {
+      float* dst = static_cast<float*>(g.D) + off;
+      const bool vec = nb + 16 <= g.N && (reinterpret_cast<uintptr_t>(dst) & 15) == 0;
+      if (g.epi == TC_STORE_F32) {
+        if (vec) {
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            reinterpret_cast<float4*>(dst)[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+        } else {
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+            if (nb + j < g.N) dst[j] = v[j];
+        }
+      } else {
+        if (vec) {
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            atomicAdd(reinterpret_cast<float4*>(dst) + j, make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]));
+        } else {
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+            if (nb + j < g.N) atomicAdd(dst + j, v[j]);
+        }
       }
     }
   }

@@ -10,10 +10,10 @@ from omb200 import ops
 
 def test_tune_table_round_trip(tmp_path):
     ops.tune_clear()
-    ops.tune_set("NVIDIA B200", 256, 256, 3, 4, 3)
+    ops.tune_set("NVIDIA B200", 256, 256, 4, 5, 3)
     ops.tune_set("NVIDIA B200", 128, 192, 0, 1)
     ops.tune_set("Other GPU", 256, 256, 1, 2, 1)
-    assert ops.tune_get("NVIDIA B200", 256, 256) == (3, 4, 3)
+    assert ops.tune_get("NVIDIA B200", 256, 256) == (4, 5, 3)
     assert ops.tune_get("Other GPU", 256, 256) == (1, 2, 1)
     p = tmp_path / "sub" / "tiles.txt"
     ops.tune_save(str(p))
@@ -36,9 +36,9 @@ def test_tune_table_round_trip(tmp_path):
 
 def test_tune_rejects_bad_entries():
     with pytest.raises(ops._lib.OmbError):
-        ops.tune_set("NVIDIA B200", 256, 256, 4, 0)
+        ops.tune_set("NVIDIA B200", 256, 256, 5, 0)
     with pytest.raises(ops._lib.OmbError):
-        ops.tune_set("NVIDIA B200", 256, 256, 1, 5)
+        ops.tune_set("NVIDIA B200", 256, 256, 1, 6)
     with pytest.raises(ops._lib.OmbError):
         ops.tune_set("", 256, 256, 1, 1)
     with pytest.raises(ops._lib.OmbError):
