@@ -3,7 +3,7 @@
 //   D[M×N] (=, +=) A[M×K] · B[N×K]ᵀ   (+ bias[N], ReLU), A and B row-major bf16 ("K-major")
 //
 // One CTA of 128 threads computes a 128×BN tile of D over a range of K (split-K CTAs add
-// their partial tiles atomically into an FP32 D):
+// their partial tiles atomically into an FP32 D); two or more CTAs share an SM:
 //   * warp 0, one lane: TMA producer.  Per 64-wide K step it loads the 128×64 A box and the
 //     BN×64 B box (128-byte swizzle, the canonical K-major UMMA layout) into one stage of a
 //     ring, completing on the stage's `full` mbarrier;
@@ -28,8 +28,12 @@ namespace omb {
 
 constexpr int TC_BM = 128;       // rows per CTA tile (UMMA M)
 constexpr int TC_BK = 64;        // K per stage: one 128-byte swizzle row of bf16
-constexpr int TC_STAGES = 4;
+constexpr int TC_MAX_STAGES = 3;
 constexpr int TC_THREADS = 128;
+// Ring depth: two stages for the widest tiles and three otherwise, so that at least two CTAs
+// fit an SM (≤ 97 KB of shared memory each, ≤ 256 TMEM columns each) and one CTA's epilogue
+// overlaps another's main loop.
+__host__ __device__ constexpr int tc_stages(int BN) { return BN >= 256 ? 2 : 3; }
 
 struct TcGemmArgs {
   void* D;              // output, row-major, leading dimension ldd (elements)
@@ -105,12 +109,14 @@ __host__ __device__ constexpr uint32_t tc_idesc(int BN) {
 }
 __host__ __device__ constexpr uint32_t tc_tmem_cols(int BN) { return BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256; }
 __host__ __device__ constexpr size_t tc_stage_bytes(int BN) { return (size_t)TC_BM * 128 + (size_t)BN * 128; }
-__host__ __device__ constexpr size_t tc_smem_bytes(int BN) { return 1024 + TC_STAGES * tc_stage_bytes(BN) + 256; }
+__host__ __device__ constexpr size_t tc_smem_bytes(int BN) { return 1024 + tc_stages(BN) * tc_stage_bytes(BN) + 256; }
 
 template <int BN>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, TcGemmArgs g) {
   static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "UMMA N for M = 128");
+  constexpr int TC_STAGES = tc_stages(BN);
+  static_assert(TC_STAGES <= TC_MAX_STAGES, "ring depth");
   extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
   // 1024-byte aligned ring (the swizzle pattern repeats every 1024 B)
   unsigned char* base = reinterpret_cast<unsigned char*>(
@@ -142,7 +148,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 
   if (warp == 0 && lane == 0) {
     // ---- TMA producer
-    int issued[TC_STAGES] = {0, 0, 0, 0};
+    int issued[TC_STAGES] = {};
     for (int i = 0; i < nk; ++i) {
       const int s = i % TC_STAGES;
       if (!mbar_wait(&empty[s], ((i / TC_STAGES) & 1) ^ 1, g.wait_ns)) { pipe_fail(g.err, PIPE_EMPTY_TIMEOUT); break; }
