@@ -49,6 +49,37 @@ cudaError_t ensure_smem(const void* func, size_t bytes, bool max_shared) {
   return e;
 }
 
+int cluster_slots(const void* func, int cluster_ctas, int threads, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, int> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = done.find({func, dev});
+  if (it != done.end()) return it->second;
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cluster_ctas * (sms / cluster_ctas > 0 ? sms / cluster_ctas : 1), 1, 1);
+  cfg.blockDim = dim3(threads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = cluster_ctas;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, func, &cfg) != cudaSuccess || n < 1) {
+    cudaGetLastError();  // a failed query leaves no sticky error; fall back to one per SM group
+    n = sms / cluster_ctas > 0 ? sms / cluster_ctas : 1;
+  }
+  return done[{func, dev}] = n;
+}
+
+bool cluster_apply_available(int Nx, int Ny) { return Nx == 256 && Ny == 256; }
+
 namespace {
 struct BigBlock {
   void* p = nullptr;

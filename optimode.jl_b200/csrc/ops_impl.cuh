@@ -1,6 +1,9 @@
 // Size/mode dispatch for the fused operator passes.  Included once per precision.
 #pragma once
 
+#include <algorithm>
+
+#include "op_cluster.cuh"
 #include "op_kernels_2l.cuh"
 #include "op_kernels_split.cuh"
 #include "ops.h"
@@ -265,11 +268,34 @@ static cudaError_t col(int mode, const OpUnit<T>* u, int nunits, int Nx, int Ny,
 
 #define OMB_TRY(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) return e_; } while (0)
 
+// The one-kernel cluster apply (op_cluster.cuh): a persistent grid of as many 8-CTA clusters
+// as can be resident, never more than there are (unit, column) pairs.
+template <int NX, int NY>
+static cudaError_t cluster_apply(const OpUnit<float>* u, int nunits, int maxcol, const float2* twx,
+                                 const float2* twy, cudaStream_t st) {
+  using S = ClShape<NX, NY>;
+  const void* kern = reinterpret_cast<const void*>(k_apply_cluster<NX, NY>);
+  cudaError_t e = ensure_smem(kern, S::SMEM, true);
+  if (e != cudaSuccess) return e;
+  const long long total = (long long)nunits * maxcol;
+  const long long ncl = std::min<long long>(cluster_slots(kern, CL_CTAS, CL_THREADS, S::SMEM), total);
+  k_apply_cluster<NX, NY><<<(unsigned)(ncl * CL_CTAS), CL_THREADS, S::SMEM, st>>>(u, nunits, maxcol, twx, twy);
+  return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t launch_op(OpKind op, const OpUnit<T>* u, int nunits, int Nx, int Ny, int maxcol,
                       const TwTables& t, cudaStream_t st) {
   if (nunits <= 0 || maxcol <= 0) return cudaSuccess;
-  const TileChoice tc = sizeof(T) == 4 ? tiles_for(Nx, Ny) : TileChoice{};
+  TileChoice tc = sizeof(T) == 4 ? tiles_for(Nx, Ny) : TileChoice{};
+  if (tc.row == ROW_CLUSTER) {
+    if constexpr (sizeof(T) == 4) {
+      if (op == OP_M && Nx == 256 && Ny == 256)
+        return cluster_apply<256, 256>(reinterpret_cast<const OpUnit<float>*>(u), nunits, maxcol, t.f32[256],
+                                       t.f32[256], st);
+    }
+    tc = TileChoice{};  // the other pipelines keep the default tiles
+  }
   if (tc.wave > 0 && (op == OP_M || op == OP_MDOT)) {
     const int per = wave_columns(tc.wave) / maxcol > 0 ? wave_columns(tc.wave) / maxcol : 1;
     if (per < nunits) {
