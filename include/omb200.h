@@ -146,9 +146,9 @@ int omb_apply_M_noalloc(int32_t Nx, int32_t Ny, double Dx, double Dy, double k, 
  * planning at ModeSolver construction, lib/MaxwellEigenmodes/src/maxwell.jl:940-943).
  * Per (device name, Nx, Ny) the combinations of row-pass variant (0, 1, 2: half, default,
  * double the grid rows per CTA; 3: default rows, row_in with one thread per line slot and field
- * component; 4: both row passes so; 5: the whole application in one kernel on 8-CTA
- * thread-block clusters, the field held in distributed shared memory, where the grid has it:
- * 256 × 256 — timed once, its column and wave slots report -1), column-pass variant (0, 1, 2: 4, 8, 16 columns per CTA;
+ * component; 4: both row passes so; 5, 6: the whole application in one kernel on thread-block
+ * clusters of 8 or 16 CTAs, the field held in distributed shared memory, where the grid has it:
+ * 256 × 256 — each timed once, their column and wave slots report -1), column-pass variant (0, 1, 2: 4, 8, 16 columns per CTA;
  * 3, 4: 8 columns, one thread per slot and component, with a register budget for three or two
  * CTAs per SM; 5: 8 columns with a budget for four) and
  * wave variant (0: all columns in one launch per pass; 1, 2, 3: waves of 32, 64, 128 columns,
@@ -160,7 +160,7 @@ int omb_apply_M_noalloc(int32_t Nx, int32_t Ny, double Dx, double Dy, double k, 
  * --------------------------------------------------------------------------------- */
 
 /* Tune one grid now for `ncol`-column applications on 64 units; the chosen variants and, if
- * `seconds` is not NULL, the 144 timings (row-major over row, column, wave variant; -1 for
+ * `seconds` is not NULL, the 168 timings (row-major over row, column, wave variant; -1 for
  * combinations not timed). */
 int omb_autotune(omb_ctx* ctx, const omb_grid* grid, int32_t ncol, int32_t* row_variant, int32_t* col_variant,
                  int32_t* wave_variant, double* seconds);

@@ -15,10 +15,30 @@ template <typename T> using cplx = typename cplx_t<T>::type;
 template <typename C> __host__ __device__ __forceinline__ C mk(decltype(C::x) a, decltype(C::x) b) {
   C r; r.x = a; r.y = b; return r;
 }
-__host__ __device__ __forceinline__ float2 operator+(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__host__ __device__ __forceinline__ float2 operator-(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-__host__ __device__ __forceinline__ float2 operator*(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
-__host__ __device__ __forceinline__ float2 operator*(float s, float2 a) { return make_float2(a.x * s, a.y * s); }
+// FP32 complex arithmetic: on the device the sm_100 packed two-lane instructions (one issue
+// slot for both halves, each half rounded like the scalar operation).
+__host__ __device__ __forceinline__ float2 operator+(float2 a, float2 b) {
+#ifdef __CUDA_ARCH__
+  return __fadd2_rn(a, b);
+#else
+  return make_float2(a.x + b.x, a.y + b.y);
+#endif
+}
+__host__ __device__ __forceinline__ float2 operator-(float2 a, float2 b) {
+#ifdef __CUDA_ARCH__
+  return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+#else
+  return make_float2(a.x - b.x, a.y - b.y);
+#endif
+}
+__host__ __device__ __forceinline__ float2 operator*(float2 a, float s) {
+#ifdef __CUDA_ARCH__
+  return __fmul2_rn(a, make_float2(s, s));
+#else
+  return make_float2(a.x * s, a.y * s);
+#endif
+}
+__host__ __device__ __forceinline__ float2 operator*(float s, float2 a) { return a * s; }
 __host__ __device__ __forceinline__ double2 operator+(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __host__ __device__ __forceinline__ double2 operator-(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 __host__ __device__ __forceinline__ double2 operator*(double2 a, double s) { return make_double2(a.x * s, a.y * s); }

@@ -30,17 +30,17 @@ bool fft_size_supported(int L);
 // row passes / columns per CTA of the column pass; row 3: row_in with one thread per line
 // slot and field component, row 4: both row passes so; column 3 and 4: the column pass so,
 // with a register budget for three or two CTAs per SM; column 5: the default tile with a
-// budget for four; row 5: the whole M̂ application in one kernel on 8-CTA thread-block
-// clusters (op_cluster.cuh) where the grid has that kernel, the column and wave choices then
-// unused) and the wave size (0: every column in one
+// budget for four; rows 5 and 6: the whole M̂ application in one kernel on thread-block
+// clusters of 8 or 16 CTAs (op_cluster.cuh) where the grid has that kernel, the column and
+// wave choices then unused) and the wave size (0: every column in one
 // launch of each pass; w > 0: the units are cut into waves of about wave_columns(w) columns,
 // each wave running its three passes while its intermediate stays in L2), chosen per grid by
 // the autotuner (tune.cu); grids never tuned use the defaults.
 struct TileChoice {
   int row = 1, col = 1, wave = 0;
 };
-constexpr int ROW_VARIANTS = 6;
-constexpr int ROW_CLUSTER = 5;
+constexpr int ROW_VARIANTS = 7;
+constexpr int ROW_CLUSTER = 5, ROW_CLUSTER16 = 6;
 constexpr int COL_VARIANTS = 6;
 constexpr int WAVE_VARIANTS = 4;
 __host__ __device__ constexpr int wave_columns(int w) { return w == 1 ? 32 : w == 2 ? 64 : w == 3 ? 128 : 0; }

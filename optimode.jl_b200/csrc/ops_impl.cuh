@@ -2,6 +2,7 @@
 #pragma once
 
 #include <algorithm>
+#include <mutex>
 
 #include "op_cluster.cuh"
 #include "op_kernels_2l.cuh"
@@ -268,19 +269,43 @@ static cudaError_t col(int mode, const OpUnit<T>* u, int nunits, int Nx, int Ny,
 
 #define OMB_TRY(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) return e_; } while (0)
 
-// The one-kernel cluster apply (op_cluster.cuh): a persistent grid of as many 8-CTA clusters
-// as can be resident, never more than there are (unit, column) pairs.
-template <int NX, int NY>
+// The one-kernel cluster apply (op_cluster.cuh): a persistent grid of as many CTAS-CTA
+// clusters as can be resident, never more than there are (unit, column) pairs.
+template <int NX, int NY, int CTAS>
 static cudaError_t cluster_apply(const OpUnit<float>* u, int nunits, int maxcol, const float2* twx,
                                  const float2* twy, cudaStream_t st) {
-  using S = ClShape<NX, NY>;
-  const void* kern = reinterpret_cast<const void*>(k_apply_cluster<NX, NY>);
-  cudaError_t e = ensure_smem(kern, S::SMEM, true);
+  using S = ClShape<NX, NY, CTAS>;
+  auto kern = k_apply_cluster<NX, NY, CTAS>;
+  const void* kp = reinterpret_cast<const void*>(kern);
+  cudaError_t e = ensure_smem(kp, S::SMEM, true);
   if (e != cudaSuccess) return e;
+  if (CTAS > 8) {  // above the portable cluster size (set once; later calls find it set)
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev < 64 && !done[dev]) {
+      e = cudaFuncSetAttribute(kp, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+      if (e != cudaSuccess) return e;
+      done[dev] = true;
+    }
+  }
   const long long total = (long long)nunits * maxcol;
-  const long long ncl = std::min<long long>(cluster_slots(kern, CL_CTAS, CL_THREADS, S::SMEM), total);
-  k_apply_cluster<NX, NY><<<(unsigned)(ncl * CL_CTAS), CL_THREADS, S::SMEM, st>>>(u, nunits, maxcol, twx, twy);
-  return cudaGetLastError();
+  const long long ncl = std::min<long long>(cluster_slots(kp, CTAS, S::THREADS, S::SMEM), total);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(ncl * CTAS), 1, 1);
+  cfg.blockDim = dim3(S::THREADS, 1, 1);
+  cfg.dynamicSmemBytes = S::SMEM;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = CTAS;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, u, nunits, maxcol, twx, twy);
 }
 
 template <typename T>
@@ -288,11 +313,13 @@ cudaError_t launch_op(OpKind op, const OpUnit<T>* u, int nunits, int Nx, int Ny,
                       const TwTables& t, cudaStream_t st) {
   if (nunits <= 0 || maxcol <= 0) return cudaSuccess;
   TileChoice tc = sizeof(T) == 4 ? tiles_for(Nx, Ny) : TileChoice{};
-  if (tc.row == ROW_CLUSTER) {
+  if (tc.row == ROW_CLUSTER || tc.row == ROW_CLUSTER16) {
     if constexpr (sizeof(T) == 4) {
-      if (op == OP_M && Nx == 256 && Ny == 256)
-        return cluster_apply<256, 256>(reinterpret_cast<const OpUnit<float>*>(u), nunits, maxcol, t.f32[256],
-                                       t.f32[256], st);
+      if (op == OP_M && Nx == 256 && Ny == 256) {
+        const auto* uf = reinterpret_cast<const OpUnit<float>*>(u);
+        return tc.row == ROW_CLUSTER ? cluster_apply<256, 256, 8>(uf, nunits, maxcol, t.f32[256], t.f32[256], st)
+                                     : cluster_apply<256, 256, 16>(uf, nunits, maxcol, t.f32[256], t.f32[256], st);
+      }
     }
     tc = TileChoice{};  // the other pipelines keep the default tiles
   }

@@ -141,7 +141,7 @@ bool tune_known(int dev, int Nx, int Ny) {
   return g_tune.count(TuneKey{name, Nx, Ny}) > 0;
 }
 
-// Times the tile × wave variants (144 slots; the cluster apply once) of one FP32 M̂ application to `ncol` columns on `units`
+// Times the tile × wave variants (168 slots; each cluster apply once) of one FP32 M̂ application to `ncol` columns on `units`
 // copies of a uniform cell and records the fastest.
 int autotune_grid(omb_ctx* ctx, const omb_grid* g, int ncol, int units, TileChoice* best, double* times) {
   int rc = check_grid(g);
@@ -186,7 +186,7 @@ int autotune_grid(omb_ctx* ctx, const omb_grid* g, int ncol, int units, TileChoi
   for (int r = 0; r < ROW_VARIANTS && !rc; ++r)
     for (int c = 0; c < COL_VARIANTS && !rc; ++c)
       for (int wv = 0; wv < WAVE_VARIANTS && !rc; ++wv, ++vi) {
-      if (r == ROW_CLUSTER && (c != 1 || wv != 0 || !cluster_apply_available(g->Nx, g->Ny))) {
+      if ((r == ROW_CLUSTER || r == ROW_CLUSTER16) && (c != 1 || wv != 0 || !cluster_apply_available(g->Nx, g->Ny))) {
         if (times) times[vi] = -1.0;  // one kernel whatever the column and wave choices: timed once
         continue;
       }
@@ -254,7 +254,7 @@ int omb_tune_set(const char* device_name, int32_t Nx, int32_t Ny, int32_t row_va
                  int32_t wave_variant) {
   if (!device_name || !*device_name || Nx <= 0 || Ny <= 0 || row_variant < 0 || row_variant >= ROW_VARIANTS ||
       col_variant < 0 || col_variant >= COL_VARIANTS || wave_variant < 0 || wave_variant >= WAVE_VARIANTS)
-    return fail(OMB_ERR_INVALID_ARG, "omb_tune_set: bad key or variant (rows 0..5, columns 0..5, wave 0..3)");
+    return fail(OMB_ERR_INVALID_ARG, "omb_tune_set: bad key or variant (rows 0..6, columns 0..5, wave 0..3)");
   std::string n = device_name;
   for (char& c : n)
     if (c == '|' || c == '\n') c = '_';

@@ -125,15 +125,15 @@ def gram_blocks(Z, AZ, precision: str = "fp32", device: int = 0):
 
 def autotune(grid, ncol: int = 4, device: int = 0):
     """Tune the FP32 operator tiles of `grid` now (``omb_autotune``): returns
-    ``(row_variant, col_variant, wave_variant, seconds[6][6][4])`` (-1 where a combination
-    is not timed: the cluster apply's column and wave slots, or grids without it)."""
+    ``(row_variant, col_variant, wave_variant, seconds[7][6][4])`` (-1 where a combination
+    is not timed: the cluster applies' column and wave slots, or grids without them)."""
     lib = _lib.load()
     ctx = _lib.context(device)
     r, c, w = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
-    t = np.zeros(144)
+    t = np.zeros(168)
     _lib.check(lib.omb_autotune(ctx.handle, ctypes.byref(grid.c()), int(ncol), ctypes.byref(r), ctypes.byref(c),
                                 ctypes.byref(w), _dptr(t)))
-    return r.value, c.value, w.value, t.reshape(6, 6, 4)
+    return r.value, c.value, w.value, t.reshape(7, 6, 4)
 
 
 def tune_set(device_name: str, Nx: int, Ny: int, row: int, col: int, wave: int = 0) -> None:

@@ -36,7 +36,7 @@ def test_tune_table_round_trip(tmp_path):
 
 def test_tune_rejects_bad_entries():
     with pytest.raises(ops._lib.OmbError):
-        ops.tune_set("NVIDIA B200", 256, 256, 6, 0)
+        ops.tune_set("NVIDIA B200", 256, 256, 7, 0)
     with pytest.raises(ops._lib.OmbError):
         ops.tune_set("NVIDIA B200", 256, 256, 1, 6)
     with pytest.raises(ops._lib.OmbError):
