@@ -139,12 +139,13 @@ def measured_peak_hbm():
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one roofline launch of the
-# operator apply (4 columns x 64 cells of 256x256, FP32), from an ncu capture of
-#   python bench.py --case apply --steps 3 --apply-cells 16
-# (the three passes k_row_in2 / k_col2 / k_row_out2, 413.2 MB per 16-cell apply) scaled by
-# the cells processed (x4).  A fixed per-apply constant of the current kernels: bench runs
+# operator apply (4 columns x 64 cells of 256x256, FP32) with the tiles the autotuner picks on
+# B200 (row variant 4, column variant 1), from an ncu capture of
+#   python bench.py --case apply --steps 3 --apply-cells 16 --tiles 4,1,0
+# (the three passes k_row_in_sp / k_col2 / k_row_out_sp, 416.7 MB per 16-cell apply) scaled
+# by the cells processed (x4).  A fixed per-apply constant of the current kernels: bench runs
 # are never profiled, and the figure changes only when the apply kernels change.
-APPLY_TRAFFIC_BYTES = 1.6528e9
+APPLY_TRAFFIC_BYTES = 1.6669e9
 
 
 def smoothing_materials(n_shapes: int, nsets: int) -> np.ndarray:

@@ -211,7 +211,7 @@ typedef struct {
   double k_tol;           /* Newton tolerance on |Δk|                       (1e-8) */
   double eig_tol;         /* residual ‖M̂h − ω²h‖ of a unit eigenvector       (1e-8) */
   int32_t max_eigsolves;  /* Newton steps per band                            (60)   */
-  int32_t maxiter;        /* eigensolver iterations per band and phase        (300)  */
+  int32_t maxiter;        /* eigensolver iterations per band and phase       (1000)  */
   int32_t precision;      /* OMB_PREC_MIXED / OMB_PREC_FP64 / OMB_PREC_FP32   (MIXED)*/
   int32_t preconditioner; /* OMB_OP_P_DIAG or OMB_OP_P (MPB-style)          (DIAG) */
   int32_t newton;         /* OMB_NEWTON_INNER or OMB_NEWTON_OUTER             (INNER)*/

@@ -130,7 +130,7 @@ int omb_options_default(omb_options* o) {
   o->k_tol = 1e-8;
   o->eig_tol = 1e-8;
   o->max_eigsolves = 60;
-  o->maxiter = 300;
+  o->maxiter = 1000;
   o->precision = OMB_PREC_MIXED;
   o->preconditioner = OMB_OP_P_DIAG;
   o->newton = OMB_NEWTON_INNER;

@@ -13,7 +13,7 @@ struct SolveOptions {
   double tol = 1e-8;
   double k_tol = 1e-8;
   int max_newton = 60;
-  int maxiter = 300;
+  int maxiter = 1000;
   int precision = OMB_PREC_MIXED;
   bool prec_diag = false;
   int newton_mode = MODE_NEWTON_INNER;

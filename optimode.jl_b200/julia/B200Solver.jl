@@ -60,7 +60,7 @@ const _WARM = Dict(:none => Int32(0), :sweep => Int32(1), :cells => Int32(2), :l
 
 """
     B200Solver(; precision=:mixed, preconditioner=:diag, newton=:inner, device=0,
-               maxiter=300, guard_bands=1, warm_start=:none, logger=NullLogger())
+               maxiter=1000, guard_bands=1, warm_start=:none, logger=NullLogger())
 
 NVIDIA B200 (sm_100a) backend: batched device LOBPCG with Newton steps on k inside the
 iteration, FP32 iterations polished in FP64 to the requested tolerance.  `warm_start=:sweep`
@@ -82,7 +82,7 @@ struct B200Solver{L<:AbstractLogger} <: AbstractEigensolver{L}
     warm_start::Symbol
 end
 
-B200Solver(; precision=:mixed, preconditioner=:diag, newton=:inner, device=0, maxiter=300,
+B200Solver(; precision=:mixed, preconditioner=:diag, newton=:inner, device=0, maxiter=1000,
     guard_bands=1, warm_start=:none, logger=NullLogger()) =
     B200Solver(logger, device, precision, preconditioner, newton, maxiter, guard_bands, warm_start)
 

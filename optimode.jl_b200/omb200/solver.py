@@ -46,7 +46,7 @@ class B200Solver:
     preconditioner: str = "diag"
     newton: str = "inner"
     device: int = 0
-    maxiter: int = 300
+    maxiter: int = 1000
     seed: int = 0
     guard_bands: int = 1
     warm_start: str = "none"
