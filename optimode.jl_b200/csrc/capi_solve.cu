@@ -305,10 +305,32 @@ int omb_batch_run(omb_batch* b) {
       add_tracks(b, i, own_k0(b, i), nullptr, 0, 0, tracks);
     }
   }
+  // Mixed precision with inner Newton: the rest of each group joins the same engine as a
+  // second wave — its FP32 phase starts from the anchors' FP32 blocks once they finish theirs,
+  // and all tracks share one FP64 phase (the anchors' polish overlaps the others' instead of
+  // running alone).  Otherwise (FP64 or FP32 only, the reference loop) a second engine starts
+  // from the anchors' converged FP64 vectors.
+  const bool waves = b->so.precision == OMB_PREC_MIXED && b->so.newton_mode == MODE_NEWTON_INNER;
+  if (waves) {
+    std::vector<int> first_track(n_inst, -1);  // instance → its band-0 track (bands are consecutive)
+    for (const auto& h : b->who)
+      if (h.band0 == 0) first_track[h.inst] = h.track;
+    for (int i = 0; i < n_inst; ++i) {
+      const int a = anchor[i];
+      if (a < 0) continue;
+      const size_t t0 = tracks.size();
+      add_tracks(b, i, own_k0(b, i), nullptr, 0, 0, tracks);
+      for (size_t t = t0; t < tracks.size(); ++t) {
+        tracks[t].wave = 1;
+        tracks[t].src = first_track[a] >= 0 ? first_track[a] + tracks[t].band : -1;
+        tracks[t].omega_src = b->inst[a].omega;
+      }
+    }
+  }
   b->engines.emplace_back(new Engine(ctx, &b->probs, tracks, b->so));
   int rc = b->engines[0]->run();
   // stage 2: the rest of each sweep group, from its anchor's eigenvectors and k
-  if (!rc) {
+  if (!rc && !waves) {
     std::vector<TrackSpec> tracks2;
     const Engine& E0 = *b->engines[0];
     std::vector<std::vector<int>> first(n_inst);  // anchor → stage-1 who entries per band

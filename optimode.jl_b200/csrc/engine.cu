@@ -28,10 +28,12 @@ Engine::Engine(omb_ctx* ctx, std::vector<Problem>* problems, std::vector<TrackSp
   nt_ = (int)tracks_.size();
   order_.resize(nt_);
   for (int i = 0; i < nt_; ++i) order_[i] = i;
+  // by grid, and within a grid by wave, so that each wave of a grid group is one contiguous
+  // range of positions (a phase of one wave launches the operator passes over that range only)
   std::stable_sort(order_.begin(), order_.end(), [&](int a, int b) {
     const Problem& pa = (*probs_)[tracks_[a].prob];
     const Problem& pb = (*probs_)[tracks_[b].prob];
-    return std::make_tuple(pa.Nx, pa.Ny, pa.Nz) < std::make_tuple(pb.Nx, pb.Ny, pb.Nz);
+    return std::make_tuple(pa.Nx, pa.Ny, pa.Nz, tracks_[a].wave) < std::make_tuple(pb.Nx, pb.Ny, pb.Nz, tracks_[b].wave);
   });
   for (int i = 0; i < nt_;) {
     const Problem& p = (*probs_)[tracks_[order_[i]].prob];
@@ -113,14 +115,15 @@ template <typename T> int Engine::init_block(int phase) {
 }
 
 template <typename T>
-int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool reuse) {
+int Engine::run_phase(int phase, bool last, double tau, double lock_tol, int mode) {
   cudaStream_t st = ctx_->stream;
   DevBuf<cplx<T>>& Y = std::is_same<T, float>::value ? reinterpret_cast<DevBuf<cplx<T>>&>(y32_)
                                                       : reinterpret_cast<DevBuf<cplx<T>>&>(y64_);
   DevBuf<cplx<T>>& Sc = std::is_same<T, float>::value ? reinterpret_cast<DevBuf<cplx<T>>&>(s32_)
                                                        : reinterpret_cast<DevBuf<cplx<T>>&>(s64_);
   int rc = OMB_OK;
-  if (!reuse) {
+  auto active = [&](int t) { return wave_ < 0 || tracks_[t].wave == wave_; };
+  if (mode == 0) {
     // ---- buffers: per track Y[2], AY[2] (3M columns each) and the operator scratch
     yoff_.assign(nt_, 0);
     soff_.assign(nt_, 0);
@@ -139,7 +142,7 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
     rc = init_block<T>(phase);
     if (rc) return rc;
     if (phase > 0 && std::is_same<T, double>::value) y32_.release(), s32_.release();
-  } else {
+  } else if (mode == 1) {
     // continue from the current block: bring it to parity 0
     for (int t = 0; t < nt_; ++t) {
       if (host_states_[t].cur_par == 0) continue;
@@ -150,9 +153,14 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
     }
   }
 
-  // ---- per-phase state
+  // ---- per-phase state (tracks outside the running wave sit this phase out, state kept)
   for (int t = 0; t < nt_; ++t) {
     TrackState& s = host_states_[t];
+    if (!active(t)) {
+      s.done = 1;
+      s.op_ncol = 0; s.pw_ncol = 0; s.hmkh_ncol = 0;
+      continue;
+    }
     s.band = tracks_[t].band + round_;
     s.done = (round_ < tracks_[t].nbands) ? 0 : 1;
     s.status = s.done ? s.status : TS_RUNNING;
@@ -289,19 +297,32 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
   const int nl = std::max(1, std::min(LANES, nt_));
   int lane_lo[LANES], lane_hi[LANES];
   {
+    // (tracks sitting the phase out weigh nothing)
+    auto w2 = [&](int gi) { const int t = order_[gi]; return active(t) ? (double)tracks_[t].M * tracks_[t].M : 0.0; };
     double tot = 0, acc = 0;
-    for (int gi = 0; gi < nt_; ++gi) tot += (double)tracks_[order_[gi]].M * tracks_[order_[gi]].M;
+    for (int gi = 0; gi < nt_; ++gi) tot += w2(gi);
     int gi = 0;
     for (int L = 0; L < nl; ++L) {
       lane_lo[L] = gi;
       if (L == nl - 1) { gi = nt_; }
       else {
         // at least one track per lane, and leave one for each later lane
-        do { acc += (double)tracks_[order_[gi]].M * tracks_[order_[gi]].M; ++gi; }
+        do { acc += w2(gi); ++gi; }
         while (gi < nt_ - (nl - 1 - L) && acc < tot * (L + 1) / nl);
       }
       lane_hi[L] = gi;
     }
+  }
+  // per grid group, the positions of the tracks taking part in this phase (contiguous: the
+  // positions of a group are sorted by wave)
+  std::vector<int> act_lo(groups_.size()), act_hi(groups_.size());
+  for (size_t gi = 0; gi < groups_.size(); ++gi) {
+    const Group& g = groups_[gi];
+    int lo = g.off + g.n, hi = g.off;
+    for (int p = g.off; p < g.off + g.n; ++p)
+      if (active(order_[p])) { lo = std::min(lo, p); hi = std::max(hi, p + 1); }
+    act_lo[gi] = lo;
+    act_hi[gi] = std::max(lo, hi);
   }
   OMB_CU(d_pre_.alloc(2 * (size_t)LANES * ((size_t)nt_ + 1), st));
   // z-periodic groups: per-lane room for the slab and line units of launch_op3d
@@ -323,10 +344,11 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, bool re
       return g.Nz > 1 ? launch_op3d<T>(kind, u, cnt, g.Nx, g.Ny, g.Nz, maxcol, ctx_->tw, d_exp[L].p, s)
                       : launch_op<T>(kind, u, cnt, g.Nx, g.Ny, maxcol, ctx_->tw, s);
     };
-    // the lane's part of every grid group
+    // the lane's part of every grid group (its positions of the running wave)
     auto for_groups = [&](auto&& f) -> bool {
-      for (const Group& g : groups_) {
-        const int lo = std::max(g.off, a), hi = std::min(g.off + g.n, a + n);
+      for (size_t gi = 0; gi < groups_.size(); ++gi) {
+        const Group& g = groups_[gi];
+        const int lo = std::max(act_lo[gi], a), hi = std::min(act_hi[gi], a + n);
         if (hi > lo && !f(g, lo, hi - lo)) return false;
       }
       return true;
@@ -524,27 +546,69 @@ int Engine::run() {
   round_ = 0;
   int rc = OMB_OK;
   if (opt_.precision == OMB_PREC_FP64) {
-    rc = run_phase<double>(0, true, opt_.tol, opt_.tol, false);
+    rc = run_phase<double>(0, true, opt_.tol, opt_.tol, 0);
   } else if (opt_.precision == OMB_PREC_FP32) {
     // tolerances clamped to what FP32 can resolve (the reference clamps to 50·eps(T),
     // src/solvers/gpu.jl:58)
     opt_.tol = std::max(opt_.tol, tauA);
     opt_.k_tol = std::max(opt_.k_tol, 50 * 1.1920929e-7);
-    rc = run_phase<float>(0, true, opt_.tol, opt_.tol, false);
+    rc = run_phase<float>(0, true, opt_.tol, opt_.tol, 0);
   } else {
-    rc = run_phase<float>(0, false, tauA, tauA, false);
-    if (!rc) rc = run_phase<double>(1, true, opt_.tol, opt_.tol, false);
+    bool waves = false;
+    for (const auto& ts : tracks_) waves = waves || ts.wave == 1;
+    if (waves) {
+      // wave 0's FP32 phase, then wave 1's from wave 0's blocks, then one FP64 phase for all
+      wave_ = 0;
+      rc = run_phase<float>(0, false, tauA, tauA, 0);
+      if (!rc) rc = start_wave(1);
+      wave_ = 1;
+      if (!rc) rc = run_phase<float>(0, false, tauA, tauA, 2);
+      wave_ = -1;
+    } else {
+      rc = run_phase<float>(0, false, tauA, tauA, 0);
+    }
+    if (!rc) rc = run_phase<double>(1, true, opt_.tol, opt_.tol, 0);
   }
   if (!rc) rc = snapshot(0);
   int maxb = 1;
   for (const auto& ts : tracks_) maxb = std::max(maxb, ts.mode == MODE_NEWTON_OUTER ? ts.nbands : 1);
   for (round_ = 1; round_ < maxb && !rc; ++round_) {
-    rc = last_prec_ == 1 ? run_phase<double>(2, true, opt_.tol, opt_.tol, true)
-                         : run_phase<float>(2, true, opt_.tol, opt_.tol, true);
+    rc = last_prec_ == 1 ? run_phase<double>(2, true, opt_.tol, opt_.tol, 1)
+                         : run_phase<float>(2, true, opt_.tol, opt_.tol, 1);
     if (!rc) rc = snapshot(round_);
   }
   round_ = 0;
   return rc;
+}
+
+// Set up the tracks of `wave` after the FP32 phase of the tracks before it: each starts from
+// the FP32 block of its source track (all M columns, at that track's current parity) with the
+// source's k carried to first order in ω, k + (ω − ω_src)·2ω_src/(∂ω²/∂k).  A source that
+// did not end its phase normally leaves the track at its own start (random block, own k).
+int Engine::start_wave(int wave) {
+  cudaStream_t st = ctx_->stream;
+  int rc = download_states();
+  if (rc) return rc;
+  for (int t = 0; t < nt_; ++t) {
+    const TrackSpec& ts = tracks_[t];
+    if (ts.wave != wave || ts.src < 0 || ts.src >= nt_) continue;
+    const TrackState& sa = host_states_[ts.src];
+    if (sa.status != TS_PHASE_DONE || !std::isfinite(sa.k) || !(sa.k > 0)) continue;
+    const double w = std::sqrt(ts.omega2), wa = ts.omega_src;
+    double k = sa.k * w / wa;  // constant n_eff
+    const double dw2dk = 2.0 * sa.hmkh;
+    if (dw2dk > 0 && std::isfinite(dw2dk)) k = sa.k + (w - wa) * 2.0 * wa / dw2dk;
+    if (!(k > 0 && std::isfinite(k))) k = ts.k0;
+    TrackState& s = host_states_[t];
+    s.k = k;
+    s.k_eig = k;
+    const size_t n2 = 2 * (*probs_)[ts.prob].N();
+    const int Ma = tracks_[ts.src].M;
+    const int ncol = std::min(ts.M, Ma);
+    const float2* from = y32_.p + yoff_[ts.src] + (size_t)sa.cur_par * 3 * Ma * n2;
+    OMB_CU(cudaMemcpyAsync(y32_.p + yoff_[t], from, ncol * n2 * sizeof(float2), cudaMemcpyDeviceToDevice, st));
+  }
+  return OMB_OK;
 }
 
 int Engine::snapshot(int round) {

@@ -36,6 +36,13 @@ struct TrackSpec {
   int nguess = 0;
   const double2* guess_dev[MMAX] = {};  // or device FP64 columns (another engine's results)
   int nguess_dev = 0;
+  // Two-wave runs (mixed precision, inner Newton): a wave-1 track starts its FP32 phase once
+  // the wave-0 tracks have finished theirs, from the FP32 block of wave-0 track `src` (the
+  // same band of a solved neighbour at ω_src) with k extrapolated to first order in ω; both
+  // waves then share one FP64 phase.
+  int wave = 0;
+  int src = -1;
+  double omega_src = 0;
 };
 
 class Engine {
@@ -64,7 +71,10 @@ class Engine {
   int max_iterations() const;
 
  private:
-  template <typename T> int run_phase(int phase, bool last, double tau, double lock_tol, bool reuse);
+  // mode: 0 fresh buffers and blocks, 1 continue from the current block (next reference-loop
+  // band), 2 keep buffers and blocks (the tracks of wave_ were set up by start_wave)
+  template <typename T> int run_phase(int phase, bool last, double tau, double lock_tol, int mode);
+  int start_wave(int wave);
   template <typename T> int init_block(int phase);
   int upload_states();
   int download_states();
@@ -77,6 +87,7 @@ class Engine {
   SolveOptions opt_;
   int nt_ = 0;
   int round_ = 0;
+  int wave_ = -1;  // the wave a phase runs (-1: every track)
   int last_prec_ = 1;  // precision of the buffers holding the final block (0 fp32, 1 fp64)
   int64_t launches_ = 0, kernels_ = 0;
 
