@@ -325,6 +325,7 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, int mod
     act_hi[gi] = std::max(lo, hi);
   }
   OMB_CU(d_pre_.alloc(2 * (size_t)LANES * ((size_t)nt_ + 1), st));
+  OMB_CU(d_wpre_.alloc(2 * (size_t)LANES * ((size_t)nt_ + 1), st));
   // z-periodic groups: per-lane room for the slab and line units of launch_op3d
   int maxNz = 1;
   for (const Group& g : groups_) maxNz = std::max(maxNz, g.Nz);
@@ -340,6 +341,8 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, int mod
     if (n <= 0) return e;
     int* preg = d_pre_.p + (size_t)L * 2 * (nt_ + 1);
     int* preu = preg + nt_ + 1;
+    long long* wpreg = d_wpre_.p + (size_t)L * 2 * (nt_ + 1);
+    long long* wpreu = wpreg + nt_ + 1;
     auto op = [&](OpKind kind, const OpUnit<T>* u, int cnt, const Group& g, int maxcol) -> cudaError_t {
       return g.Nz > 1 ? launch_op3d<T>(kind, u, cnt, g.Nx, g.Ny, g.Nz, maxcol, ctx_->tw, d_exp[L].p, s)
                       : launch_op<T>(kind, u, cnt, g.Nx, g.Ny, maxcol, ctx_->tw, s);
@@ -368,16 +371,17 @@ int Engine::run_phase(int phase, bool last, double tau, double lock_tol, int mod
           return ok("operator pass", op(OP_M, d_uA[par].p + off, cnt, g, 3 * g.Mmax));
         }))
       return e;
-    k_live_prefix<<<1, 1024, 0, s>>>(d_state_ptrs_.p + a, d_n2_.p + a, n, rg, UpdCfg<T>::R, preg, preu);
+    k_live_prefix<<<1, 1024, 0, s>>>(d_state_ptrs_.p + a, d_n2_.p + a, n, rg, UpdCfg<T>::R, preg, preu, wpreg,
+                                     wpreu);
     if (!ok("k_live_prefix", cudaGetLastError())) return e;
-    k_gram<T><<<grid_g, GramCfg<T>::NT, sm_gram, s>>>(d_descs.p + a, preg, n, par, nmax, rg, gstages, d_err_.p,
-                                                       ctx_->wait_ns);
+    k_gram<T><<<grid_g, GramCfg<T>::NT, sm_gram, s>>>(d_descs.p + a, preg, wpreg, n, par, nmax, rg, gstages,
+                                                       d_err_.p, ctx_->wait_ns);
     if (!ok("k_gram", cudaGetLastError())) return e;
     k_rr<<<n, RR_NT, sm_rr, s>>>(d_state_ptrs_.p + a, d_gram_ptrs_.p + a, d_coef_ptrs_.p + a, d_coef32_ptrs_.p + a, n,
                                  prm);
     if (!ok("k_rr", cudaGetLastError())) return e;
-    update_kernel<<<grid_u, UpdCfg<T>::NT, sm_upd, s>>>(d_descs.p + a, preu, n, par, prm.prec_diag, d_err_.p,
-                                                        ctx_->wait_ns);
+    update_kernel<<<grid_u, UpdCfg<T>::NT, sm_upd, s>>>(d_descs.p + a, preu, wpreu, n, par, prm.prec_diag,
+                                                        d_err_.p, ctx_->wait_ns);
     if (!ok("k_update", cudaGetLastError())) return e;
     k_control<<<(n + 3) / 4, 128, 0, s>>>(d_state_ptrs_.p + a, d_res_ptrs_.p + a, n, prm);
     ok("k_control", cudaGetLastError());

@@ -107,6 +107,7 @@ class Engine {
   DevBuf<int> d_hmkh_nb_;
   DevBuf<long long> d_n2_;
   DevBuf<int> d_pre_;   // live-tile prefixes: Gram tiles [0, nt], update tiles [nt+1, 2nt+1]
+  DevBuf<long long> d_wpre_;  // the same prefixes weighted by each tile's cost
   DevBuf<int> d_err_;   // first pipeline error of the streaming kernels (0: none)
 
   // block buffers of the current precision (Y/AY per parity, scratch)

@@ -66,7 +66,7 @@ int gram_blocks(omb_ctx* ctx, long long n2, int n, const double* Z, const double
   const size_t sm = 128 + gstages * gstage + gred;
   OMB_CU(ensure_smem(reinterpret_cast<const void*>(k_gram<T>), sm));
   const int grid = std::min(tiles, ctx->num_sms);
-  k_gram<T><<<grid, GramCfg<T>::NT, sm, st>>>(dd.p, pre.p, 1, 0, nmax, rg, gstages, err.p, ctx->wait_ns);
+  k_gram<T><<<grid, GramCfg<T>::NT, sm, st>>>(dd.p, pre.p, nullptr, 1, 0, nmax, rg, gstages, err.p, ctx->wait_ns);
   OMB_CU(cudaGetLastError());
   std::vector<double2> h(2 * (size_t)NMAX * NMAX);
   int herr = 0;

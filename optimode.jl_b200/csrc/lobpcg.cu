@@ -4,31 +4,46 @@
 namespace omb {
 
 __global__ void k_live_prefix(TrackState* const* __restrict__ states, const long long* __restrict__ n2,
-                              int ntracks, int rg, int ru, int* __restrict__ pre_g, int* __restrict__ pre_u) {
-  // one CTA of 1024 threads: inclusive scans of the live tracks' tile counts
+                              int ntracks, int rg, int ru, int* __restrict__ pre_g, int* __restrict__ pre_u,
+                              long long* __restrict__ wpre_g, long long* __restrict__ wpre_u) {
+  // one CTA of 1024 threads: inclusive scans of the live tracks' tile counts and tile costs
   __shared__ int sg[1024], su[1024];
+  __shared__ long long wg[1024], wu[1024];
   __shared__ int carry[2];
+  __shared__ long long wcarry[2];
   const int tid = threadIdx.x;
-  if (tid == 0) { carry[0] = carry[1] = 0; pre_g[0] = 0; pre_u[0] = 0; }
+  if (tid == 0) {
+    carry[0] = carry[1] = 0; pre_g[0] = 0; pre_u[0] = 0;
+    wcarry[0] = wcarry[1] = 0; wpre_g[0] = 0; wpre_u[0] = 0;
+  }
   __syncthreads();
   for (int base = 0; base < ntracks; base += 1024) {
     const int t = base + tid;
     int vg = 0, vu = 0;
+    long long xg = 0, xu = 0;
     if (t < ntracks && !states[t]->done) {
+      const TrackState& s = *states[t];
+      const int n = s.M + s.nWa + s.nP;
       vg = (int)((n2[t] + rg - 1) / rg);
       vu = (int)((n2[t] + ru - 1) / ru);
+      xg = vg * gram_tile_cost(n);
+      xu = vu * update_tile_cost(n, s.M);
     }
-    sg[tid] = vg; su[tid] = vu;
+    sg[tid] = vg; su[tid] = vu; wg[tid] = xg; wu[tid] = xu;
     __syncthreads();
     for (int off = 1; off < 1024; off <<= 1) {
       const int ag = tid >= off ? sg[tid - off] : 0, au = tid >= off ? su[tid - off] : 0;
+      const long long bg = tid >= off ? wg[tid - off] : 0, bu = tid >= off ? wu[tid - off] : 0;
       __syncthreads();
-      sg[tid] += ag; su[tid] += au;
+      sg[tid] += ag; su[tid] += au; wg[tid] += bg; wu[tid] += bu;
       __syncthreads();
     }
-    if (t < ntracks) { pre_g[t + 1] = carry[0] + sg[tid]; pre_u[t + 1] = carry[1] + su[tid]; }
+    if (t < ntracks) {
+      pre_g[t + 1] = carry[0] + sg[tid]; pre_u[t + 1] = carry[1] + su[tid];
+      wpre_g[t + 1] = wcarry[0] + wg[tid]; wpre_u[t + 1] = wcarry[1] + wu[tid];
+    }
     __syncthreads();
-    if (tid == 1023) { carry[0] += sg[1023]; carry[1] += su[1023]; }
+    if (tid == 1023) { carry[0] += sg[1023]; carry[1] += su[1023]; wcarry[0] += wg[1023]; wcarry[1] += wu[1023]; }
     __syncthreads();
   }
 }

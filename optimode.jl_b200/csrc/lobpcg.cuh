@@ -99,8 +99,9 @@ __device__ __forceinline__ int z_phys(const TrackState& s, int M, int l) {
 // (one producer warp, a ring of `stages` buffers guarded by full/empty mbarriers) while
 // the consumer warps compute.  The rows of all live tracks form one sequence of tiles
 // (k_live_prefix counts them after the Newton step of the iteration); CTA b of a 1D grid
-// of X takes tiles [b·T/X, (b+1)·T/X), so the work stays spread over every SM however
-// few tracks are left.  Per-track sums leave each CTA through FP64 atomics into the
+// of X takes the tiles that start in [b·W/X, (b+1)·W/X) of the tiles' summed cost W (a
+// tile of a wide track costs several times one of a narrow track), so the work stays
+// spread evenly over every SM however few tracks are left.  Per-track sums leave each CTA through FP64 atomics into the
 // track's accumulators, which k_rr (Gram) and k_control (‖R‖²) read and clear.
 
 // Tile sequence of one CTA: tiles of R rows of the live tracks, in track order.
@@ -109,11 +110,32 @@ struct TileWalk {
   int ntracks, t;      // current track
   long long i, end;    // current global tile, one past the last
   int R;
-  __device__ __forceinline__ void start(const int* pre_, int ntracks_, int R_) {
+  // first global tile whose cost-weighted start is ≥ x (wpre: prefix of the tracks' summed
+  // tile costs, the tiles of one track costing the same)
+  __device__ __forceinline__ long long tile_at(const long long* wpre, long long x) const {
+    if (x >= wpre[ntracks]) return pre[ntracks];
+    int lo = 0, hi = ntracks - 1;  // first track with wpre[t+1] > x
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (wpre[mid + 1] > x) hi = mid; else lo = mid + 1;
+    }
+    const long long nt = pre[lo + 1] - pre[lo];
+    const long long wt = (wpre[lo + 1] - wpre[lo]) / nt;
+    const long long j = (x - wpre[lo] + wt - 1) / wt;
+    return pre[lo] + (j < nt ? j : nt);
+  }
+  // wpre == nullptr: every tile costs the same
+  __device__ __forceinline__ void start(const int* pre_, const long long* wpre, int ntracks_, int R_) {
     pre = pre_; ntracks = ntracks_; R = R_;
-    const long long T = pre[ntracks];
-    i = (long long)blockIdx.x * T / gridDim.x;
-    end = (long long)(blockIdx.x + 1) * T / gridDim.x;
+    if (wpre && wpre[ntracks] > 0) {
+      const long long W = wpre[ntracks];
+      i = tile_at(wpre, (long long)blockIdx.x * W / gridDim.x);
+      end = tile_at(wpre, (long long)(blockIdx.x + 1) * W / gridDim.x);
+    } else {
+      const long long T = pre[ntracks];
+      i = (long long)blockIdx.x * T / gridDim.x;
+      end = (long long)(blockIdx.x + 1) * T / gridDim.x;
+    }
     // first track whose tile range contains i (skips tracks with no tiles)
     int lo = 0, hi = ntracks - 1;
     while (lo < hi) {
@@ -132,9 +154,19 @@ struct TileWalk {
   __device__ __forceinline__ bool last_of_track() const { return i + 1 >= end || pre[t + 1] <= i + 1; }
 };
 
-// Live-tile prefixes for the Gram (rows per tile rg) and update (ru) kernels.
+// Live-tile prefixes for the Gram (rows per tile rg) and update (ru) kernels, and the
+// prefixes of their cost-weighted tile counts (wpre_g, wpre_u).
 __global__ void k_live_prefix(TrackState* const* __restrict__ states, const long long* __restrict__ n2,
-                              int ntracks, int rg, int ru, int* __restrict__ pre_g, int* __restrict__ pre_u);
+                              int ntracks, int rg, int ru, int* __restrict__ pre_g, int* __restrict__ pre_u,
+                              long long* __restrict__ wpre_g, long long* __restrict__ wpre_u);
+// Relative cost of one tile of a track with n block columns of which M are X: the Gram's 4×4
+// items (each 16 complex products per row) plus its loads; the update's n·M products per row
+// of X, AX, P, AP plus its 4M stores.
+__host__ __device__ __forceinline__ long long gram_tile_cost(int n) {
+  const int nb4 = (n + 3) / 4;
+  return 8LL * nb4 * (nb4 + 1) + n;
+}
+__host__ __device__ __forceinline__ long long update_tile_cost(int n, int M) { return (long long)n * M + 4LL * M; }
 
 // ---- Gram ---------------------------------------------------------------------------
 // G = ZᴴZ and S = ZᴴAZ (upper triangles).  The outputs are cut into 4×4 blocks (items);
@@ -187,8 +219,8 @@ __device__ __forceinline__ void two_sum_acc(float& s, float& lo, float x) {
 
 template <typename T>
 __global__ void __launch_bounds__(GramCfg<T>::NT, 1)
-    k_gram(const TrackDesc<T>* __restrict__ D, const int* __restrict__ pre, int ntracks, int par, int nmax,
-           int R, int stages, int* __restrict__ err, uint64_t wait_ns) {
+    k_gram(const TrackDesc<T>* __restrict__ D, const int* __restrict__ pre, const long long* __restrict__ wpre,
+           int ntracks, int par, int nmax, int R, int stages, int* __restrict__ err, uint64_t wait_ns) {
   using C = cplx<T>;
   using Cfg = GramCfg<T>;
   const int CS = R + Cfg::PAD;
@@ -204,7 +236,7 @@ __global__ void __launch_bounds__(GramCfg<T>::NT, 1)
   }
   __syncthreads();
   TileWalk w;
-  w.start(pre, ntracks, R);
+  w.start(pre, wpre, ntracks, R);
   if (warp == Cfg::NCW) {
     // ---- producer: one bulk copy per column segment of the tile
     int q = 0, fills[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -476,8 +508,8 @@ __device__ __forceinline__ void update_tile(const TrackDesc<T>& d, const TrackSt
 // MB: the largest block size of the launch (the tile bodies for M ≤ MB are compiled in).
 template <typename T, int MB>
 __global__ void __launch_bounds__(UpdCfg<T>::NT, 1)
-    k_update(const TrackDesc<T>* __restrict__ D, const int* __restrict__ pre, int ntracks, int par,
-             int prec_diag, int* __restrict__ err, uint64_t wait_ns) {
+    k_update(const TrackDesc<T>* __restrict__ D, const int* __restrict__ pre, const long long* __restrict__ wpre,
+             int ntracks, int par, int prec_diag, int* __restrict__ err, uint64_t wait_ns) {
   using C = cplx<T>;
   using Cfg = UpdCfg<T>;
   constexpr int R = Cfg::R, LG = Cfg::LG, S = Cfg::STAGES;
@@ -492,7 +524,7 @@ __global__ void __launch_bounds__(UpdCfg<T>::NT, 1)
   }
   __syncthreads();
   TileWalk w;
-  w.start(pre, ntracks, R);
+  w.start(pre, wpre, ntracks, R);
   if (warp == Cfg::NCW) {
     // ---- producer
     int q = 0, fills[S] = {};
