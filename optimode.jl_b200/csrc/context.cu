@@ -249,6 +249,111 @@ int gather_to_host(omb_ctx* ctx, const D2HPiece* pieces, size_t n) {
   return OMB_OK;
 }
 
+// ---- ε⁻¹ upload: validation and the per-precision layouts on the device ----------------
+// The caller's (3, 3, Nx, Ny[, Nz]) FP64 array is copied once; one kernel finds the largest
+// |entry| and the first non-finite one, a second checks symmetry (relative to that largest
+// entry) and the trace pixel by pixel, writes the FP32 (float4 + float2) and FP64 (3 double2)
+// unique entries and ε_ave = 3/tr, and reduces min diag, max trace and per-block sums of ε_ave
+// (summed on the host in block order, so the mean does not depend on scheduling).
+namespace {
+constexpr int EPS_NT = 256;
+constexpr unsigned long long NONE = ~0ull;
+struct EpsStats {
+  unsigned long long emax;      // bits of max |entry| (non-negative doubles order like their bits)
+  unsigned long long bad_nan;   // first non-finite entry
+  unsigned long long bad_asym;  // first pixel whose off-diagonal pairs differ by > 1e-9·max|entry|
+  unsigned long long bad_trace; // first pixel with trace ≤ 0
+  unsigned long long bad_diag;  // first pixel with a diagonal entry ≤ 0
+  unsigned long long mind;      // bits of the least (positive) diagonal entry
+  unsigned long long maxtr;     // bits of the largest (positive) trace
+};
+
+// Block-wide minimum (every thread calls it; the result is valid in thread 0).
+__device__ __forceinline__ unsigned long long block_min_u64(unsigned long long v, unsigned long long* sh) {
+  for (int o = 16; o > 0; o >>= 1) { const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o); v = w < v ? w : v; }
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    v = threadIdx.x < EPS_NT / 32 ? sh[threadIdx.x] : NONE;
+    for (int o = 16; o > 0; o >>= 1) { const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o); v = w < v ? w : v; }
+  }
+  __syncthreads();
+  return v;
+}
+__device__ __forceinline__ unsigned long long block_max_u64(unsigned long long v, unsigned long long* sh) {
+  return ~block_min_u64(~v, sh);
+}
+
+__global__ void __launch_bounds__(EPS_NT) k_eps_scan(const double* __restrict__ raw, size_t n, EpsStats* st) {
+  __shared__ unsigned long long sh[EPS_NT / 32];
+  unsigned long long mx = 0, bad = NONE;
+  for (size_t i = (size_t)blockIdx.x * EPS_NT + threadIdx.x; i < n; i += (size_t)gridDim.x * EPS_NT) {
+    const double v = raw[i];
+    if (!isfinite(v)) bad = i < bad ? i : bad;
+    else { const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(v)); mx = b > mx ? b : mx; }
+  }
+  mx = block_max_u64(mx, sh);
+  bad = block_min_u64(bad, sh);
+  if (threadIdx.x == 0) {
+    atomicMax(&st->emax, mx);
+    if (bad != NONE) atomicMin(&st->bad_nan, bad);
+  }
+}
+
+__global__ void __launch_bounds__(EPS_NT) k_eps_convert(const double* __restrict__ raw, size_t N, EpsStats* st,
+                                                        float4* __restrict__ a32, float2* __restrict__ b32,
+                                                        double2* __restrict__ e64, float* __restrict__ ea32,
+                                                        double* __restrict__ ea64, double* __restrict__ part) {
+  __shared__ unsigned long long sh[EPS_NT / 32];
+  __shared__ double ssum[EPS_NT];
+  const double emax = __longlong_as_double((long long)st->emax);
+  const size_t p = (size_t)blockIdx.x * EPS_NT + threadIdx.x;
+  unsigned long long basym = NONE, btr = NONE, bdiag = NONE, mind = NONE, maxtr = 0;
+  double eave = 0;
+  if (p < N) {
+    const double* m = raw + 9 * p;  // column-major 3x3: m[a + 3b] = ε⁻¹[a,b]
+    const double xx = m[0], yy = m[4], zz = m[8];
+    const double xy = 0.5 * (m[1] + m[3]), xz = 0.5 * (m[2] + m[6]), yz = 0.5 * (m[5] + m[7]);
+    const double asym = fmax(fabs(m[1] - m[3]), fmax(fabs(m[2] - m[6]), fabs(m[5] - m[7])));
+    if (asym > 1e-9 * emax) basym = p;
+    const double tr = xx + yy + zz;
+    if (!(tr > 0)) btr = p;
+    const double dmin = fmin(xx, fmin(yy, zz));
+    if (!(dmin > 0)) bdiag = p;
+    else mind = (unsigned long long)__double_as_longlong(dmin);
+    if (tr > 0) maxtr = (unsigned long long)__double_as_longlong(tr);
+    a32[p] = make_float4((float)xx, (float)yy, (float)zz, (float)xy);
+    b32[p] = make_float2((float)xz, (float)yz);
+    e64[3 * p] = make_double2(xx, yy);
+    e64[3 * p + 1] = make_double2(zz, xy);
+    e64[3 * p + 2] = make_double2(xz, yz);
+    eave = 3.0 / tr;
+    ea64[p] = eave;
+    ea32[p] = (float)eave;
+  }
+  // per-block sum of ε_ave in a fixed order (pairwise tree)
+  ssum[threadIdx.x] = eave;
+  __syncthreads();
+  for (int s = EPS_NT / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) ssum[threadIdx.x] += ssum[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = ssum[0];
+  basym = block_min_u64(basym, sh);
+  btr = block_min_u64(btr, sh);
+  bdiag = block_min_u64(bdiag, sh);
+  mind = block_min_u64(mind, sh);
+  maxtr = block_max_u64(maxtr, sh);
+  if (threadIdx.x == 0) {
+    if (basym != NONE) atomicMin(&st->bad_asym, basym);
+    if (btr != NONE) atomicMin(&st->bad_trace, btr);
+    if (bdiag != NONE) atomicMin(&st->bad_diag, bdiag);
+    if (mind != NONE) atomicMin(&st->mind, mind);
+    atomicMax(&st->maxtr, maxtr);
+  }
+}
+}  // namespace
+
 int upload_problem(omb_ctx* ctx, const omb_grid* g, const double* epsinv, Problem& P, int Nz, double Dz) {
   int rc = check_grid(g);
   if (rc) return rc;
@@ -264,55 +369,47 @@ int upload_problem(omb_ctx* ctx, const omb_grid* g, const double* epsinv, Proble
   P.Nx = g->Nx; P.Ny = g->Ny; P.Dx = g->Dx; P.Dy = g->Dy;
   P.Nz = Nz; P.Dz = Nz > 1 ? Dz : 0;
   const size_t N = P.N();
-  std::vector<float4> a32(N);
-  std::vector<float2> b32(N);
-  std::vector<double2> e64(3 * N);
-  std::vector<float> ea32(N);
-  std::vector<double> ea64(N);
-  double emax = 0, mind = INFINITY, mean = 0, maxtr = 0;
-  for (size_t p = 0; p < 9 * N; ++p) {
-    const double v = epsinv[p];
-    if (!std::isfinite(v)) return fail(OMB_ERR_NAN, "epsinv holds a non-finite value");
-    emax = std::fmax(emax, std::fabs(v));
-  }
-  for (size_t p = 0; p < N; ++p) {
-    const double* m = epsinv + 9 * p;  // column-major 3x3: m[a + 3b] = ε⁻¹[a,b]
-    const double xx = m[0], yy = m[4], zz = m[8];
-    const double xy = 0.5 * (m[1] + m[3]), xz = 0.5 * (m[2] + m[6]), yz = 0.5 * (m[5] + m[7]);
-    const double asym = std::fmax(std::fabs(m[1] - m[3]), std::fmax(std::fabs(m[2] - m[6]), std::fabs(m[5] - m[7])));
-    if (asym > 1e-9 * emax)
-      return fail(OMB_ERR_INVALID_ARG, "epsinv is not symmetric at pixel " + std::to_string(p) +
-                                           " (the Helmholtz operator needs a real symmetric ε⁻¹)");
-    const double tr = xx + yy + zz;
-    if (!(tr > 0)) return fail(OMB_ERR_INVALID_ARG, "epsinv has a non-positive trace at pixel " + std::to_string(p));
-    mind = std::fmin(mind, std::fmin(xx, std::fmin(yy, zz)));
-    maxtr = std::fmax(maxtr, tr);
-    a32[p] = make_float4((float)xx, (float)yy, (float)zz, (float)xy);
-    b32[p] = make_float2((float)xz, (float)yz);
-    e64[3 * p] = make_double2(xx, yy);
-    e64[3 * p + 1] = make_double2(zz, xy);
-    e64[3 * p + 2] = make_double2(xz, yz);
-    ea64[p] = 3.0 / tr;
-    ea32[p] = (float)ea64[p];
-    mean += ea64[p];
-  }
-  if (!(mind > 0)) return fail(OMB_ERR_INVALID_ARG, "epsinv has a non-positive diagonal entry");
-  P.eps_mean = mean / (double)N;
-  P.min_diag = mind;
-  P.max_trace = maxtr;
   cudaStream_t st = ctx->stream;
+  const unsigned nb = (unsigned)((N + EPS_NT - 1) / EPS_NT);
+  DevBuf<double> raw, part;
+  DevBuf<EpsStats> dst;
+  OMB_CU(raw.alloc(9 * N, st));
+  OMB_CU(part.alloc(nb, st));
+  OMB_CU(dst.alloc(1, st));
   OMB_CU(P.e32a.alloc(N, st));
   OMB_CU(P.e32b.alloc(N, st));
   OMB_CU(P.e64.alloc(3 * N, st));
   OMB_CU(P.eave32.alloc(N, st));
   OMB_CU(P.eave64.alloc(N, st));
-  OMB_CU(cudaMemcpyAsync(P.e32a.p, a32.data(), N * sizeof(float4), cudaMemcpyHostToDevice, st));
-  OMB_CU(cudaMemcpyAsync(P.e32b.p, b32.data(), N * sizeof(float2), cudaMemcpyHostToDevice, st));
-  OMB_CU(cudaMemcpyAsync(P.e64.p, e64.data(), 3 * N * sizeof(double2), cudaMemcpyHostToDevice, st));
-  OMB_CU(cudaMemcpyAsync(P.eave32.p, ea32.data(), N * sizeof(float), cudaMemcpyHostToDevice, st));
-  OMB_CU(cudaMemcpyAsync(P.eave64.p, ea64.data(), N * sizeof(double), cudaMemcpyHostToDevice, st));
-  // host vectors die at return: make the copies complete first
+  const EpsStats init{0, NONE, NONE, NONE, NONE, NONE, 0};
+  OMB_CU(cudaMemcpyAsync(dst.p, &init, sizeof(EpsStats), cudaMemcpyHostToDevice, st));
+  OMB_CU(cudaMemcpyAsync(raw.p, epsinv, 9 * N * sizeof(double), cudaMemcpyHostToDevice, st));
+  const unsigned nscan = std::min<unsigned>(4 * (unsigned)std::max(ctx->num_sms, 1),
+                                            (unsigned)((9 * N + EPS_NT - 1) / EPS_NT));
+  k_eps_scan<<<nscan, EPS_NT, 0, st>>>(raw.p, 9 * N, dst.p);
+  OMB_CU(cudaGetLastError());
+  k_eps_convert<<<nb, EPS_NT, 0, st>>>(raw.p, N, dst.p, P.e32a.p, P.e32b.p, P.e64.p, P.eave32.p, P.eave64.p, part.p);
+  OMB_CU(cudaGetLastError());
+  EpsStats hs;
+  std::vector<double> hp(nb);
+  OMB_CU(cudaMemcpyAsync(&hs, dst.p, sizeof(EpsStats), cudaMemcpyDeviceToHost, st));
+  OMB_CU(cudaMemcpyAsync(hp.data(), part.p, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
   OMB_CU(cudaStreamSynchronize(st));
+  if (hs.bad_nan != NONE) return fail(OMB_ERR_NAN, "epsinv holds a non-finite value");
+  if (hs.bad_asym != NONE && hs.bad_asym <= hs.bad_trace)
+    return fail(OMB_ERR_INVALID_ARG, "epsinv is not symmetric at pixel " + std::to_string(hs.bad_asym) +
+                                         " (the Helmholtz operator needs a real symmetric ε⁻¹)");
+  if (hs.bad_trace != NONE)
+    return fail(OMB_ERR_INVALID_ARG, "epsinv has a non-positive trace at pixel " + std::to_string(hs.bad_trace));
+  if (hs.bad_diag != NONE) return fail(OMB_ERR_INVALID_ARG, "epsinv has a non-positive diagonal entry");
+  double mean = 0;
+  for (unsigned b = 0; b < nb; ++b) mean += hp[b];
+  P.eps_mean = mean / (double)N;
+  double v;
+  std::memcpy(&v, &hs.mind, sizeof v);
+  P.min_diag = v;
+  std::memcpy(&v, &hs.maxtr, sizeof v);
+  P.max_trace = v;
   return OMB_OK;
 }
 

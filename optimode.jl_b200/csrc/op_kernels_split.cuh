@@ -1,4 +1,5 @@
-// Component-parallel FP32 operator passes for two-level lines (≤ 256 points).
+// Component-parallel operator passes for two-level lines (≤ 256 points): FP32 row and
+// column passes (tile variants) and the FP64 row passes.
 //
 // The same transforms, modes, layouts and results as k_row_in2 / k_col2 / k_row_out2
 // (op_kernels_2l.cuh), with one thread per (line slot, field component) instead of one per
@@ -19,16 +20,19 @@ namespace omb {
 
 __host__ __device__ constexpr int sp_row_threads(int NX, int G) { return (3 * G * plan2_max(NX) + 31) / 32 * 32; }
 __host__ __device__ constexpr int sp_col_threads(int NY, int TX) { return (3 * TX * plan2_max(NY) + 31) / 32 * 32; }
-// CTAs per SM the register budget is set for (the 52 KB block allows four)
+// CTAs per SM the register budget is set for (the 52 KB FP32 block allows four; an FP64 row
+// block is twice as large and its A or B complex doubles need ≈80 registers)
 __host__ __device__ constexpr int sp_min_blocks(int nt) { return nt <= 384 ? 3 : (nt <= 512 ? 2 : 1); }
+template <typename T> __host__ __device__ constexpr int sp_row_min_blocks(int nt) {
+  return sizeof(T) == 4 ? sp_min_blocks(nt) : (nt <= 512 ? 2 : 1);
+}
 
 // ------------------------------------------------------------------------------------
 // row_in.  Grid: (ceil(Ny/G), max columns, units); sp_row_threads(NX, G) threads.
-template <int NX, int MODE, bool INV, int G>
-__global__ void __launch_bounds__(sp_row_threads(NX, G), sp_min_blocks(sp_row_threads(NX, G)))
-    k_row_in_sp(const OpUnit<float>* __restrict__ units, const float2* __restrict__ tw_g) {
-  using T = float;
-  using C = cplx<float>;
+template <typename T, int NX, int MODE, bool INV, int G>
+__global__ void __launch_bounds__(sp_row_threads(NX, G), sp_row_min_blocks<T>(sp_row_threads(NX, G)))
+    k_row_in_sp(const OpUnit<T>* __restrict__ units, const cplx<T>* __restrict__ tw_g) {
+  using C = cplx<T>;
   constexpr int A = plan2_a(NX), B = NX / A, NT = sp_row_threads(NX, G);
   constexpr int LS = l2_row_lstr<C, NX>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -179,11 +183,10 @@ __global__ void __launch_bounds__(sp_col_threads(NY, TX), MINB)
 
 // ------------------------------------------------------------------------------------
 // row_out.  Grid: (ceil(Ny/G), max columns, units); sp_row_threads(NX, G) threads.
-template <int NX, int MODE, bool INV, int G>
-__global__ void __launch_bounds__(sp_row_threads(NX, G), sp_min_blocks(sp_row_threads(NX, G)))
-    k_row_out_sp(const OpUnit<float>* __restrict__ units, const float2* __restrict__ tw_g) {
-  using T = float;
-  using C = cplx<float>;
+template <typename T, int NX, int MODE, bool INV, int G>
+__global__ void __launch_bounds__(sp_row_threads(NX, G), sp_row_min_blocks<T>(sp_row_threads(NX, G)))
+    k_row_out_sp(const OpUnit<T>* __restrict__ units, const cplx<T>* __restrict__ tw_g) {
+  using C = cplx<T>;
   constexpr int A = plan2_a(NX), B = NX / A, NT = sp_row_threads(NX, G);
   constexpr int LS = l2_row_lstr<C, NX>();
   extern __shared__ __align__(16) unsigned char smem_raw[];

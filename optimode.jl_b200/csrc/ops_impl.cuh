@@ -81,20 +81,22 @@ static cudaError_t col_tx(const OpUnit<T>* u, int nunits, int Nx, int maxcol, co
   return launch_pass<T>(k_col2<T, NY, S1, PW, S2, TX>, g, NT, sm, st, u, tw);
 }
 
-template <int NX, int MODE, bool INV>
-static cudaError_t row_in_sp(const OpUnit<float>* u, int nunits, int Ny, int maxcol, const float2* tw, cudaStream_t st) {
+template <int NX, int MODE, bool INV, typename T = float>
+static cudaError_t row_in_sp(const OpUnit<T>* u, int nunits, int Ny, int maxcol, const cplx<T>* tw, cudaStream_t st) {
   constexpr int G = l2_rows(NX), NT = sp_row_threads(NX, G);
-  const size_t sm = (size_t)3 * G * l2_row_lstr<float2, NX>() * sizeof(float2);
+  const size_t sm = (size_t)3 * G * l2_row_lstr<cplx<T>, NX>() * sizeof(cplx<T>);
   const dim3 g((Ny + G - 1) / G, maxcol, nunits);
-  return launch_pass<float>(k_row_in_sp<NX, MODE, INV, G>, g, NT, sm, st, u, tw);
+  return launch_pass<T>(k_row_in_sp<T, NX, MODE, INV, G>, g, NT, sm, st, u, tw);
 }
-template <int NX, int MODE, bool INV>
-static cudaError_t row_out_sp(const OpUnit<float>* u, int nunits, int Ny, int maxcol, const float2* tw, cudaStream_t st) {
+template <int NX, int MODE, bool INV, typename T = float>
+static cudaError_t row_out_sp(const OpUnit<T>* u, int nunits, int Ny, int maxcol, const cplx<T>* tw, cudaStream_t st) {
   constexpr int G = l2_rows(NX), NT = sp_row_threads(NX, G);
-  const size_t sm = (size_t)3 * G * l2_row_lstr<float2, NX>() * sizeof(float2);
+  const size_t sm = (size_t)3 * G * l2_row_lstr<cplx<T>, NX>() * sizeof(cplx<T>);
   const dim3 g((Ny + G - 1) / G, maxcol, nunits);
-  return launch_pass<float>(k_row_out_sp<NX, MODE, INV, G>, g, NT, sm, st, u, tw);
+  return launch_pass<T>(k_row_out_sp<T, NX, MODE, INV, G>, g, NT, sm, st, u, tw);
 }
+// FP64 M̂ row passes in the component-parallel form (one thread per line slot and component)
+constexpr bool FP64_ROW_SPLIT = true;
 template <int NY, int S1, int PW, int S2, int MINB>
 static cudaError_t col_sp(const OpUnit<float>* u, int nunits, int Nx, int maxcol, const float2* tw, cudaStream_t st) {
   constexpr int TX = l2_tx<float>(NY), NT = sp_col_threads(NY, TX);
@@ -113,6 +115,9 @@ static cudaError_t row_in_nx(int mode, const OpUnit<T>* u, int nunits, int Ny, i
     if (mode == RI_KXTC && gv != 1)
       return gv == 0 ? row_in_g<T, NX, row_g_variant<NX>(0), RI_KXTC, false>(u, nunits, Ny, maxcol, tw, st)
                      : row_in_g<T, NX, row_g_variant<NX>(2), RI_KXTC, false>(u, nunits, Ny, maxcol, tw, st);
+  }
+  if constexpr (plan2_a(NX) != 0 && sizeof(T) == 8) {
+    if (FP64_ROW_SPLIT && mode == RI_KXTC) return row_in_sp<NX, RI_KXTC, false, T>(u, nunits, Ny, maxcol, tw, st);
   }
   if constexpr (plan2_a(NX) != 0) {  // two-level register FFT
     constexpr int G = l2_rows(NX), NT = l2_row_threads(NX);
@@ -157,6 +162,9 @@ static cudaError_t row_out_nx(int mode, const OpUnit<T>* u, int nunits, int Ny, 
     if (mode == RO_KXCT && gv != 1)
       return gv == 0 ? row_out_g<T, NX, row_g_variant<NX>(0), RO_KXCT, true>(u, nunits, Ny, maxcol, tw, st)
                      : row_out_g<T, NX, row_g_variant<NX>(2), RO_KXCT, true>(u, nunits, Ny, maxcol, tw, st);
+  }
+  if constexpr (plan2_a(NX) != 0 && sizeof(T) == 8) {
+    if (FP64_ROW_SPLIT && mode == RO_KXCT) return row_out_sp<NX, RO_KXCT, true, T>(u, nunits, Ny, maxcol, tw, st);
   }
   if constexpr (plan2_a(NX) != 0) {  // two-level register FFT
     constexpr int G = l2_rows(NX), NT = l2_row_threads(NX);
