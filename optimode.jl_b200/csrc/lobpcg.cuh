@@ -370,16 +370,34 @@ __global__ void __launch_bounds__(GramCfg<T>::NT, 1)
     if (++q == stages) { q = 0; ph ^= 1; }
     if (w.last_of_track()) {
       // the split partial sums of each item meet in shared memory (FP64), then one global
-      // atomic per matrix entry
-      if (active) {
+      // atomic per matrix entry.  The split threads of an item are a contiguous run of lanes
+      // (item = tid / split), so each warp first sums its part of every run with a segmented
+      // shuffle (suffix sums toward the run's first lane; every lane of the warp takes part,
+      // idle ones with zeros) and only that first lane adds to shared memory: a few adds per
+      // entry instead of `split` (up to 80) contending ones.
+      {
+        const int key = active ? item : -1;
+        const unsigned seg = __match_any_sync(0xffffffffu, key);
+        const int head = __ffs(seg) - 1;
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
-            double vx = (double)acc[i][j].x, vy = (double)acc[i][j].y;
-            if constexpr (COMP) { vx += (double)lo[i][j].x; vy += (double)lo[i][j].y; }
-            atomicAdd(&red[item * 16 + i * 4 + j].x, vx);
-            atomicAdd(&red[item * 16 + i * 4 + j].y, vy);
+            double vx = 0.0, vy = 0.0;
+            if (active) {
+              vx = (double)acc[i][j].x;
+              vy = (double)acc[i][j].y;
+              if constexpr (COMP) { vx += (double)lo[i][j].x; vy += (double)lo[i][j].y; }
+            }
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+              const double tx = __shfl_down_sync(0xffffffffu, vx, o), ty = __shfl_down_sync(0xffffffffu, vy, o);
+              if (lane + o < 32 && ((seg >> (lane + o)) & 1u)) { vx += tx; vy += ty; }
+            }
+            if (active && lane == head) {
+              atomicAdd(&red[item * 16 + i * 4 + j].x, vx);
+              atomicAdd(&red[item * 16 + i * 4 + j].y, vy);
+            }
           }
       }
       bar_sync_count(1, NC);
