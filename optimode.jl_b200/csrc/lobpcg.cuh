@@ -161,12 +161,14 @@ __global__ void k_live_prefix(TrackState* const* __restrict__ states, const long
                               long long* __restrict__ wpre_g, long long* __restrict__ wpre_u);
 // Relative cost of one tile of a track with n block columns of which M are X: the Gram's 4×4
 // items (each 16 complex products per row) plus its loads; the update's n·M products per row
-// of X, AX, P, AP plus its 4M stores.
+// of X, AX, P, AP plus its 4M stores plus a fixed 16 per tile (pipeline round trips and
+// bulk-copy set-up: per-CTA times on B200 fit 1.25 µs per tile + 0.08 µs per unit of
+// n·M + 4M to 5 %).
 __host__ __device__ __forceinline__ long long gram_tile_cost(int n) {
   const int nb4 = (n + 3) / 4;
   return 8LL * nb4 * (nb4 + 1) + n;
 }
-__host__ __device__ __forceinline__ long long update_tile_cost(int n, int M) { return (long long)n * M + 4LL * M; }
+__host__ __device__ __forceinline__ long long update_tile_cost(int n, int M) { return (long long)n * M + 4LL * M + 16; }
 
 // ---- Gram ---------------------------------------------------------------------------
 // G = ZᴴZ and S = ZᴴAZ (upper triangles).  The outputs are cut into 4×4 blocks (items);
