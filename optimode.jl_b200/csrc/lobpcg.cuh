@@ -219,6 +219,18 @@ __device__ __forceinline__ void two_sum_acc(float& s, float& lo, float x) {
   s = t;
 }
 
+// (acc, lo) += t entry by entry with two-sum; t is cleared.
+__device__ __forceinline__ void gram_fold(float2 (&acc)[4][4], float2 (&lo)[4][4], float2 (&t)[4][4]) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      two_sum_acc(acc[i][j].x, lo[i][j].x, t[i][j].x);
+      two_sum_acc(acc[i][j].y, lo[i][j].y, t[i][j].y);
+      t[i][j] = make_float2(0.f, 0.f);
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(GramCfg<T>::NT, 1)
     k_gram(const TrackDesc<T>* __restrict__ D, const int* __restrict__ pre, const long long* __restrict__ wpre,
@@ -283,11 +295,17 @@ __global__ void __launch_bounds__(GramCfg<T>::NT, 1)
   int q = 0;
   uint32_t ph = 0;
   bool failed = false;
-  // FP32: each tile's rows are summed into t, and the tile sums into the compensated pair
-  // (acc, lo) by two-sum (Knuth), so the rounding error of the track's sum stays at the
-  // FP32 level of one tile instead of growing with the number of tiles; FP64 sums directly.
+  // FP32: a thread's rows are summed into t, and t into the compensated pair (acc, lo) by
+  // two-sum (Knuth) once the thread has summed GRAM_FOLD_ROWS rows (or a whole tile's share,
+  // when that is more), so the rounding error of the track's sum stays at the FP32 level of
+  // that many rows instead of growing with the number of tiles; FP64 sums directly.  Folding
+  // by rows rather than every tile keeps the fold (32 two-sums, the compensation terms in
+  // local memory) off the tiles of narrow tracks, whose items are split over ≈240 threads
+  // with one or two rows each.
   constexpr bool COMP = sizeof(T) == 4;
-  C acc[4][4], lo[COMP ? 4 : 1][COMP ? 4 : 1];
+  constexpr int GRAM_FOLD_ROWS = 16;
+  C acc[4][4], lo[COMP ? 4 : 1][COMP ? 4 : 1], t[COMP ? 4 : 1][COMP ? 4 : 1];
+  int tcnt = 0;
   int cur = -1, items = 0, split = 1, nblk = 0, nb4 = 1, n = 0, item = 0, sub = 0, which = 0, bi = 0, bj = 0;
   bool active = false;
   for (; w.valid(); w.next()) {
@@ -312,7 +330,8 @@ __global__ void __launch_bounds__(GramCfg<T>::NT, 1)
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
-          for (int j = 0; j < 4; ++j) lo[i][j] = mk<C>(0, 0);
+          for (int j = 0; j < 4; ++j) { lo[i][j] = mk<C>(0, 0); t[i][j] = mk<C>(0, 0); }
+        tcnt = 0;
       }
     }
     const int rows = (int)min((long long)R, d.n2 - w.row0());
@@ -325,11 +344,12 @@ __global__ void __launch_bounds__(GramCfg<T>::NT, 1)
         const C* za = st + (size_t)(4 * bi) * CS;
         const C* zb = st + (size_t)((which ? Cfg::n4(n) : 0) + 4 * bj) * CS;
         if constexpr (COMP) {
-          C t[4][4];
-#pragma unroll
-          for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) t[i][j] = mk<C>(0, 0);
+          const int mine = rows > sub ? (rows - sub + split - 1) / split : 0;
+          if (tcnt > 0 && tcnt + mine > GRAM_FOLD_ROWS) {
+            gram_fold(acc, lo, t);
+            tcnt = 0;
+          }
+          tcnt += mine;
 #pragma unroll 2
           for (int r = sub; r < rows; r += split) {
             C a[4], b[4];
@@ -343,13 +363,6 @@ __global__ void __launch_bounds__(GramCfg<T>::NT, 1)
                 t[i][j].y += a[i].x * b[j].y - a[i].y * b[j].x;
               }
           }
-#pragma unroll
-          for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              two_sum_acc(acc[i][j].x, lo[i][j].x, t[i][j].x);
-              two_sum_acc(acc[i][j].y, lo[i][j].y, t[i][j].y);
-            }
         } else {
 #pragma unroll 2
           for (int r = sub; r < rows; r += split) {
@@ -377,6 +390,9 @@ __global__ void __launch_bounds__(GramCfg<T>::NT, 1)
       // shuffle (suffix sums toward the run's first lane; every lane of the warp takes part,
       // idle ones with zeros) and only that first lane adds to shared memory: a few adds per
       // entry instead of `split` (up to 80) contending ones.
+      if constexpr (COMP) {
+        if (active && tcnt > 0) gram_fold(acc, lo, t);
+      }
       {
         const int key = active ? item : -1;
         const unsigned seg = __match_any_sync(0xffffffffu, key);
