@@ -26,7 +26,7 @@ __global__ void k_live_prefix(TrackState* const* __restrict__ states, const long
       const int n = s.M + s.nWa + s.nP;
       vg = (int)((n2[t] + rg - 1) / rg);
       vu = (int)((n2[t] + ru - 1) / ru);
-      xg = vg * gram_tile_cost(n);
+      xg = vg * gram_tile_cost(n) + GRAM_TRACK_COST;
       xu = vu * update_tile_cost(n, s.M);
     }
     sg[tid] = vg; su[tid] = vu; wg[tid] = xg; wu[tid] = xu;

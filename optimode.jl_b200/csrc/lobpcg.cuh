@@ -110,9 +110,10 @@ struct TileWalk {
   int ntracks, t;      // current track
   long long i, end;    // current global tile, one past the last
   int R;
-  // first global tile whose cost-weighted start is ≥ x (wpre: prefix of the tracks' summed
-  // tile costs, the tiles of one track costing the same)
-  __device__ __forceinline__ long long tile_at(const long long* wpre, long long x) const {
+  // first global tile whose cost-weighted start is ≥ x (wpre: prefix of the tracks' costs,
+  // each a fixed F followed by its tiles, the tiles of one track costing the same; a point
+  // inside a track's F maps to its first tile)
+  __device__ __forceinline__ long long tile_at(const long long* wpre, long long F, long long x) const {
     if (x >= wpre[ntracks]) return pre[ntracks];
     int lo = 0, hi = ntracks - 1;  // first track with wpre[t+1] > x
     while (lo < hi) {
@@ -120,17 +121,19 @@ struct TileWalk {
       if (wpre[mid + 1] > x) hi = mid; else lo = mid + 1;
     }
     const long long nt = pre[lo + 1] - pre[lo];
-    const long long wt = (wpre[lo + 1] - wpre[lo]) / nt;
-    const long long j = (x - wpre[lo] + wt - 1) / wt;
+    const long long wt = (wpre[lo + 1] - wpre[lo] - F) / nt;
+    const long long xr = x - wpre[lo] - F;
+    const long long j = xr > 0 ? (xr + wt - 1) / wt : 0;
     return pre[lo] + (j < nt ? j : nt);
   }
-  // wpre == nullptr: every tile costs the same
-  __device__ __forceinline__ void start(const int* pre_, const long long* wpre, int ntracks_, int R_) {
+  // wpre == nullptr: every tile costs the same; F: the fixed cost per live track in wpre
+  __device__ __forceinline__ void start(const int* pre_, const long long* wpre, int ntracks_, int R_,
+                                        long long F = 0) {
     pre = pre_; ntracks = ntracks_; R = R_;
     if (wpre && wpre[ntracks] > 0) {
       const long long W = wpre[ntracks];
-      i = tile_at(wpre, (long long)blockIdx.x * W / gridDim.x);
-      end = tile_at(wpre, (long long)(blockIdx.x + 1) * W / gridDim.x);
+      i = tile_at(wpre, F, (long long)blockIdx.x * W / gridDim.x);
+      end = tile_at(wpre, F, (long long)(blockIdx.x + 1) * W / gridDim.x);
     } else {
       const long long T = pre[ntracks];
       i = (long long)blockIdx.x * T / gridDim.x;
@@ -160,13 +163,16 @@ __global__ void k_live_prefix(TrackState* const* __restrict__ states, const long
                               int ntracks, int rg, int ru, int* __restrict__ pre_g, int* __restrict__ pre_u,
                               long long* __restrict__ wpre_g, long long* __restrict__ wpre_u);
 // Relative cost of one tile of a track with n block columns of which M are X: the Gram's 4×4
-// items (each 16 complex products per row) plus its loads; the update's n·M products per row
-// of X, AX, P, AP plus its 4M stores plus a fixed 16 per tile (pipeline round trips and
-// bulk-copy set-up: per-CTA times on B200 fit 1.25 µs per tile + 0.08 µs per unit of
-// n·M + 4M to 5 %).
+// items (each 16 complex products per row) plus its loads plus a fixed GRAM_TILE_FIXED, and
+// GRAM_TRACK_COST once per track for the flush of its sums (each CTA that takes part in a
+// track adds its partial sums to the track's Gram); the update's n·M products per row of X,
+// AX, P, AP plus its 4M stores plus a fixed 16 per tile (pipeline round trips and bulk-copy
+// set-up: per-CTA times on B200 fit 1.25 µs per tile + 0.08 µs per unit of n·M + 4M to 5 %).
+constexpr long long GRAM_TILE_FIXED = 48;
+constexpr long long GRAM_TRACK_COST = 390;
 __host__ __device__ __forceinline__ long long gram_tile_cost(int n) {
   const int nb4 = (n + 3) / 4;
-  return 8LL * nb4 * (nb4 + 1) + n;
+  return 8LL * nb4 * (nb4 + 1) + n + GRAM_TILE_FIXED;
 }
 __host__ __device__ __forceinline__ long long update_tile_cost(int n, int M) { return (long long)n * M + 4LL * M + 16; }
 
@@ -250,7 +256,7 @@ __global__ void __launch_bounds__(GramCfg<T>::NT, 1)
   }
   __syncthreads();
   TileWalk w;
-  w.start(pre, wpre, ntracks, R);
+  w.start(pre, wpre, ntracks, R, GRAM_TRACK_COST);
   if (warp == Cfg::NCW) {
     // ---- producer: one bulk copy per column segment of the tile
     int q = 0, fills[8] = {0, 0, 0, 0, 0, 0, 0, 0};
