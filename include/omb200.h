@@ -349,7 +349,8 @@ int omb_profile_apply(omb_ctx* ctx, int op, int precision, const omb_grid* grid,
  * (≤ 36) of n2 complex rows (host ComplexF64, column after column), computed by the same
  * streaming kernel as a LOBPCG iteration (n2 even, as every solver vector is) in FP32
  * (operands rounded to FP32, products summed
- * per tile and the tile sums compensated by two-sum) or FP64.  G and S receive n×n ComplexF64,
+ * over at most 16 rows per thread, or one tile's share, and those sums compensated by
+ * two-sum) or FP64.  G and S receive n×n ComplexF64,
  * column-major.  No reference counterpart (accuracy check of the FP32 reductions; the
  * reference's products are BLAS calls, ME/src/solvers/dftk.jl:129-132). */
 int omb_gram_blocks(omb_ctx* ctx, int precision, int64_t n2, int32_t n, const double* Z, const double* AZ,
