@@ -358,16 +358,21 @@ __global__ void __launch_bounds__(GramCfg<T>::NT, 1)
           tcnt += mine;
 #pragma unroll 2
           for (int r = sub; r < rows; r += split) {
-            C a[4], b[4];
+            C a[4], b[4], bs[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) { a[i] = za[i * CS + r]; b[i] = zb[i * CS + r]; }
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) bs[j] = make_float2(b[j].y, b[j].x);
+            // conj(a)·b = a.x·(b.x, b.y) + a.y·(b.y, −b.x): two packed FP32x2 FMAs per product
 #pragma unroll
-              for (int j = 0; j < 4; ++j) {  // conj(a)·b
-                t[i][j].x += a[i].x * b[j].x + a[i].y * b[j].y;
-                t[i][j].y += a[i].x * b[j].y - a[i].y * b[j].x;
+            for (int i = 0; i < 4; ++i) {
+              const float2 ax = make_float2(a[i].x, a[i].x), ay = make_float2(a[i].y, -a[i].y);
+#pragma unroll
+              for (int j = 0; j < 4; ++j) {
+                t[i][j] = __ffma2_rn(ax, b[j], t[i][j]);
+                t[i][j] = __ffma2_rn(ay, bs[j], t[i][j]);
               }
+            }
           }
         } else {
 #pragma unroll 2
@@ -494,15 +499,15 @@ __device__ __forceinline__ void update_tile(const TrackDesc<T>& d, const TrackSt
 #pragma unroll
             for (int m = 0; m < M; ++m) {
               const C c = Cs[j * MMAX + m];
-              x[m] = x[m] + cmul(z, c);
-              ax[m] = ax[m] + cmul(az, c);
+              x[m] = cmac(x[m], z, c);
+              ax[m] = cmac(ax[m], az, c);
             }
             if (l0 + j >= M) {  // the X rows of CP are zero
 #pragma unroll
               for (int m = 0; m < M; ++m) {
                 const C c = CPs[j * MMAX + m];
-                p[m] = p[m] + cmul(z, c);
-                ap[m] = ap[m] + cmul(az, c);
+                p[m] = cmac(p[m], z, c);
+                ap[m] = cmac(ap[m], az, c);
               }
             }
           }

@@ -47,6 +47,14 @@ __host__ __device__ __forceinline__ double2 operator*(double s, double2 a) { ret
 template <typename C> __host__ __device__ __forceinline__ C cmul(C a, C b) {
   C r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
 }
+// acc + a·b; in FP32 two packed FP32x2 FMAs: acc + (a.x, a.x)·(b.x, b.y) + (a.y, a.y)·(−b.y, b.x)
+__device__ __forceinline__ float2 cmac(float2 acc, float2 a, float2 b) {
+  acc = __ffma2_rn(make_float2(a.x, a.x), b, acc);
+  return __ffma2_rn(make_float2(a.y, a.y), make_float2(-b.y, b.x), acc);
+}
+__device__ __forceinline__ double2 cmac(double2 acc, double2 a, double2 b) {
+  return make_double2(acc.x + (a.x * b.x - a.y * b.y), acc.y + (a.x * b.y + a.y * b.x));
+}
 // a * conj(b)
 template <typename C> __host__ __device__ __forceinline__ C cmulc(C a, C b) {
   C r; r.x = a.x * b.x + a.y * b.y; r.y = a.y * b.x - a.x * b.y; return r;
